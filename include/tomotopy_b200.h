@@ -1,0 +1,158 @@
+/*
+ * tomotopy_b200.h -- C ABI of the B200 collapsed-Gibbs LDA engine.
+ *
+ * This is the drop-in boundary for tomotopy's plain LDAModel hot path.  Each
+ * entry point names the tomotopy interface it replaces (paths relative to
+ * the tomotopy source tree).  Conventions:
+ *   - status codes only (tmt_status); no C++ exception crosses this ABI;
+ *     tmt_last_error() returns the message of a handle's last failure;
+ *   - the caller owns every host buffer; a handle owns its device buffers;
+ *   - calls on one handle are serialised by the caller (tomotopy holds the
+ *     GIL across train/infer, py_LDA.cpp:277-411); the server functions are
+ *     internally thread-safe;
+ *   - word ids >= V (tomotopy's realV, the vocabulary after stop-word
+ *     removal) are carried but never sampled, as in LDAModel.hpp:339;
+ *   - topic ids are uint16 (tomotopy's Tid, Dictionary.h:16), so 1 <= K <= 32767
+ *     (models.py:84);  count matrices are int32 (TermWeight::one);
+ *   - n_kw is K x V column-major: column v holds K contiguous int32, the
+ *     layout of ModelStateLDA::numByTopicWord (LDAModel.hpp:61-67, LDA.h:80-95);
+ *   - n_dk is D x K row-major: row d holds K contiguous int32, one
+ *     DocumentLDA::numByTopic per document (LDA.h:146).
+ */
+#ifndef TOMOTOPY_B200_H
+#define TOMOTOPY_B200_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tmt_status {
+    TMT_OK = 0,
+    TMT_ERR_INVALID_ARGUMENT = -1,  /* tomotopy: exc::InvalidArgument -> ValueError */
+    TMT_ERR_CUDA = -2,
+    TMT_ERR_OUT_OF_MEMORY = -3,     /* device allocation or HBM budget exceeded */
+    TMT_ERR_STATE = -4,             /* call out of order (e.g. train before upload) */
+    TMT_ERR_UNSUPPORTED = -5,
+    TMT_ERR_CANCELLED = -6,
+    TMT_ERR_TIMEOUT = -7,
+    TMT_ERR_INTERNAL = -8           /* tomotopy: train() < 0 -> RuntimeError("Train failed") */
+} tmt_status;
+
+typedef struct tmt_handle tmt_handle;
+
+/* Sampler kernels for the training sweep. */
+typedef enum tmt_sampler {
+    TMT_SAMPLER_AUTO = 0,   /* dense for K <= 256, sparse above */
+    TMT_SAMPLER_DENSE = 1,  /* full K-vector conditional per token */
+    TMT_SAMPLER_SPARSE = 2  /* exact doc/word bucket decomposition */
+} tmt_sampler;
+
+/* Model hyper-parameters.  Mirrors LDAArgs (LDA.h:170-176) plus the
+ * optimiser settings of LDAModel (LDAModel.hpp:210). */
+typedef struct tmt_config {
+    uint32_t K;              /* topics, 1..32767 */
+    uint32_t V;              /* realV: word ids >= V are skipped */
+    const float* alpha;      /* K Dirichlet doc-topic priors, or NULL to use alpha_scalar */
+    float alpha_scalar;
+    float eta;               /* symmetric topic-word prior, > 0 */
+    uint64_t seed;
+    uint32_t optim_interval; /* re-fit alpha every n sweeps after burn_in; 0 = never (tomotopy default 10) */
+    uint32_t burn_in;
+    int32_t device;          /* CUDA device ordinal */
+    int32_t sampler;         /* tmt_sampler */
+    uint64_t hbm_budget;     /* bytes this handle may allocate; 0 = unlimited */
+} tmt_config;
+
+/* Read-only facts about a handle. */
+typedef struct tmt_info {
+    uint64_t D;              /* documents */
+    uint64_t N_all;          /* tokens uploaded (all word ids) */
+    uint64_t N;              /* tokens sampled (word id < V) */
+    uint64_t global_step;    /* sweeps done (TopicModel::globalStep) */
+    uint64_t device_bytes;   /* device memory held by the handle */
+    uint32_t K, V;
+    int32_t sampler;         /* the sampler the last sweep used */
+    float last_sweep_ms;     /* device time of the last sweep (CUDA events) */
+    uint64_t kernel_launches;/* kernels launched by this handle so far */
+    double sweep_kernel_ms;  /* device time of the sweep kernels of the last tmt_train call */
+    uint32_t sweeps_timed;   /* sweeps in that sum */
+} tmt_info;
+
+/* Replaces ILDAModel::create (LDAModel.cpp:10-13) + the LDAModel ctor checks
+ * (LDAModel.hpp:962-983): K in 1..32767, alpha > 0, eta > 0. */
+tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out);
+
+/* Replaces LDAModel::prepare's device-relevant part (LDAModel.hpp:1073-1138):
+ * uploads the doc-major corpus (words already vocab-reordered and sorted by
+ * id inside each document, as prepareDoc does, LDAModel.hpp:716-722), builds
+ * the word-major layout, draws z0 ~ Discrete(alpha) (initializeDocState,
+ * LDAModel.hpp:781-813) unless z0 is given, and builds n_dk, n_kw and n_k.
+ * wid[doc_off[D]], doc_off[D+1]; z0 is doc-major or NULL. */
+tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off,
+                             uint64_t D, const uint16_t* z0);
+
+/* Replaces TopicModel::train (TopicModel.hpp:684-755) -> LDAModel::trainOne
+ * (LDAModel.hpp:505-539): `iters` sweeps, each = sampling (performSampling /
+ * sampleDocument, :326-428) + count merge (mergeState, :552-580) + alpha
+ * optimisation when due (:529-532).  When ll_every > 0 and ll_out != NULL,
+ * writes the FP64 log-likelihood after every ll_every-th sweep
+ * (iters / ll_every values). */
+tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* ll_out);
+
+/* Replaces getLLDocs / getLLRest (LDAModel.hpp:616-668) in FP64:
+ * ll_docs over n_dk, ll_rest over n_kw and n_k.  ll_per_word =
+ * (ll_docs + ll_rest) / N (TopicModel.hpp:757-760). */
+tmt_status tmt_ll(tmt_handle* h, double* ll_docs, double* ll_rest);
+
+/* Downloads the model state (any pointer may be NULL): z doc-major
+ * (N_all uint16, 0xFFFF for skipped words; DocumentLDA::Zs), n_kw (K x V
+ * column-major), n_k (K), alpha (K, after optimisation). */
+tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t* n_k, float* alpha);
+
+/* Downloads n_dk (D x K row-major int32; DocumentLDA::numByTopic). */
+tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
+
+/* Host-side preparation of an integer-id corpus, replacing the vocabulary
+ * part of LDAModel::prepare (LDAModel.hpp:1073-1138): removeStopwords
+ * (TopicModel.hpp:526-571) reorders ids by (cf, df) descending with the
+ * min_cf / min_df / rm_top rules and yields realV; prepareDoc
+ * (LDAModel.hpp:716-722) sorts every document by the new ids.  Outputs:
+ * words_out[N] (doc-major, re-numbered, sorted per doc), w_order[N]
+ * (w_order[original position] = sorted position within the doc; may be NULL),
+ * vocab_order[n_vocab] (old id -> new id), vocab_cf / vocab_df (by new id;
+ * may be NULL), *real_v. */
+tmt_status tmt_prepare_corpus(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                              uint32_t n_vocab, uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
+                              uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
+                              uint64_t* vocab_cf, uint64_t* vocab_df, uint32_t* real_v);
+
+tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out);
+const char* tmt_last_error(const tmt_handle* h);
+void tmt_destroy(tmt_handle* h);
+
+/* ---- synthetic corpus (workload generator; not a tomotopy interface) ---- */
+typedef enum tmt_len_kind { TMT_LEN_POISSON = 0, TMT_LEN_LOGNORMAL = 1 } tmt_len_kind;
+typedef struct tmt_synth_spec {
+    uint32_t V, T;           /* vocabulary, true topics */
+    uint64_t D;              /* documents */
+    int32_t len_kind;        /* tmt_len_kind */
+    double len_a, len_b;     /* Poisson mean | lognormal mu, sigma */
+    uint32_t len_min, len_max;
+    double doc_alpha;        /* theta_d ~ Dirichlet(doc_alpha) */
+    double topic_beta;       /* phi_t ~ Dirichlet(topic_beta * V * Zipf(zipf_s)) */
+    double zipf_s;
+    uint64_t seed;
+    uint32_t threads;        /* 0 = all hardware threads */
+} tmt_synth_spec;
+
+/* Two calls: with words == NULL fills doc_off[D+1] and *n_tokens; then with
+ * words of capacity >= *n_tokens fills the word ids (doc-major). */
+tmt_status tmt_synth_corpus(const tmt_synth_spec* spec, uint64_t* doc_off,
+                            uint32_t* words, uint64_t capacity, uint64_t* n_tokens);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,964 @@
+/*
+ * tmt_oracle.c -- CPU oracle for the tomotopy LDA collapsed-Gibbs path.
+ * TEST INFRASTRUCTURE ONLY: see tmt_oracle.h for scope, citations and the
+ * parity status.  Build with -ffp-contract=off so that float expressions
+ * round exactly as written (the device code spells out the same operations
+ * with round-to-nearest intrinsics).
+ */
+#include "tmt_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10                                                            */
+/* ------------------------------------------------------------------------ */
+static inline void mulhilo32(uint32_t a, uint32_t b, uint32_t* hi, uint32_t* lo)
+{
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    *hi = (uint32_t)(p >> 32);
+    *lo = (uint32_t)p;
+}
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c0, &hi0, &lo0);
+        mulhilo32(0xCD9E8D57u, c2, &hi1, &lo1);
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        uint32_t n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+float orc_u01(uint32_t x)
+{
+    return (float)(x >> 8) * (1.0f / 16777216.0f);
+}
+
+static inline uint32_t philox_first(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint64_t seed)
+{
+    uint32_t ctr[4] = { c0, c1, c2, c3 };
+    uint32_t key[2] = { (uint32_t)seed, (uint32_t)(seed >> 32) };
+    uint32_t out[4];
+    orc_philox4x32_10(ctr, key, out);
+    return out[0];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Float LUTs (restating src/Utils/LUT.hpp:11-70 and math.h:119-153)        */
+/* ------------------------------------------------------------------------ */
+/* LUT3<F, float, N, S, M, T, L, U>: three linear-interpolation segments,
+ * [0, N/S) step 1/S, [N/S, N/S + M/T) step 1/T, then step 1/U for L points;
+ * below smallThreshold and above the last point a closed form is used. */
+typedef struct {
+    float* points;
+    size_t N, M, L;
+    float P, Q, R;
+} lut3;
+
+static const float ORC_PI = 3.14159265f;
+
+/* tomotopy's F_lgamma calls the unqualified lgamma / log, which resolve to
+ * the double overloads: the table holds (float)lgamma((double)x) and the
+ * closed forms are evaluated in double, then rounded to float. */
+static float F_lgamma_small(float x)
+{
+    if (x == 0) return INFINITY;
+    return (float)((x + 0.5f) * log((double)(x + 1)) - (double)(x + 1) + log((double)(2 * ORC_PI)) / 2
+                   + (double)(1 / 12.f / (x + 1)) - log((double)x));
+}
+static float F_lgamma_large(float x)
+{
+    return (float)((x - 0.5f) * log((double)x) - (double)x + log((double)(2 * ORC_PI)) / 2
+                   + (double)(1 / 12.f / x));
+}
+static float F_lgamma_nonfinite(float x)
+{
+    if (isnan(x)) return NAN;
+    if (x > 0) return INFINITY;
+    return -INFINITY;
+}
+
+static float F_digamma_small(float x)
+{
+    if (x == 0) return -INFINITY;
+    return logf(x + 2) - 0.5f / (x + 2) - 1 / 12.f / powf(x + 2, 2) - 1 / (x + 1) - 1 / x;
+}
+static float F_digamma_large(float x)
+{
+    return logf(x) - 0.5f / x - 1 / 12.f / powf(x, 2);
+}
+static float F_digamma_nonfinite(float x)
+{
+    if (isnan(x) || x < 0) return NAN;
+    return INFINITY;
+}
+
+/* digammaf: the float recursion + Chebyshev series of math.h:72-115 */
+float orc_digammaf(float x)
+{
+    static const float gam = 0.577215664f, ln2 = 0.693147180f;
+    if (x < 0.0f)
+        return orc_digammaf(1.0f - x) + ORC_PI / tanf(ORC_PI * (1.0f - x));
+    else if (x < 1.0f)
+        return orc_digammaf(1.0f + x) - 1.0f / x;
+    else if (x == 1.0f)
+        return -gam;
+    else if (x == 2.0f)
+        return (float)(1.0L - gam);
+    else if (x == 3.0f)
+        return (float)(1.5L - gam);
+    else if (x > 3.0f)
+        return 0.5f * (orc_digammaf(x / 2.0f) + orc_digammaf((x + 1.0f) / 2.0f)) + ln2;
+    else {
+        static const float kn[] = { .304591985f,
+            .720379774f, -.124549592f,
+            .277694573e-1f, -.677623714e-2f,
+            .172387551e-2f, -.448176990e-3f,
+            .117936600e-3f, -.312538942e-4f,
+            .831739970e-5f, -.221914276e-5f,
+            .593022667e-6f, -.158630511e-6f,
+            .424592039e-7f, -.113691296e-7f,
+            .304502217e-8f, -.815684550e-9f, };
+        float Tn_1 = 1.0f;
+        float Tn = (float)(x - 2.0);
+        float resul = kn[0] + kn[1] * Tn;
+        x = (float)(x - 2.0L);
+        for (size_t n = 2; n < sizeof(kn) / sizeof(float); n++) {
+            const float Tn1 = (float)(2.0L * x * Tn - Tn_1);
+            resul += kn[n] * Tn1;
+            Tn_1 = Tn;
+            Tn = Tn1;
+        }
+        return resul;
+    }
+}
+
+static lut3 g_lgamma, g_digamma;
+static pthread_once_t g_lut_once = PTHREAD_ONCE_INIT;
+
+static void lut3_build(lut3* t, int which, size_t N, size_t S, size_t M, size_t T, size_t L, size_t U)
+{
+    t->N = N; t->M = M; t->L = L;
+    t->P = (float)(1. / S); t->Q = (float)(1. / T); t->R = (float)(1. / U);
+    t->points = (float*)calloc(N + M + L, sizeof(float));
+    for (size_t i = 0; i < N; i++) {
+        float x = i ? i * t->P : (float)0.0001;
+        t->points[i] = which ? orc_digammaf(x) : (float)lgamma((double)x);
+    }
+    for (size_t i = 0; i < M; i++) {
+        float x = i * t->Q + N * t->P;
+        t->points[i + N] = which ? orc_digammaf(x) : (float)lgamma((double)x);
+    }
+    for (size_t i = 0; i < L; i++) {
+        float x = i * t->R + N * t->P + M * t->Q;
+        t->points[i + N + M] = which ? orc_digammaf(x) : (float)lgamma((double)x);
+    }
+}
+
+static void luts_init(void)
+{
+    lut3_build(&g_lgamma, 0, 1 * 1024, 1024, 100 * 64, 64, 1000 * 8, 8);
+    lut3_build(&g_digamma, 1, 1 * 1024, 1024, 100 * 64, 64, 1000 * 4, 4);
+}
+
+static float lut3_get(const lut3* t, float x, int which)
+{
+    if (!isfinite(x)) return which ? F_digamma_nonfinite(x) : F_lgamma_nonfinite(x);
+    if (x < 0) return NAN;
+    if (x < (float)0.001) return which ? F_digamma_small(x) : F_lgamma_small(x);
+    const size_t N = t->N, M = t->M, L = t->L;
+    const float P = t->P, Q = t->Q, R = t->R;
+    if (x >= N * P + M * Q + (L - 1) * R) return which ? F_digamma_large(x) : F_lgamma_large(x);
+    size_t idx;
+    float a;
+    float nx = x;
+    if (x < N * P) {
+        idx = (size_t)(nx / P);
+        a = (nx - idx * P) / P;
+    } else {
+        nx -= N * P;
+        if (nx < M * Q) {
+            idx = (size_t)(nx / Q);
+            a = (nx - idx * Q) / Q;
+            idx += N;
+        } else {
+            nx -= M * Q;
+            idx = (size_t)(nx / R);
+            a = (nx - idx * R) / R;
+            idx += N + M;
+        }
+    }
+    return t->points[idx] + a * (t->points[idx + 1] - t->points[idx]);
+}
+
+float orc_lgammaT(float x)
+{
+    pthread_once(&g_lut_once, luts_init);
+    return lut3_get(&g_lgamma, x, 0);
+}
+
+float orc_digammaT(float x)
+{
+    pthread_once(&g_lut_once, luts_init);
+    return lut3_get(&g_digamma, x, 1);
+}
+
+/* digammaApprox (math.h:170-176) evaluated in float, as it is over Eigen float arrays */
+float orc_digammaApprox(float z)
+{
+    return logf(z + 4) - 1.f / 2.f / (z + 4) - 1.f / 12.f / ((z + 4) * (z + 4))
+        - 1.f / z - 1.f / (z + 1) - 1.f / (z + 2) - 1.f / (z + 3);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sampling primitives                                                      */
+/* ------------------------------------------------------------------------ */
+/* prefixSum, SSE2 path (sample.hpp:62-86): groups of four are scanned as
+ * x + (x<<1 lane), then + (x<<2 lanes), then offset by the previous group's
+ * last value; the tail (n % 4) is a sequential running sum. */
+void orc_prefix_sum_sse(float* arr, int n)
+{
+    int n4 = n & ~3;
+    float offset = 0.f;
+    for (int i = 0; i < n4; i += 4) {
+        float x0 = arr[i], x1 = arr[i + 1], x2 = arr[i + 2], x3 = arr[i + 3];
+        float y0 = x0, y1 = x1 + x0, y2 = x2 + x1, y3 = x3 + x2;
+        float s0 = y0, s1 = y1, s2 = y2 + y0, s3 = y3 + y1;
+        arr[i] = s0 + offset;
+        arr[i + 1] = s1 + offset;
+        arr[i + 2] = s2 + offset;
+        arr[i + 3] = s3 + offset;
+        offset = arr[i + 3];
+    }
+    if (!n4) n4 = 1;
+    for (int i = n4; i < n; ++i) arr[i] += arr[i - 1];
+}
+
+/* sampleFromDiscreteAcc (sample.hpp:133-189): r = u * cum[K-1]; first z with
+ * r < cum[z]; K-1 if none. */
+size_t orc_sample_acc(const float* cum, size_t K, float u01)
+{
+    float r = u01 * cum[K - 1];
+    for (size_t z = 0; z < K; ++z)
+        if (r < cum[z]) return z;
+    return K - 1;
+}
+
+/* forShuffled (Utils.hpp:157-178) */
+void orc_shuffled_order(size_t N, size_t seed, uint64_t* out)
+{
+    static const size_t primes[16] = {
+        65537, 65539, 65543, 65551, 65557, 65563,
+        65579, 65581, 65587, 65599, 65609, 65617,
+        65629, 65633, 65647, 65651
+    };
+    if (!N) return;
+    size_t P = primes[seed & 0xF];
+    if (N % P == 0) {
+        P = primes[(seed + 1) & 0xF];
+        if (N % P == 0) P = primes[(seed + 2) & 0xF];
+        if (N % P == 0) P = primes[(seed + 3) & 0xF];
+    }
+    P %= N;
+    for (size_t i = 0; i < N; ++i) out[i] = ((i + seed) * P) % N;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Corpus preparation                                                       */
+/* ------------------------------------------------------------------------ */
+typedef struct { uint64_t cf, df; uint32_t idx; } cfdf;
+static uint64_t g_min_cf, g_min_df;
+
+static int cfdf_bad(const cfdf* a) { return a->cf < g_min_cf || a->df < g_min_df; }
+/* the comparator of removeStopwords (TopicModel.hpp:538-551): valid words
+ * first, each group by (cf, df) descending */
+static int cfdf_less(const cfdf* a, const cfdf* b)
+{
+    int ab = cfdf_bad(a), bb = cfdf_bad(b);
+    if (ab) {
+        if (bb) return (a->cf > b->cf) || (a->cf == b->cf && a->df > b->df);
+        return 0;
+    }
+    if (bb) return 1;
+    return (a->cf > b->cf) || (a->cf == b->cf && a->df > b->df);
+}
+
+/* stable merge sort of cfdf (std::stable_sort semantics) */
+static void cfdf_msort(cfdf* a, cfdf* tmp, size_t n)
+{
+    if (n < 2) return;
+    size_t h = n / 2;
+    cfdf_msort(a, tmp, h);
+    cfdf_msort(a + h, tmp, n - h);
+    size_t i = 0, j = h, k = 0;
+    while (i < h && j < n) {
+        if (cfdf_less(&a[j], &a[i])) tmp[k++] = a[j++];
+        else tmp[k++] = a[i++];
+    }
+    while (i < h) tmp[k++] = a[i++];
+    while (j < n) tmp[k++] = a[j++];
+    memcpy(a, tmp, n * sizeof(cfdf));
+}
+
+uint64_t orc_remove_stopwords(uint64_t nv, uint64_t* cf, uint64_t* df,
+                              uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
+                              uint32_t* order)
+{
+    cfdf* v = (cfdf*)malloc((nv + 1) * sizeof(cfdf));
+    cfdf* tmp = (cfdf*)malloc((nv + 1) * sizeof(cfdf));
+    g_min_cf = min_cf; g_min_df = min_df;
+    for (uint64_t i = 0; i < nv; ++i) { v[i].cf = cf[i]; v[i].df = df[i]; v[i].idx = (uint32_t)i; }
+    cfdf_msort(v, tmp, nv);
+    /* std::rotate(begin, begin + rm_top, end) */
+    if (rm_top && nv) {
+        uint64_t r = rm_top < nv ? rm_top : nv;
+        memcpy(tmp, v, r * sizeof(cfdf));
+        memmove(v, v + r, (nv - r) * sizeof(cfdf));
+        memcpy(v + (nv - r), tmp, r * sizeof(cfdf));
+    }
+    uint64_t lim = nv - (rm_top < nv ? rm_top : nv);
+    uint64_t realV = lim;
+    for (uint64_t i = 0; i < lim; ++i) {
+        if (cfdf_bad(&v[i])) { realV = i; break; }
+    }
+    for (uint64_t i = 0; i < nv; ++i) {
+        order[v[i].idx] = (uint32_t)i;
+        cf[i] = v[i].cf;
+        df[i] = v[i].df;
+    }
+    free(v); free(tmp);
+    return realV;
+}
+
+typedef struct { uint32_t w; uint32_t i; } wpair;
+static void wpair_msort(wpair* a, wpair* tmp, size_t n)
+{
+    if (n < 2) return;
+    size_t h = n / 2;
+    wpair_msort(a, tmp, h);
+    wpair_msort(a + h, tmp, n - h);
+    size_t i = 0, j = h, k = 0;
+    while (i < h && j < n) {
+        if (a[j].w < a[i].w) tmp[k++] = a[j++];
+        else tmp[k++] = a[i++];
+    }
+    while (i < h) tmp[k++] = a[i++];
+    while (j < n) tmp[k++] = a[j++];
+    memcpy(a, tmp, n * sizeof(wpair));
+}
+
+void orc_sort_doc(uint32_t* words, size_t n, uint32_t* w_order)
+{
+    wpair* pv = (wpair*)malloc((n + 1) * sizeof(wpair));
+    wpair* tmp = (wpair*)malloc((n + 1) * sizeof(wpair));
+    for (size_t i = 0; i < n; ++i) { pv[i].w = words[i]; pv[i].i = (uint32_t)i; }
+    wpair_msort(pv, tmp, n);
+    for (size_t i = 0; i < n; ++i) {
+        words[i] = pv[i].w;
+        w_order[pv[i].i] = (uint32_t)i;
+    }
+    free(pv); free(tmp);
+}
+
+void orc_init_z(uint64_t N, const uint32_t* words, uint32_t V, uint32_t K,
+                const float* alpha, uint64_t seed, uint16_t* z)
+{
+    float* cum = (float*)malloc(K * sizeof(float));
+    float s = 0.f;
+    for (uint32_t k = 0; k < K; ++k) { s = s + alpha[k]; cum[k] = s; }
+    for (uint64_t i = 0; i < N; ++i) {
+        if (words[i] >= V) { z[i] = 0xFFFF; continue; }
+        float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_INIT, 0, seed));
+        z[i] = (uint16_t)orc_sample_acc(cum, K, u);
+    }
+    free(cum);
+}
+
+void orc_counts_from_z(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                       const uint16_t* z, uint32_t V, uint32_t K,
+                       int32_t* ndk, int32_t* nkw, int32_t* nk)
+{
+    memset(ndk, 0, D * K * sizeof(int32_t));
+    memset(nkw, 0, (size_t)V * K * sizeof(int32_t));
+    memset(nk, 0, K * sizeof(int32_t));
+    for (uint64_t d = 0; d < D; ++d) {
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t w = words[i];
+            if (w >= V) continue;
+            uint16_t k = z[i];
+            ndk[d * K + k]++;
+            nkw[(size_t)w * K + k]++;
+            nk[k]++;
+        }
+    }
+}
+
+uint64_t orc_word_major(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                        uint32_t V, uint64_t* w_off, uint32_t* tok_doc, uint64_t* tok_pos)
+{
+    memset(w_off, 0, (V + 1) * sizeof(uint64_t));
+    uint64_t N = doc_off[D];
+    for (uint64_t i = 0; i < N; ++i)
+        if (words[i] < V) w_off[words[i] + 1]++;
+    for (uint32_t v = 0; v < V; ++v) w_off[v + 1] += w_off[v];
+    uint64_t* cur = (uint64_t*)malloc((V + 1) * sizeof(uint64_t));
+    memcpy(cur, w_off, (V + 1) * sizeof(uint64_t));
+    for (uint64_t d = 0; d < D; ++d) {
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t w = words[i];
+            if (w >= V) continue;
+            uint64_t t = cur[w]++;
+            tok_doc[t] = (uint32_t)d;
+            if (tok_pos) tok_pos[t] = i;
+        }
+    }
+    free(cur);
+    return w_off[V];
+}
+
+/* ------------------------------------------------------------------------ */
+/* The device sampler's semantics                                           */
+/* ------------------------------------------------------------------------ */
+/* Segmented warp scan + strict search, the order the dense device kernel
+ * uses: c = ceil(K/32) topics per lane; lane l sums its segment
+ * sequentially; lane totals get a Hillis-Steele inclusive scan over 32
+ * lanes (offsets 1,2,4,8,16); lane l's exclusive offset is lane l-1's
+ * inclusive value; cum[j] = excl[lane(j)] + loc[j]; r = u * incl[31];
+ * result = first j with r < cum[j], else K-1. */
+static uint32_t seg_scan_draw(const float* w, uint32_t K, float u, float* loc)
+{
+    uint32_t c = (K + 31) / 32;
+    float T[32], x[32], y[32], excl[32];
+    for (uint32_t l = 0; l < 32; ++l) {
+        float s = 0.f;
+        uint32_t b = l * c, e = b + c < K ? b + c : K;
+        for (uint32_t j = b; j < e; ++j) { s = s + w[j]; loc[j] = s; }
+        T[l] = s;
+        x[l] = s;
+    }
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+        for (uint32_t l = 0; l < 32; ++l) y[l] = (l >= off) ? x[l] + x[l - off] : x[l];
+        memcpy(x, y, sizeof(x));
+    }
+    for (uint32_t l = 0; l < 32; ++l) excl[l] = l ? x[l - 1] : 0.f;
+    float total = x[31];
+    float r = u * total;
+    (void)T;
+    for (uint32_t j = 0; j < K; ++j) {
+        float cj = excl[j / c] + loc[j];
+        if (r < cj) return j;
+    }
+    return K - 1;
+}
+
+void orc_sweep_snapshot(uint32_t K, uint32_t V, const float* alpha, float eta,
+                        uint64_t seed, uint32_t iter,
+                        const uint64_t* w_off, const uint32_t* tok_doc,
+                        const int32_t* ndk, const int32_t* nkw, const int32_t* nk,
+                        const uint16_t* z_old, uint16_t* z_new)
+{
+    float veta = eta * (float)V;
+    float* R = (float*)malloc(K * sizeof(float));
+    float* w = (float*)malloc(K * sizeof(float));
+    float* loc = (float*)malloc(K * sizeof(float));
+    for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / ((float)nk[k] + veta);
+    for (uint32_t v = 0; v < V; ++v) {
+        const int32_t* col = nkw + (size_t)v * K;
+        for (uint64_t t = w_off[v]; t < w_off[v + 1]; ++t) {
+            uint32_t d = tok_doc[t];
+            uint16_t zo = z_old[t];
+            const int32_t* row = ndk + (size_t)d * K;
+            for (uint32_t k = 0; k < K; ++k) {
+                int own = (k == zo);
+                float a = (float)(row[k] - own) + alpha[k];
+                float b = (float)(col[k] - own) + eta;
+                float r = own ? 1.0f / ((float)(nk[k] - 1) + veta) : R[k];
+                w[k] = (a * b) * r;
+            }
+            float u = orc_u01(philox_first((uint32_t)t, (uint32_t)(t >> 32), ORC_STREAM_SWEEP, iter, seed));
+            z_new[t] = (uint16_t)seg_scan_draw(w, K, u, loc);
+        }
+    }
+    free(R); free(w); free(loc);
+}
+
+void orc_conditional_f64(uint32_t K, uint32_t V, const float* alpha, float eta,
+                         const int32_t* ndk_row, const int32_t* nkw_col, const int32_t* nk,
+                         uint16_t z_own, double* p)
+{
+    double veta = (double)eta * (double)V, s = 0;
+    for (uint32_t k = 0; k < K; ++k) {
+        int own = (k == z_own);
+        p[k] = ((double)(ndk_row[k] - own) + alpha[k]) * ((double)(nkw_col[k] - own) + eta)
+             / ((double)(nk[k] - own) + veta);
+        s += p[k];
+    }
+    for (uint32_t k = 0; k < K; ++k) p[k] /= s;
+}
+
+void orc_apply_sweep(uint32_t K, uint32_t V, const uint64_t* w_off, const uint32_t* tok_doc,
+                     int32_t* ndk, int32_t* nkw, int32_t* nk,
+                     uint16_t* z_old, const uint16_t* z_new)
+{
+    for (uint32_t v = 0; v < V; ++v) {
+        for (uint64_t t = w_off[v]; t < w_off[v + 1]; ++t) {
+            uint16_t zo = z_old[t], zn = z_new[t];
+            if (zo == zn) continue;
+            uint32_t d = tok_doc[t];
+            ndk[(size_t)d * K + zo]--; ndk[(size_t)d * K + zn]++;
+            nkw[(size_t)v * K + zo]--; nkw[(size_t)v * K + zn]++;
+            nk[zo]--; nk[zn]++;
+            z_old[t] = zn;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* The reference's sequential sampler                                       */
+/* ------------------------------------------------------------------------ */
+static inline uint64_t splitmix64(uint64_t* s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static inline float sm_u01(uint64_t* s) { return (float)(splitmix64(s) >> 40) * (1.0f / 16777216.0f); }
+
+/* sampleDocument for tokens [b, e) of one doc (LDAModel.hpp:326-354) with
+ * getZLikelihoods (:273-285) and addWordTo (:287-299). */
+static void sample_doc_range(uint32_t K, uint32_t V, const float* alpha, float eta, float veta,
+                             const uint32_t* words, uint16_t* z, uint64_t b, uint64_t e,
+                             int32_t* ndk_row, int32_t* nkw, int32_t* nk, float* dist, uint64_t* rng)
+{
+    for (uint64_t i = b; i < e; ++i) {
+        uint32_t v = words[i];
+        if (v >= V) continue;
+        uint16_t k0 = z[i];
+        int32_t* col = nkw + (size_t)v * K;
+        ndk_row[k0]--; nk[k0]--; col[k0]--;
+        for (uint32_t k = 0; k < K; ++k)
+            dist[k] = ((float)ndk_row[k] + alpha[k]) * ((float)col[k] + eta) / ((float)nk[k] + veta);
+        orc_prefix_sum_sse(dist, (int)K);
+        uint16_t k1 = (uint16_t)orc_sample_acc(dist, K, sm_u01(rng));
+        z[i] = k1;
+        ndk_row[k1]++; nk[k1]++; col[k1]++;
+    }
+}
+
+void orc_gibbs_none(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                    uint32_t V, uint32_t K, const float* alpha, float eta,
+                    uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk,
+                    uint64_t* rng_state)
+{
+    float veta = eta * (float)V;
+    float* dist = (float*)malloc(K * sizeof(float));
+    uint64_t* order = (uint64_t*)malloc((D + 1) * sizeof(uint64_t));
+    orc_shuffled_order(D, (size_t)(splitmix64(rng_state) & 0xFFFFFFFFu), order);
+    for (uint64_t j = 0; j < D; ++j) {
+        uint64_t d = order[j];
+        sample_doc_range(K, V, alpha, eta, veta, words, z, doc_off[d], doc_off[d + 1],
+                         ndk + d * K, nkw, nk, dist, rng_state);
+    }
+    free(dist); free(order);
+}
+
+/* ------------------------------------------------------------------------ */
+/* PARTITION scheme on host threads (CPU baseline)                          */
+/* ------------------------------------------------------------------------ */
+struct orc_partition {
+    uint64_t D; const uint64_t* doc_off; const uint32_t* words;
+    uint32_t V, K, W; const float* alpha; float eta, veta;
+    uint16_t* z; int32_t* ndk; int32_t* nkw; int32_t* nk;
+    uint32_t* vchunk;      /* W chunk ends */
+    uint64_t* chunk_off;   /* (W+1) x D */
+    int32_t** local_nk;    /* W private n_k */
+    float** dist;
+    uint64_t* rng;         /* W splitmix states */
+    pthread_t* th;
+    void* args;
+    pthread_barrier_t bar;
+    uint32_t iters, stop;
+};
+
+typedef struct { orc_partition* p; uint32_t id; } part_arg;
+
+static void* partition_worker(void* a_)
+{
+    part_arg* a = (part_arg*)a_;
+    orc_partition* p = a->p;
+    uint32_t pid = a->id, W = p->W;
+    uint64_t* order = (uint64_t*)malloc((p->D / W + 2) * sizeof(uint64_t));
+    for (;;) {
+        pthread_barrier_wait(&p->bar);          /* start of a train() call */
+        if (p->stop) break;
+        for (uint32_t it = 0; it < p->iters; ++it) {
+            for (uint32_t i = 0; i < W; ++i) {
+                uint32_t didx = (i + pid) % W;
+                uint64_t n = (p->D + (W - 1) - didx) / W;
+                orc_shuffled_order(n, (size_t)(splitmix64(&p->rng[pid]) & 0xFFFFFFFFu), order);
+                for (uint64_t j = 0; j < n; ++j) {
+                    uint64_t d = order[j] * W + didx;
+                    uint64_t b = p->doc_off[d] + p->chunk_off[(uint64_t)pid * p->D + d];
+                    uint64_t e = p->doc_off[d] + p->chunk_off[(uint64_t)(pid + 1) * p->D + d];
+                    sample_doc_range(p->K, p->V, p->alpha, p->eta, p->veta, p->words, p->z, b, e,
+                                     p->ndk + d * p->K, p->nkw, p->local_nk[pid], p->dist[pid], &p->rng[pid]);
+                }
+                pthread_barrier_wait(&p->bar);  /* the round's join */
+            }
+            /* mergeState (rowsum) by worker 0, distributeMergedState by all */
+            if (pid == 0) {
+                memset(p->nk, 0, p->K * sizeof(int32_t));
+                for (uint32_t v = 0; v < p->V; ++v) {
+                    const int32_t* col = p->nkw + (size_t)v * p->K;
+                    for (uint32_t k = 0; k < p->K; ++k) p->nk[k] += col[k];
+                }
+            }
+            pthread_barrier_wait(&p->bar);
+            memcpy(p->local_nk[pid], p->nk, p->K * sizeof(int32_t));
+            pthread_barrier_wait(&p->bar);
+        }
+        pthread_barrier_wait(&p->bar);          /* end of the train() call */
+    }
+    free(order);
+    return NULL;
+}
+
+orc_partition* orc_partition_create(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                                    uint32_t V, uint32_t K, const float* alpha, float eta,
+                                    uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk,
+                                    const uint64_t* vocab_cf, uint32_t nthreads, uint64_t seed)
+{
+    orc_partition* p = (orc_partition*)calloc(1, sizeof(orc_partition));
+    uint32_t W = nthreads ? nthreads : 1;
+    uint32_t maxw = (V + 3) / 4;          /* estimateMaxThreads (LDAModel.hpp:494-497) */
+    if (maxw < 1) maxw = 1;
+    if (W > maxw) W = maxw;
+    p->D = D; p->doc_off = doc_off; p->words = words; p->V = V; p->K = K; p->W = W;
+    p->alpha = alpha; p->eta = eta; p->veta = eta * (float)V;
+    p->z = z; p->ndk = ndk; p->nkw = nkw; p->nk = nk;
+    /* updatePartition (LDAModel.hpp:437-472): chunk ends by cumulative cf */
+    p->vchunk = (uint32_t*)malloc(W * sizeof(uint32_t));
+    uint64_t tot = 0, cum = 0;
+    uint32_t nch = 0;
+    for (uint32_t v = 0; v < V; ++v) tot += vocab_cf[v];
+    for (uint32_t v = 0; v < V && nch < W; ++v) {
+        cum += vocab_cf[v];
+        if (cum * W >= tot * (nch + 1)) p->vchunk[nch++] = v + 1;
+    }
+    while (nch < W) p->vchunk[nch++] = V;
+    p->chunk_off = (uint64_t*)malloc((uint64_t)(W + 1) * D * sizeof(uint64_t));
+    for (uint64_t d = 0; d < D; ++d) {
+        uint64_t len = doc_off[d + 1] - doc_off[d];
+        const uint32_t* ws = words + doc_off[d];
+        p->chunk_off[d] = 0;
+        uint32_t g = 0;
+        for (uint64_t j = 0; j < len; ++j)
+            for (; g < W && ws[j] >= p->vchunk[g]; ++g) p->chunk_off[(uint64_t)(g + 1) * D + d] = j;
+        for (; g < W; ++g) p->chunk_off[(uint64_t)(g + 1) * D + d] = len;
+    }
+    p->local_nk = (int32_t**)malloc(W * sizeof(int32_t*));
+    p->dist = (float**)malloc(W * sizeof(float*));
+    p->rng = (uint64_t*)malloc(W * sizeof(uint64_t));
+    for (uint32_t i = 0; i < W; ++i) {
+        p->local_nk[i] = (int32_t*)malloc(K * sizeof(int32_t));
+        memcpy(p->local_nk[i], nk, K * sizeof(int32_t));
+        p->dist[i] = (float*)aligned_alloc(64, ((K + 15) / 16) * 64);
+        p->rng[i] = seed * 0x9E3779B97F4A7C15ull + i + 1;
+    }
+    pthread_barrier_init(&p->bar, NULL, W);
+    p->th = (pthread_t*)malloc(W * sizeof(pthread_t));
+    part_arg* args = (part_arg*)malloc(W * sizeof(part_arg));
+    for (uint32_t i = 1; i < W; ++i) {
+        args[i].p = p; args[i].id = i;
+        pthread_create(&p->th[i], NULL, partition_worker, &args[i]);
+    }
+    args[0].p = p; args[0].id = 0;   /* worker 0 is the calling thread */
+    p->args = args;
+    return p;
+}
+
+void orc_partition_train(orc_partition* p, uint32_t iters)
+{
+    p->iters = iters;
+    p->stop = 0;
+    /* worker 0 runs on the calling thread: one train() call = one pass of
+     * the worker loop body, bracketed by the start/end barriers. */
+    uint32_t W = p->W;
+    uint64_t* order = (uint64_t*)malloc((p->D / W + 2) * sizeof(uint64_t));
+    if (W > 1) pthread_barrier_wait(&p->bar);
+    for (uint32_t it = 0; it < iters; ++it) {
+        for (uint32_t i = 0; i < W; ++i) {
+            uint32_t didx = i % W;
+            uint64_t n = (p->D + (W - 1) - didx) / W;
+            orc_shuffled_order(n, (size_t)(splitmix64(&p->rng[0]) & 0xFFFFFFFFu), order);
+            for (uint64_t j = 0; j < n; ++j) {
+                uint64_t d = order[j] * W + didx;
+                uint64_t b = p->doc_off[d] + p->chunk_off[d];
+                uint64_t e = p->doc_off[d] + p->chunk_off[(uint64_t)1 * p->D + d];
+                sample_doc_range(p->K, p->V, p->alpha, p->eta, p->veta, p->words, p->z, b, e,
+                                 p->ndk + d * p->K, p->nkw, p->local_nk[0], p->dist[0], &p->rng[0]);
+            }
+            if (W > 1) pthread_barrier_wait(&p->bar);
+        }
+        memset(p->nk, 0, p->K * sizeof(int32_t));
+        for (uint32_t v = 0; v < p->V; ++v) {
+            const int32_t* col = p->nkw + (size_t)v * p->K;
+            for (uint32_t k = 0; k < p->K; ++k) p->nk[k] += col[k];
+        }
+        if (W > 1) pthread_barrier_wait(&p->bar);
+        memcpy(p->local_nk[0], p->nk, p->K * sizeof(int32_t));
+        if (W > 1) pthread_barrier_wait(&p->bar);
+    }
+    if (W > 1) pthread_barrier_wait(&p->bar);
+    free(order);
+}
+
+void orc_partition_destroy(orc_partition* p)
+{
+    if (!p) return;
+    if (p->W > 1) {
+        p->stop = 1;
+        pthread_barrier_wait(&p->bar);
+        for (uint32_t i = 1; i < p->W; ++i) pthread_join(p->th[i], NULL);
+    }
+    pthread_barrier_destroy(&p->bar);
+    for (uint32_t i = 0; i < p->W; ++i) { free(p->local_nk[i]); free(p->dist[i]); }
+    free(p->local_nk); free(p->dist); free(p->rng); free(p->vchunk); free(p->chunk_off);
+    free(p->th); free(p->args); free(p);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Log-likelihood                                                           */
+/* ------------------------------------------------------------------------ */
+static float alpha_sum_f(uint32_t K, const float* alpha)
+{
+    float s = 0.f;
+    for (uint32_t k = 0; k < K; ++k) s += alpha[k];
+    return s;
+}
+
+double orc_ll_docs_lut(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                       const float* alpha)
+{
+    double ll = 0;
+    float as = alpha_sum_f(K, alpha);
+    for (uint64_t d = 0; d < D; ++d) {
+        ll -= orc_lgammaT((float)doc_len[d] + as) - orc_lgammaT(as);
+        for (uint32_t k = 0; k < K; ++k)
+            ll += orc_lgammaT((float)ndk[d * K + k] + alpha[k]) - orc_lgammaT(alpha[k]);
+    }
+    return ll;
+}
+
+double orc_ll_rest_lut(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta)
+{
+    double ll = 0;
+    float lge = orc_lgammaT(eta);
+    float veta = (float)V * eta;
+    ll += orc_lgammaT(veta) * K;
+    for (uint32_t k = 0; k < K; ++k) {
+        ll -= orc_lgammaT((float)nk[k] + veta);
+        for (uint32_t v = 0; v < V; ++v) {
+            int32_t c = nkw[(size_t)v * K + k];
+            if (!c) continue;
+            ll += orc_lgammaT((float)c + eta) - lge;
+        }
+    }
+    return ll;
+}
+
+double orc_ll_docs_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                       const float* alpha)
+{
+    double ll = 0, as = 0;
+    for (uint32_t k = 0; k < K; ++k) as += (double)alpha[k];
+    double lgas = lgamma(as);
+    for (uint64_t d = 0; d < D; ++d) {
+        double s = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            int32_t c = ndk[d * K + k];
+            if (!c) continue;
+            s += lgamma((double)c + (double)alpha[k]) - lgamma((double)alpha[k]);
+        }
+        ll += s - (lgamma((double)doc_len[d] + as) - lgas);
+    }
+    return ll;
+}
+
+double orc_ll_rest_f64(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta)
+{
+    double ll = 0, e = (double)eta, veta = (double)V * (double)eta;
+    double lge = lgamma(e);
+    ll += lgamma(veta) * K;
+    for (uint32_t k = 0; k < K; ++k) ll -= lgamma((double)nk[k] + veta);
+    for (uint64_t i = 0; i < (uint64_t)V * K; ++i) {
+        if (!nkw[i]) continue;
+        ll += lgamma((double)nkw[i] + e) - lge;
+    }
+    return ll;
+}
+
+/* ------------------------------------------------------------------------ */
+/* optimizeParameters (LDAModel.hpp:221-265)                                */
+/* ------------------------------------------------------------------------ */
+void orc_optimize_alpha(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                        float* alpha)
+{
+    for (int it = 0; it < 10; ++it) {
+        float as = alpha_sum_f(K, alpha);
+        float dsum = orc_digammaT(as);
+        double denom = 0;
+        for (uint64_t d = 0; d < D; ++d)
+            denom += (double)(orc_digammaApprox((float)doc_len[d] + as) - dsum);
+        for (uint32_t k = 0; k < K; ++k) {
+            float dk = orc_digammaT(alpha[k]);
+            double nom = 0;
+            for (uint64_t d = 0; d < D; ++d)
+                nom += (double)(orc_digammaApprox((float)ndk[d * K + k] + alpha[k]) - dk);
+            float a = (float)nom / (float)denom * alpha[k];
+            alpha[k] = a > 1e-5f ? a : 1e-5f;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Per-document infer (LDAModel.hpp:920-953)                                */
+/* ------------------------------------------------------------------------ */
+double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
+                     const int32_t* nkw, const int32_t* nk,
+                     const uint32_t* words, uint32_t len, uint32_t iters,
+                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk)
+{
+    float veta = eta * (float)V;
+    /* own[k, j] = count of this doc's tokens of word words[j] at topic k,
+     * kept per run of equal words (the doc is vid-sorted). */
+    int32_t* own = (int32_t*)calloc((size_t)len * K + 1, sizeof(int32_t));
+    int32_t* dnk = (int32_t*)calloc(K, sizeof(int32_t));
+    uint32_t* run0 = (uint32_t*)malloc((len + 1) * sizeof(uint32_t));
+    float* w = (float*)malloc(K * sizeof(float));
+    float* loc = (float*)malloc(K * sizeof(float));
+    float acum[32768];
+    float s = 0.f;
+    for (uint32_t k = 0; k < K; ++k) { s = s + alpha[k]; acum[k] = s; }
+    memset(ndk, 0, K * sizeof(int32_t));
+    for (uint32_t j = 0; j < len; ++j)
+        run0[j] = (j && words[j] == words[j - 1]) ? run0[j - 1] : j;
+    /* initializeDocState<true>: z ~ Discrete(alpha), added to the private state */
+    for (uint32_t j = 0; j < len; ++j) {
+        if (words[j] >= V) { z[j] = 0xFFFF; continue; }
+        float u = orc_u01(philox_first(j, 0xFFFFFFFFu, (uint32_t)doc_key, (uint32_t)(doc_key >> 32),
+                                       seed ^ ORC_STREAM_INFER));
+        uint16_t k = (uint16_t)orc_sample_acc(acum, K, u);
+        z[j] = k;
+        ndk[k]++;
+        own[(size_t)run0[j] * K + k]++;
+    }
+    for (uint32_t it = 0; it < iters; ++it) {
+        for (uint32_t j = 0; j < len; ++j) {
+            uint32_t v = words[j];
+            if (v >= V) continue;
+            uint16_t k0 = z[j];
+            int32_t* o = own + (size_t)run0[j] * K;
+            const int32_t* g = nkw + (size_t)v * K;
+            ndk[k0]--; o[k0]--;
+            for (uint32_t k = 0; k < K; ++k) {
+                float a = (float)ndk[k] + alpha[k];
+                float b = (float)(g[k] + o[k]) + eta;
+                float c = (float)(nk[k] + ndk[k]) + veta;
+                w[k] = (a * b) / c;
+            }
+            float u = orc_u01(philox_first(j, it, (uint32_t)doc_key, (uint32_t)(doc_key >> 32),
+                                           seed ^ ORC_STREAM_INFER));
+            uint16_t k1 = (uint16_t)seg_scan_draw(w, K, u, loc);
+            z[j] = k1;
+            ndk[k1]++; o[k1]++;
+        }
+    }
+    /* ll = LLRest(tmp) - LLRest(global) + LLDocs(doc), FP64, only touched cells */
+    double e = (double)eta, vd = (double)V * (double)eta, ll = 0, as = 0;
+    for (uint32_t k = 0; k < K; ++k) as += (double)alpha[k];
+    for (uint32_t k = 0; k < K; ++k) {
+        if (!ndk[k]) continue;
+        ll += lgamma((double)nk[k] + vd) - lgamma((double)(nk[k] + ndk[k]) + vd);
+    }
+    for (uint32_t j = 0; j < len; ++j) {
+        if (words[j] >= V || run0[j] != j) continue;
+        const int32_t* o = own + (size_t)j * K;
+        const int32_t* g = nkw + (size_t)words[j] * K;
+        for (uint32_t k = 0; k < K; ++k) {
+            if (!o[k]) continue;
+            double after = lgamma((double)(g[k] + o[k]) + e) - lgamma(e);
+            double before = g[k] ? lgamma((double)g[k] + e) - lgamma(e) : 0.0;
+            ll += after - before;
+        }
+    }
+    uint32_t n = 0;
+    for (uint32_t j = 0; j < len; ++j) n += words[j] < V;
+    double ld = 0;
+    for (uint32_t k = 0; k < K; ++k)
+        if (ndk[k]) ld += lgamma((double)ndk[k] + alpha[k]) - lgamma((double)alpha[k]);
+    ld -= lgamma((double)n + as) - lgamma(as);
+    ll += ld;
+    free(own); free(dnk); free(run0); free(w); free(loc);
+    return ll;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Doc-major sweep: live n_dk, snapshot n_kw / n_k                          */
+/* ------------------------------------------------------------------------ */
+/* tomotopy's COPY_MERGE with one worker per document (LDAModel.hpp:401-423,
+ * 555-570): each document is sampled sequentially with its own n_dk live;
+ * n_kw and n_k are the start-of-sweep copy with the token's own assignment
+ * removed; every count delta lands in the next state after the sweep.
+ * Draw counter: (doc-major token index, iter).  Same segmented scan as the
+ * snapshot sweep. */
+void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
+                        uint64_t seed, uint32_t iter, uint64_t D, const uint64_t* doc_off,
+                        const uint32_t* words, int32_t* ndk,
+                        const int32_t* nkw, const int32_t* nk,
+                        int32_t* nkw_next, int32_t* nk_next, uint16_t* z)
+{
+    float veta = eta * (float)V;
+    float* R = (float*)malloc(K * sizeof(float));
+    float* w = (float*)malloc(K * sizeof(float));
+    float* loc = (float*)malloc(K * sizeof(float));
+    for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / ((float)nk[k] + veta);
+    for (uint64_t d = 0; d < D; ++d) {
+        int32_t* row = ndk + d * K;
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            uint16_t zo = z[i];
+            const int32_t* col = nkw + (size_t)v * K;
+            row[zo]--;
+            for (uint32_t k = 0; k < K; ++k) {
+                int own = (k == zo);
+                float a = (float)row[k] + alpha[k];
+                float b = (float)(col[k] - own) + eta;
+                float r = own ? 1.0f / ((float)(nk[k] - 1) + veta) : R[k];
+                w[k] = (a * b) * r;
+            }
+            float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, iter, seed));
+            uint16_t zn = (uint16_t)seg_scan_draw(w, K, u, loc);
+            row[zn]++;
+            z[i] = zn;
+            if (zn != zo) {
+                nkw_next[(size_t)v * K + zo]--; nkw_next[(size_t)v * K + zn]++;
+                nk_next[zo]--; nk_next[zn]++;
+            }
+        }
+    }
+    free(R); free(w); free(loc);
+}

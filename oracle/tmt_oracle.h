@@ -1,0 +1,168 @@
+/*
+ * tmt_oracle.h -- CPU oracle for the tomotopy LDA collapsed-Gibbs path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
+ * calls this code; only tests/, __graft_entry__.smoke() and the CPU-baseline
+ * arm of bench.py use it, and only as the checker (or as the timed CPU
+ * baseline).  The product path fails loudly when its CUDA library is missing.
+ *
+ * What it restates (reference paths are relative to the tomotopy source tree):
+ *   - the float lgamma / digamma lookup tables        src/Utils/math.h:119-153, src/Utils/LUT.hpp:11-70
+ *   - digammaApprox                                   src/Utils/math.h:170-176
+ *   - prefixSum (SSE order) / sampleFromDiscreteAcc   src/Utils/sample.hpp:62-86, 133-189
+ *   - forShuffled doc order                           src/Utils/Utils.hpp:157-178
+ *   - removeStopwords vocab reorder                   src/TopicModel/TopicModel.hpp:526-571
+ *   - per-doc word sort (sortAndWriteOrder)           src/Utils/Utils.hpp:227-248, LDAModel.hpp:716-722
+ *   - sampleDocument / getZLikelihoods / addWordTo    src/TopicModel/LDAModel.hpp:273-354
+ *   - PARTITION scheme (vocab chunks, W rounds)       src/TopicModel/LDAModel.hpp:356-399, 436-489
+ *   - getLLDocs / getLLRest                           src/TopicModel/LDAModel.hpp:616-668
+ *   - optimizeParameters / calcDigammaSum             src/TopicModel/LDAModel.hpp:221-265
+ *   - per-document infer (together=False)             src/TopicModel/LDAModel.hpp:920-953
+ *
+ * Parity status: the numeric primitives (LUTs, digammaApprox, prefixSum,
+ * sampleFromDiscreteAcc, forShuffled, sortAndWriteOrder) are pinned bit-exactly
+ * against the reference's own sources compiled from the tomotopy tree into
+ * oracle/_ref (see oracle/Makefile and tests/test_oracle_ref.py).  The full
+ * sampler is NOT pinned against tomotopy itself: tomotopy's model code needs
+ * Eigen 3.4.0 and EigenRand 0.5.1, neither of which exists here, and its RNG
+ * (EigenRand P8_mt19937_64_32) is not restated.  Sampler parity is therefore
+ * statistical (ll_per_word) plus the exact invariants below.
+ *
+ * The "snapshot sweep" (orc_sweep_snapshot) defines the device sampler's
+ * semantics exactly: every token of a sweep reads the start-of-sweep counts
+ * with its own assignment removed, draws with a counter-based Philox4x32-10
+ * stream, and the count deltas are applied after the sweep.  Its float
+ * arithmetic and summation order are spelled out so that the device dense
+ * kernel can be checked bit-exactly against it.
+ */
+#ifndef TMT_ORACLE_H
+#define TMT_ORACLE_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ---------------- */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* upper 24 bits of x scaled into [0, 1) */
+float orc_u01(uint32_t x);
+
+/* Philox stream tags (third counter word) */
+#define ORC_STREAM_INIT  0x494E4954u /* 'INIT' */
+#define ORC_STREAM_SWEEP 0x53574550u /* 'SWEP' */
+#define ORC_STREAM_INFER 0x494E4652u /* 'INFR' */
+
+/* ---- special functions (reference float LUTs) -------------------------- */
+float orc_lgammaT(float x);
+float orc_digammaT(float x);
+float orc_digammaf(float x);
+float orc_digammaApprox(float x);
+
+/* ---- sampling primitives ----------------------------------------------- */
+void   orc_prefix_sum_sse(float* arr, int n);
+size_t orc_sample_acc(const float* cum, size_t K, float u01);
+/* forShuffled: writes the visiting order of N items for `seed` */
+void   orc_shuffled_order(size_t N, size_t seed, uint64_t* out);
+
+/* ---- corpus preparation ------------------------------------------------ */
+/* removeStopwords: sorts (cf, df) pairs descending with the min_cf/min_df
+ * rule and the rm_top rotation.  order[old_id] = new_id.  Returns realV. */
+uint64_t orc_remove_stopwords(uint64_t nv, uint64_t* cf, uint64_t* df,
+                              uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
+                              uint32_t* order);
+/* sortAndWriteOrder on one doc: stable sort of words, w_order[old] = new */
+void orc_sort_doc(uint32_t* words, size_t n, uint32_t* w_order);
+
+/* z0 ~ Discrete(alpha) per doc-major token i (Philox stream INIT); tokens
+ * with word >= V get 0xFFFF (tomotopy's non_topic_id). */
+void orc_init_z(uint64_t N, const uint32_t* words, uint32_t V, uint32_t K,
+                const float* alpha, uint64_t seed, uint16_t* z);
+
+/* counts from assignments (doc-major CSR) */
+void orc_counts_from_z(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                       const uint16_t* z, uint32_t V, uint32_t K,
+                       int32_t* ndk /*D*K*/, int32_t* nkw /*V*K: column v is K ints*/,
+                       int32_t* nk /*K*/);
+
+/* word-major layout: stable counting sort of the doc-major tokens by word.
+ * w_off[V+1]; tok_doc[Nv]; tok_pos[Nv] = doc-major position. Returns Nv. */
+uint64_t orc_word_major(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                        uint32_t V, uint64_t* w_off, uint32_t* tok_doc, uint64_t* tok_pos);
+
+/* ---- the device sampler's semantics (snapshot sweep) ------------------- */
+/* z_old/z_new are word-major.  `iter` is the global step.  Reads only the
+ * start-of-sweep counts; does not modify them. */
+void orc_sweep_snapshot(uint32_t K, uint32_t V, const float* alpha, float eta,
+                        uint64_t seed, uint32_t iter,
+                        const uint64_t* w_off, const uint32_t* tok_doc,
+                        const int32_t* ndk, const int32_t* nkw, const int32_t* nk,
+                        const uint16_t* z_old, uint16_t* z_new);
+/* the conditional of one token as FP64 probabilities (normalised), own
+ * assignment removed.  For the 1e-5 relative check. */
+void orc_conditional_f64(uint32_t K, uint32_t V, const float* alpha, float eta,
+                         const int32_t* ndk_row, const int32_t* nkw_col, const int32_t* nk,
+                         uint16_t z_own, double* p);
+/* apply the deltas of a sweep (word-major z) to the counts, then z_old = z_new */
+void orc_apply_sweep(uint32_t K, uint32_t V, const uint64_t* w_off, const uint32_t* tok_doc,
+                     int32_t* ndk, int32_t* nkw, int32_t* nk,
+                     uint16_t* z_old, const uint16_t* z_new);
+
+/* doc-major sweep: live n_dk; n_kw / n_k read from the start-of-sweep
+ * snapshot (own assignment removed) and deltas written to *_next, which the
+ * caller initialises as copies of the snapshot.  z is doc-major. */
+void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
+                        uint64_t seed, uint32_t iter, uint64_t D, const uint64_t* doc_off,
+                        const uint32_t* words, int32_t* ndk,
+                        const int32_t* nkw, const int32_t* nk,
+                        int32_t* nkw_next, int32_t* nk_next, uint16_t* z);
+
+/* ---- the reference's sequential sampler (ParallelScheme::NONE) ---------- */
+/* Doc-major; live counts; forShuffled doc order; SSE prefix sum; strict
+ * search.  rng_state is a splitmix64 state (tomotopy's EigenRand stream is
+ * not restated). */
+void orc_gibbs_none(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                    uint32_t V, uint32_t K, const float* alpha, float eta,
+                    uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk,
+                    uint64_t* rng_state);
+
+/* ---- the reference's PARTITION scheme on nthreads host threads ---------- */
+/* vocab chunks by cumulative cf; W rounds per sweep; shared nkw (disjoint
+ * columns), private nk copies merged by rowsum.  This is the CPU baseline. */
+typedef struct orc_partition orc_partition;
+orc_partition* orc_partition_create(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                                    uint32_t V, uint32_t K, const float* alpha, float eta,
+                                    uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk,
+                                    const uint64_t* vocab_cf, uint32_t nthreads, uint64_t seed);
+void orc_partition_train(orc_partition* p, uint32_t iters);
+void orc_partition_destroy(orc_partition* p);
+
+/* ---- log-likelihood ---------------------------------------------------- */
+/* reference style: float LUT lgamma, double accumulation (LDAModel.hpp:616-668) */
+double orc_ll_docs_lut(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                       const float* alpha);
+double orc_ll_rest_lut(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta);
+/* FP64: lgamma() in double, same terms */
+double orc_ll_docs_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                       const float* alpha);
+double orc_ll_rest_f64(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta);
+
+/* ---- alpha optimisation (Minka fixed point, 10 inner iterations) -------- */
+void orc_optimize_alpha(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                        float* alpha);
+
+/* ---- per-document infer (together=False) -------------------------------- */
+/* Runs `iters` sequential Gibbs sweeps over one (prepared, vid-sorted) doc on
+ * a private copy of the frozen model, as LDAModel::_infer does.  Draws come
+ * from Philox stream INFER keyed by (seed, doc_key).  Writes the doc's topic
+ * counts and returns ll = LLRest(tmp) - LLRest(global) + LLDocs(doc) in FP64. */
+double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
+                     const int32_t* nkw, const int32_t* nk,
+                     const uint32_t* words, uint32_t len, uint32_t iters,
+                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

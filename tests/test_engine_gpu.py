@@ -1,0 +1,249 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Gates:
+  (a) n_dk, n_kw, n_k recomputed from z equal the device counts after every sweep;
+  (b) the same seed gives bit-identical z;
+  (c) the device draws are exactly the oracle's (same float arithmetic and
+      scan order), the float conditional is within 1e-5 relative of FP64,
+      and a chi-square test on many i.i.d. draws accepts the FP64 conditional;
+  (d) ll_per_word within 1% of the reference's sequential sampler at the same
+      iteration count, averaged over seeds.
+"""
+import numpy as np
+import pytest
+from scipy import stats
+
+import oracle as O
+import tomotopy_b200 as T
+from tomotopy_b200._lib import TmtError
+
+pytestmark = pytest.mark.gpu
+
+
+def corpus(V=800, Tt=8, D=120, mean=60, seed=1, min_cf=0, rm_top=0, lognormal=False):
+    if lognormal:
+        off, w = T.synth_corpus(V, Tt, D, ("lognormal", np.log(mean), 1.0, 1, 20 * mean), seed=seed)
+    else:
+        off, w = T.synth_corpus(V, Tt, D, ("poisson", mean, 1, 10 * mean), seed=seed)
+    off, w, rv, _ = T.prepare_ids(off, w, min_cf=min_cf, rm_top=rm_top)
+    return off, w, rv
+
+
+def oracle_state(off, w, V, K, alpha, eta, seed, z0=None):
+    c = O.Corpus(off, w, V)
+    return O.State(c, K, alpha, eta, seed, z0=z0)
+
+
+def assert_same_state(eng, st):
+    z, nkw, nk, _ = eng.state()
+    np.testing.assert_array_equal(z, st.z)
+    np.testing.assert_array_equal(nk, st.nk)
+    np.testing.assert_array_equal(nkw, st.nkw)
+    np.testing.assert_array_equal(eng.doc_topic(), st.ndk)
+
+
+@pytest.mark.parametrize("K", [1, 7, 20, 100, 1000, 1100])
+def test_init_and_counts_bitexact(K):
+    off, w, V = corpus(min_cf=2)
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=42, optim_interval=0)
+    eng.upload(off, w)
+    st = oracle_state(off, w, V, K, 0.1, 0.01, 42)
+    assert_same_state(eng, st)
+    assert eng.info().N == st.c.N
+
+
+@pytest.mark.parametrize("K", [1, 5, 20, 33, 100, 250, 1000, 1100])
+def test_sweeps_bitexact(K):
+    """Every sweep's z and counts equal the oracle's doc-major sweep exactly."""
+    off, w, V = corpus(V=600, D=90, mean=50, seed=K, min_cf=2, rm_top=3)
+    alpha = np.float32(0.1) if K != 20 else (0.05 * (np.arange(K) + 1)).astype(np.float32)
+    eng = T.Engine(K, V, alpha=alpha, eta=0.01, seed=7, optim_interval=0)
+    eng.upload(off, w)
+    st = oracle_state(off, w, V, K, alpha, 0.01, 7)
+    step = 0
+    for n in (1, 2):
+        eng.train(n)
+        st.doc_live_sweeps(n, start_step=step)
+        step += n
+        assert_same_state(eng, st)
+
+
+def test_counts_invariant_after_every_sweep():
+    off, w, V = corpus(V=1500, D=300, mean=80, seed=3, lognormal=True)
+    K = 50
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=5, optim_interval=10)
+    eng.upload(off, w)
+    c = O.Corpus(off, w, V)
+    for _ in range(12):
+        eng.train(1)
+        z, nkw, nk, alpha = eng.state()
+        st = O.State(c, K, alpha, 0.01, 0, z0=z)   # recount from z
+        np.testing.assert_array_equal(nkw, st.nkw)
+        np.testing.assert_array_equal(nk, st.nk)
+        np.testing.assert_array_equal(eng.doc_topic(), st.ndk)
+        assert nk.sum() == c.N
+
+
+def test_seed_determinism():
+    off, w, V = corpus(V=1000, D=200, mean=70, seed=4)
+    zs = []
+    for seed in (11, 11, 12):
+        eng = T.Engine(64, V, alpha=0.1, eta=0.01, seed=seed)
+        eng.upload(off, w)
+        eng.train(15)
+        zs.append(eng.state()[0])
+    np.testing.assert_array_equal(zs[0], zs[1])
+    assert not np.array_equal(zs[0], zs[2])
+
+
+@pytest.mark.parametrize("K", [20, 300])
+def test_ll_fp64_matches_oracle(K):
+    off, w, V = corpus(V=900, D=150, mean=70, seed=9, min_cf=2)
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
+    eng.upload(off, w)
+    eng.train(3)
+    st = oracle_state(off, w, V, K, 0.1, 0.01, 3)
+    st.doc_live_sweeps(3)
+    ld, lr = eng.ll()
+    od, orr = st.ll_f64()
+    assert ld == pytest.approx(od, rel=1e-11, abs=1e-7)
+    assert lr == pytest.approx(orr, rel=1e-11, abs=1e-7)
+    # the reference's float-LUT likelihood agrees to LUT accuracy
+    lut = sum(st.ll_lut())
+    assert (ld + lr) == pytest.approx(lut, rel=2e-5)
+
+
+@pytest.mark.parametrize("asym", [False, True])
+def test_alpha_optimisation_matches_oracle(asym):
+    off, w, V = corpus(V=700, D=250, mean=60, seed=21)
+    K = 16
+    alpha = (0.02 * (np.arange(K) + 1)).astype(np.float32) if asym else np.float32(0.1)
+    eng = T.Engine(K, V, alpha=alpha, eta=0.01, seed=8, optim_interval=1)
+    eng.upload(off, w)
+    st = oracle_state(off, w, V, K, alpha, 0.01, 8)
+    for step in range(3):
+        eng.train(1)
+        st.doc_live_sweeps(1, start_step=step)
+        st.optimize_alpha()
+        _, _, _, a_dev = eng.state()
+        np.testing.assert_allclose(a_dev, st.alpha, rtol=2e-4)
+        # keep the oracle on the device's alpha so later sweeps stay comparable
+        st.alpha[:] = a_dev
+        z = eng.state()[0]
+        if not np.array_equal(z, st.z):
+            break
+
+
+def test_conditional_fp32_vs_fp64():
+    """The float conditional the sampler uses is within 1e-5 relative of FP64."""
+    off, w, V = corpus(V=500, D=60, mean=80, seed=2)
+    K = 100
+    st = oracle_state(off, w, V, K, 0.1, 0.01, 1)
+    rng = np.random.default_rng(0)
+    veta = np.float32(0.01) * np.float32(V)
+    for _ in range(200):
+        d = int(rng.integers(0, st.c.D))
+        b, e = int(st.c.doc_off[d]), int(st.c.doc_off[d + 1])
+        if e == b:
+            continue
+        i = int(rng.integers(b, e))
+        v, zo = int(st.c.words[i]), int(st.z[i])
+        row = st.ndk[d].copy()
+        row[zo] -= 1
+        p64 = np.zeros(K)
+        O.lib.orc_conditional_f64(K, V, O._ptr(st.alpha), 0.01, O._ptr(np.ascontiguousarray(st.ndk[d])),
+                                  O._ptr(np.ascontiguousarray(st.nkw[v])), O._ptr(st.nk), zo, O._ptr(p64))
+        own = (np.arange(K) == zo).astype(np.int32)
+        a32 = row.astype(np.float32) + st.alpha
+        b32 = (st.nkw[v] - own).astype(np.float32) + np.float32(0.01)
+        r32 = np.float32(1.0) / ((st.nk - own).astype(np.float32) + veta)
+        w32 = (a32 * b32) * r32
+        p32 = w32.astype(np.float64) / w32.astype(np.float64).sum()
+        np.testing.assert_allclose(p32, p64, rtol=1e-5, atol=1e-12)
+
+
+def test_chi_square_on_draws():
+    """Identical documents with identical z0 give every first token the same
+    start-of-sweep conditional; the device's draws across documents must fit
+    the FP64 oracle's distribution."""
+    rng = np.random.default_rng(1)
+    K, V, D, L = 24, 300, 40000, 12
+    doc = np.sort(rng.integers(0, V, L)).astype(np.uint32)
+    z_doc = rng.integers(0, K, L).astype(np.uint16)
+    off = np.arange(D + 1, dtype=np.uint64) * L
+    words = np.tile(doc, D)
+    z0 = np.tile(z_doc, D)
+    eng = T.Engine(K, V, alpha=0.3, eta=0.05, seed=99, optim_interval=0)
+    eng.upload(off, words, z0=z0)
+    st = oracle_state(off, words, V, K, 0.3, 0.05, 99, z0=z0)
+    p64 = np.zeros(K)
+    v0, zo = int(doc[0]), int(z_doc[0])
+    O.lib.orc_conditional_f64(K, V, O._ptr(st.alpha), 0.05, O._ptr(np.ascontiguousarray(st.ndk[0])),
+                              O._ptr(np.ascontiguousarray(st.nkw[v0])), O._ptr(st.nk), zo, O._ptr(p64))
+    eng.train(1)
+    z = eng.state()[0]
+    first = z[off[:-1].astype(np.int64)]
+    obs = np.bincount(first, minlength=K).astype(np.float64)
+    exp = p64 * D
+    keep = exp >= 5
+    obs_m = np.append(obs[keep], obs[~keep].sum())
+    exp_m = np.append(exp[keep], exp[~keep].sum())
+    if exp_m[-1] == 0:
+        obs_m, exp_m = obs_m[:-1], exp_m[:-1]
+    chi2, p = stats.chisquare(obs_m, exp_m)
+    assert p > 1e-4, (chi2, p)
+
+
+@pytest.mark.parametrize("K", [10, 40])
+def test_ll_per_word_matches_sequential_sampler(K):
+    """(d) at the same iteration count, the device's ll_per_word is within 1%
+    of the reference's sequential sampler (ParallelScheme::NONE restated),
+    averaged over 3 seeds."""
+    off, w, V = corpus(V=2000, Tt=10, D=300, mean=200, seed=31)
+    iters = 150
+    gpu, seq = [], []
+    for seed in (1, 2, 3):
+        eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
+        eng.upload(off, w)
+        eng.train(iters)
+        gpu.append(eng.ll_per_word())
+        st = oracle_state(off, w, V, K, 0.1, 0.01, seed)
+        st.gibbs_none(iters, 1000 + seed)
+        seq.append(st.ll_per_word())
+    g, s = np.mean(gpu), np.mean(seq)
+    assert abs(g - s) / abs(s) < 0.01, (gpu, seq)
+
+
+def test_edge_cases():
+    # empty corpus, empty docs, docs whose words are all removed
+    eng = T.Engine(5, 10, alpha=0.1, eta=0.01, seed=1)
+    eng.upload(np.zeros(1, np.uint64), np.zeros(0, np.uint32))
+    eng.train(3)
+    assert eng.info().global_step == 3
+    assert eng.ll() == (0.0, 0.0)
+    off = np.array([0, 0, 3, 3, 5, 6], dtype=np.uint64)
+    words = np.array([1, 1, 9, 11, 12, 2], dtype=np.uint32)     # V=10: 11, 12 are skipped
+    eng = T.Engine(3, 10, alpha=0.1, eta=0.01, seed=2, optim_interval=0)
+    eng.upload(off, words)
+    st = oracle_state(off, words, 10, 3, 0.1, 0.01, 2)
+    assert_same_state(eng, st)
+    eng.train(4)
+    st.doc_live_sweeps(4)
+    assert_same_state(eng, st)
+    z = eng.state()[0]
+    assert z[3] == 0xFFFF and z[4] == 0xFFFF
+    assert eng.info().N == 4
+
+
+def test_bad_inputs_raise():
+    eng = T.Engine(4, 10, alpha=0.1, eta=0.01, seed=1)
+    with pytest.raises(TmtError):
+        eng.train(1)                       # before upload: TMT_ERR_STATE
+    with pytest.raises(ValueError):
+        eng.upload(np.array([0, 2], np.uint64), np.array([1, 2], np.uint32), z0=np.array([0, 9], np.uint16))
+    with pytest.raises(ValueError):
+        eng.upload(np.array([0, 2, 1], np.uint64), np.array([1, 2], np.uint32))
+    small = T.Engine(4, 10, alpha=0.1, eta=0.01, seed=1, hbm_budget=1024)
+    with pytest.raises(TmtError) as e:
+        small.upload(np.array([0, 300], np.uint64), np.ones(300, np.uint32))
+    assert e.value.status == -3

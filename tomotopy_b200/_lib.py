@@ -1,0 +1,90 @@
+"""ctypes binding of libtomotopy_b200.so (the C ABI in include/tomotopy_b200.h).
+
+The library is the product path: if it is missing and cannot be built here,
+importing this module raises -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtomotopy_b200.so")
+
+TMT_OK = 0
+STATUS_NAMES = {
+    0: "TMT_OK", -1: "TMT_ERR_INVALID_ARGUMENT", -2: "TMT_ERR_CUDA", -3: "TMT_ERR_OUT_OF_MEMORY",
+    -4: "TMT_ERR_STATE", -5: "TMT_ERR_UNSUPPORTED", -6: "TMT_ERR_CANCELLED", -7: "TMT_ERR_TIMEOUT",
+    -8: "TMT_ERR_INTERNAL",
+}
+SAMPLER_AUTO, SAMPLER_DENSE, SAMPLER_SPARSE = 0, 1, 2
+LEN_POISSON, LEN_LOGNORMAL = 0, 1
+
+
+class TmtConfig(C.Structure):
+    _fields_ = [("K", C.c_uint32), ("V", C.c_uint32), ("alpha", C.POINTER(C.c_float)),
+                ("alpha_scalar", C.c_float), ("eta", C.c_float), ("seed", C.c_uint64),
+                ("optim_interval", C.c_uint32), ("burn_in", C.c_uint32), ("device", C.c_int32),
+                ("sampler", C.c_int32), ("hbm_budget", C.c_uint64)]
+
+
+class TmtInfo(C.Structure):
+    _fields_ = [("D", C.c_uint64), ("N_all", C.c_uint64), ("N", C.c_uint64), ("global_step", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("K", C.c_uint32), ("V", C.c_uint32), ("sampler", C.c_int32),
+                ("last_sweep_ms", C.c_float), ("kernel_launches", C.c_uint64),
+                ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32)]
+
+
+class TmtSynthSpec(C.Structure):
+    _fields_ = [("V", C.c_uint32), ("T", C.c_uint32), ("D", C.c_uint64), ("len_kind", C.c_int32),
+                ("len_a", C.c_double), ("len_b", C.c_double), ("len_min", C.c_uint32), ("len_max", C.c_uint32),
+                ("doc_alpha", C.c_double), ("topic_beta", C.c_double), ("zipf_s", C.c_double),
+                ("seed", C.c_uint64), ("threads", C.c_uint32)]
+
+
+_P = C.c_void_p
+_H = C.c_void_p
+SIGNATURES = {
+    "tmt_create": (C.c_int, [C.POINTER(TmtConfig), C.POINTER(_H)]),
+    "tmt_upload_corpus": (C.c_int, [_H, _P, _P, C.c_uint64, _P]),
+    "tmt_train": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P]),
+    "tmt_ll": (C.c_int, [_H, _P, _P]),
+    "tmt_download_state": (C.c_int, [_H, _P, _P, _P, _P]),
+    "tmt_download_doc_topic": (C.c_int, [_H, _P]),
+    "tmt_get_info": (C.c_int, [_H, C.POINTER(TmtInfo)]),
+    "tmt_last_error": (C.c_char_p, [_H]),
+    "tmt_destroy": (None, [_H]),
+    "tmt_prepare_corpus": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
+                                     _P, _P, _P, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_synth_corpus": (C.c_int, [C.POINTER(TmtSynthSpec), _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        try:
+            from . import build as _b
+            _b.build()
+        except Exception as e:  # no nvcc, no prebuilt library: fail loudly
+            raise ImportError(f"libtomotopy_b200.so is missing and could not be built: {e}") from e
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class TmtError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+
+
+def check(status, handle=None, what=""):
+    if status != TMT_OK:
+        msg = lib.tmt_last_error(handle).decode() if handle else what
+        if status == -1:
+            raise ValueError(msg)
+        raise TmtError(status, msg or what)

@@ -1,0 +1,1026 @@
+// engine.cu -- B200 collapsed-Gibbs LDA engine behind the C ABI in
+// include/tomotopy_b200.h.
+//
+// Sampler semantics (one sweep = tomotopy's trainOne, LDAModel.hpp:505-539):
+// tomotopy's COPY_MERGE scheme (LDAModel.hpp:401-423, 555-570) with one worker
+// per document.  A warp owns a document and samples its tokens in order, its
+// n_dk row live in shared memory, exactly as sampleDocument does
+// (LDAModel.hpp:326-354).  n_kw and n_k are read from the start-of-sweep copy
+// with the token's own assignment removed; count deltas go to the next copy
+// with integer atomics (the merge, :555-570).  Each draw is Philox4x32-10 of
+// (doc-major token index, global step), so z depends only on the seed and the
+// start-of-sweep state: results are bit-identical for any scheduling.
+//
+// Conditional per topic k (getZLikelihoods, LDAModel.hpp:273-285):
+//   w_k = ((float)n_dk[k] + alpha_k) * ((float)(n_kw[k,v] - own) + eta) * R_k
+//   R_k = 1 / ((float)n_k[k] + V*eta), own topic: 1 / ((float)(n_k[k]-1) + V*eta)
+// each operation rounded to nearest (no contraction).  The inclusive scan is
+// segmented: lane l owns topics [l*c, l*c+c), c = ceil(K/32), sums them in
+// order, then a Hillis-Steele scan over the 32 lane totals.  The draw is the
+// first k with u*total < cum[k], else K-1 (sampleFromDiscreteAcc,
+// sample.hpp:133-189).
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <numeric>
+#include <algorithm>
+#include <stdexcept>
+#include "philox.cuh"
+#include "special.cuh"
+#include "../../include/tomotopy_b200.h"
+
+namespace {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+constexpr int kSweepWarps = 8;           // warps per sweep block
+
+__device__ __forceinline__ int sk(int k) { return k + (k >> 5); }   // bank skew
+
+// ---------------------------------------------------------------------------
+// initialisation: z0 ~ Discrete(alpha) (initializeDocState, LDAModel.hpp:781-813)
+// ---------------------------------------------------------------------------
+__global__ void k_init_z(const uint32_t* __restrict__ words, uint64_t n_all, uint32_t V, uint32_t K,
+                         const float* __restrict__ acum, uint64_t seed, uint16_t* __restrict__ z)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_all;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (words[i] >= V) { z[i] = 0xFFFF; continue; }
+        float u = tmt::u01(tmt::philox_u32((uint32_t)i, (uint32_t)(i >> 32), tmt::kStreamInit, 0, seed));
+        float r = __fmul_rn(u, acum[K - 1]);
+        uint32_t lo = 0, hi = K - 1;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (r < acum[mid]) hi = mid; else lo = mid + 1;
+        }
+        z[i] = (uint16_t)lo;
+    }
+}
+
+// counts from assignments: warp per document (resetStatistics, LDAModel.hpp:301-316)
+__global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* __restrict__ words,
+                         const uint16_t* __restrict__ z, uint64_t D, uint32_t K, uint32_t V,
+                         int32_t* __restrict__ ndk, int32_t* __restrict__ nkw, int32_t* __restrict__ nk,
+                         int32_t* __restrict__ doc_len)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t d = warp; d < D; d += nwarps) {
+        int cnt = 0;
+        for (uint64_t i = doc_off[d] + lane; i < doc_off[d + 1]; i += 32) {
+            uint32_t w = words[i];
+            if (w >= V) continue;
+            uint32_t k = z[i];
+            atomicAdd(&ndk[d * K + k], 1);
+            atomicAdd(&nkw[(uint64_t)w * K + k], 1);
+            atomicAdd(&nk[k], 1);
+            ++cnt;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
+        if (lane == 0 && doc_len) doc_len[d] = cnt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the training sweep
+// ---------------------------------------------------------------------------
+struct SweepArgs {
+    const uint64_t* doc_off;
+    const uint32_t* words;
+    uint16_t* z;
+    int32_t* ndk;
+    const int32_t* nkw;
+    const int32_t* nk;
+    int32_t* nkw_next;
+    int32_t* nk_next;
+    const float* alpha;
+    const uint32_t* doc_order;
+    uint32_t* doc_counter;
+    uint64_t D;
+    uint32_t K, V, c;
+    float eta, veta;
+    uint64_t seed;
+    uint32_t iter;
+};
+
+// Segment loads of an int32 K-vector: lane owns [k0, k0 + c).
+template <int CMAX, bool VEC>
+__device__ __forceinline__ void load_segment(const int32_t* __restrict__ p, int k0, int c, int K, int (&out)[CMAX])
+{
+    if (VEC) {
+#pragma unroll
+        for (int j = 0; j < CMAX; j += 4) {
+            if (j < c && k0 + j < K) {
+                int4 q = __ldg(reinterpret_cast<const int4*>(p + k0 + j));
+                out[j] = q.x; out[j + 1] = q.y; out[j + 2] = q.z; out[j + 3] = q.w;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < CMAX; ++j)
+            if (j < c && k0 + j < K) out[j] = __ldg(p + k0 + j);
+    }
+}
+
+template <int CMAX, bool VEC>
+__global__ void __launch_bounds__(kSweepWarps * 32)
+k_sweep_doc(SweepArgs a)
+{
+    extern __shared__ int smem[];
+    const int K = (int)a.K;
+    const int KS = K + (K >> 5) + 1;
+    float* s_alpha = reinterpret_cast<float*>(smem);
+    float* s_R = s_alpha + KS;
+    int* s_dnk = reinterpret_cast<int*>(s_R + KS);
+    int* s_rows = s_dnk + K;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* row = s_rows + warp * KS;
+
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        s_alpha[sk(k)] = a.alpha[k];
+        s_R[sk(k)] = __fdiv_rn(1.0f, __fadd_rn((float)a.nk[k], a.veta));
+        s_dnk[k] = 0;
+    }
+    __syncthreads();
+
+    const int c = (int)a.c;
+    const int k0 = lane * c;
+    const float eta = a.eta, veta = a.veta;
+
+    for (;;) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
+        q = __shfl_sync(FULL, q, 0);
+        if (q >= a.D) break;
+        const uint64_t d = a.doc_order[q];
+        int32_t* grow = a.ndk + d * (uint64_t)K;
+        for (int k = lane; k < K; k += 32) row[sk(k)] = grow[k];
+        __syncwarp();
+        const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
+        for (uint64_t base = b; base < e; base += 32) {
+            const uint64_t my_i = base + lane;
+            uint32_t my_w = 0xFFFFFFFFu;
+            uint32_t my_z = 0xFFFF;
+            if (my_i < e) { my_w = a.words[my_i]; my_z = a.z[my_i]; }
+            uint32_t my_new = my_z;
+            const int nb = (int)min((uint64_t)32, e - base);
+            for (int j = 0; j < nb; ++j) {
+                const uint32_t v = __shfl_sync(FULL, my_w, j);
+                const int zo = (int)__shfl_sync(FULL, my_z, j);
+                if (v >= a.V) continue;
+                if (lane == 0) row[sk(zo)] -= 1;
+                __syncwarp();
+                const int32_t* col = a.nkw + (uint64_t)v * K;
+                int cv[CMAX];
+                load_segment<CMAX, VEC>(col, k0, c, K, cv);
+                float loc[CMAX];
+                float s = 0.f;
+#pragma unroll
+                for (int jj = 0; jj < CMAX; ++jj) {
+                    const int k = k0 + jj;
+                    if (jj < c && k < K) {
+                        const int own = (k == zo);
+                        const float A = __fadd_rn((float)row[sk(k)], s_alpha[sk(k)]);
+                        const float B = __fadd_rn((float)(cv[jj] - own), eta);
+                        const float R = own ? __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + k) - 1), veta))
+                                            : s_R[sk(k)];
+                        s = __fadd_rn(s, __fmul_rn(__fmul_rn(A, B), R));
+                    }
+                    loc[jj] = s;
+                }
+                float x = s;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const float y = __shfl_up_sync(FULL, x, off);
+                    if (lane >= off) x = __fadd_rn(x, y);
+                }
+                float excl = __shfl_up_sync(FULL, x, 1);
+                if (lane == 0) excl = 0.f;
+                const float total = __shfl_sync(FULL, x, 31);
+                const uint64_t ti = base + j;
+                const float u = tmt::u01(tmt::philox_u32((uint32_t)ti, (uint32_t)(ti >> 32), tmt::kStreamSweep,
+                                                         a.iter, a.seed));
+                const float r = __fmul_rn(u, total);
+                const bool has = (k0 < K) && (r < __fadd_rn(excl, s));
+                const unsigned m = __ballot_sync(FULL, has);
+                int zn = K - 1;
+                if (m) {
+                    const int hl = __ffs(m) - 1;
+                    int hit = 0;
+                    if (lane == hl) {
+                        hit = c - 1;
+#pragma unroll
+                        for (int jj = CMAX - 1; jj >= 0; --jj)
+                            if (jj < c && k0 + jj < K && r < __fadd_rn(excl, loc[jj])) hit = jj;
+                    }
+                    hit = __shfl_sync(FULL, hit, hl);
+                    zn = hl * c + hit;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    row[sk(zn)] += 1;
+                    if (zn != zo) {
+                        atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
+                        atomicAdd(&a.nkw_next[(uint64_t)v * K + zn], 1);
+                        atomicSub(&s_dnk[zo], 1);
+                        atomicAdd(&s_dnk[zn], 1);
+                    }
+                }
+                if (lane == j) my_new = (uint32_t)zn;
+            }
+            if (my_i < e && my_w < a.V) a.z[my_i] = (uint16_t)my_new;
+        }
+        __syncwarp();
+        for (int k = lane; k < K; k += 32) grow[k] = row[sk(k)];
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x)
+        if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
+}
+
+// K > 1024: two passes per token -- lane totals first, then the hit lane
+// recomputes its segment with identical arithmetic.  The doc row stays in
+// global memory (only its own warp touches it during the sweep).
+__global__ void __launch_bounds__(kSweepWarps * 32)
+k_sweep_doc_large(SweepArgs a)
+{
+    const int K = (int)a.K;
+    const int lane = threadIdx.x & 31;
+    const int c = (int)a.c;
+    const int k0 = lane * c;
+    const float eta = a.eta, veta = a.veta;
+    for (;;) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
+        q = __shfl_sync(FULL, q, 0);
+        if (q >= a.D) break;
+        const uint64_t d = a.doc_order[q];
+        int32_t* row = a.ndk + d * (uint64_t)K;
+        const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
+        for (uint64_t i = b; i < e; ++i) {
+            const uint32_t v = a.words[i];
+            if (v >= a.V) continue;
+            const int zo = a.z[i];
+            if (lane == 0) row[zo] -= 1;
+            __syncwarp();
+            __threadfence_block();
+            const int32_t* col = a.nkw + (uint64_t)v * K;
+            auto weight = [&](int k) -> float {
+                const int own = (k == zo);
+                const float A = __fadd_rn((float)row[k], a.alpha[k]);
+                const float B = __fadd_rn((float)(col[k] - own), eta);
+                const float R = __fdiv_rn(1.0f, __fadd_rn((float)(a.nk[k] - own), veta));
+                return __fmul_rn(__fmul_rn(A, B), R);
+            };
+            float s = 0.f;
+            for (int jj = 0; jj < c && k0 + jj < K; ++jj) s = __fadd_rn(s, weight(k0 + jj));
+            float x = s;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const float y = __shfl_up_sync(FULL, x, off);
+                if (lane >= off) x = __fadd_rn(x, y);
+            }
+            float excl = __shfl_up_sync(FULL, x, 1);
+            if (lane == 0) excl = 0.f;
+            const float total = __shfl_sync(FULL, x, 31);
+            const float u = tmt::u01(tmt::philox_u32((uint32_t)i, (uint32_t)(i >> 32), tmt::kStreamSweep,
+                                                     a.iter, a.seed));
+            const float r = __fmul_rn(u, total);
+            const bool has = (k0 < K) && (r < __fadd_rn(excl, s));
+            const unsigned m = __ballot_sync(FULL, has);
+            int zn = K - 1;
+            if (m) {
+                const int hl = __ffs(m) - 1;
+                int hit = 0;
+                if (lane == hl) {
+                    float t = 0.f;
+                    hit = c - 1;
+                    for (int jj = 0; jj < c && k0 + jj < K; ++jj) {
+                        t = __fadd_rn(t, weight(k0 + jj));
+                        if (r < __fadd_rn(excl, t)) { hit = jj; break; }
+                    }
+                }
+                hit = __shfl_sync(FULL, hit, hl);
+                zn = hl * c + hit;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                row[zn] += 1;
+                a.z[i] = (uint16_t)zn;
+                if (zn != zo) {
+                    atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
+                    atomicAdd(&a.nkw_next[(uint64_t)v * K + zn], 1);
+                    atomicSub(&a.nk_next[zo], 1);
+                    atomicAdd(&a.nk_next[zn], 1);
+                }
+            }
+            __syncwarp();
+            __threadfence_block();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// log-likelihood in FP64 (getLLDocs / getLLRest, LDAModel.hpp:616-668)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double x)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+    return x;
+}
+
+// Rows 0..D-1 are n_dk rows, rows D..D+V-1 are n_kw columns.  Static
+// warp-to-row assignment and fixed reduction trees: bit-reproducible.
+// lg_alpha[k] = lgamma(alpha_k); asum[0] = sum(alpha), asum[1] = lgamma(sum(alpha))
+__global__ void k_ll_prep(const float* __restrict__ alpha, uint32_t K, double* __restrict__ lg_alpha,
+                          double* __restrict__ asum)
+{
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) lg_alpha[k] = lgamma((double)alpha[k]);
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (uint32_t k = 0; k < K; ++k) s += (double)alpha[k];
+        asum[0] = s;
+        asum[1] = lgamma(s);
+    }
+}
+
+__global__ void k_ll_partials(const int32_t* __restrict__ ndk, uint64_t D, uint32_t K,
+                              const double* __restrict__ lg_alpha, const float* __restrict__ alpha,
+                              const int32_t* __restrict__ doc_len, const double* __restrict__ asum_p,
+                              const int32_t* __restrict__ nkw, uint32_t V, double eta, double lg_eta,
+                              double* __restrict__ partials)
+{
+    __shared__ double s_d[32], s_r[32];
+    const double asum = asum_p[0], lg_asum = asum_p[1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    double accd = 0, accr = 0;
+    for (uint64_t r = gw; r < D + V; r += nw) {
+        if (r < D) {
+            const int32_t* p = ndk + r * K;
+            for (uint32_t k = lane; k < K; k += 32) {
+                int32_t n = p[k];
+                if (n) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
+            }
+            if (lane == 0) accd -= lgamma((double)doc_len[r] + asum) - lg_asum;
+        } else {
+            const int32_t* p = nkw + (r - D) * K;
+            for (uint32_t k = lane; k < K; k += 32) {
+                int32_t n = p[k];
+                if (n) accr += lgamma((double)n + eta) - lg_eta;
+            }
+        }
+    }
+    accd = warp_sum(accd);
+    accr = warp_sum(accr);
+    if (lane == 0) { s_d[warp] = accd; s_r[warp] = accr; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nwb = blockDim.x >> 5;
+        double x = lane < nwb ? s_d[lane] : 0.0, y = lane < nwb ? s_r[lane] : 0.0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        if (lane == 0) { partials[2 * blockIdx.x] = x; partials[2 * blockIdx.x + 1] = y; }
+    }
+}
+
+__global__ void k_ll_final(const double* __restrict__ partials, uint32_t nparts,
+                           const int32_t* __restrict__ nk, uint32_t K, double veta, double* __restrict__ out)
+{
+    __shared__ double s_d[32], s_r[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double x = 0, y = 0;
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) { x += partials[2 * i]; y += partials[2 * i + 1]; }
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) y += lgamma(veta) - lgamma((double)nk[k] + veta);
+    x = warp_sum(x);
+    y = warp_sum(y);
+    if (lane == 0) { s_d[warp] = x; s_r[warp] = y; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nwb = blockDim.x >> 5;
+        x = lane < nwb ? s_d[lane] : 0.0;
+        y = lane < nwb ? s_r[lane] : 0.0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        if (lane == 0) { out[0] = x; out[1] = y; }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// alpha optimisation (optimizeParameters / calcDigammaSum, LDAModel.hpp:221-265)
+// ---------------------------------------------------------------------------
+// part_nom[bx*K + k] = sum over this block's docs of digammaApprox(n_dk + alpha_k)
+// part_den[bx]       = sum over this block's docs of digammaApprox(N_d + sum(alpha))
+__global__ void k_alpha_sums(const int32_t* __restrict__ ndk, uint64_t D, uint32_t K,
+                             const float* __restrict__ alpha, const int32_t* __restrict__ doc_len,
+                             const float* __restrict__ asum_p,
+                             double* __restrict__ part_nom, double* __restrict__ part_den)
+{
+    __shared__ double s_red[32];
+    const uint64_t per = (D + gridDim.x - 1) / gridDim.x;
+    const uint64_t d0 = blockIdx.x * per, d1 = min(D, d0 + per);
+    const uint32_t k = blockIdx.y * blockDim.x + threadIdx.x;
+    if (k < K) {
+        const float ak = alpha[k];
+        double acc = 0;
+        uint64_t zeros = 0;
+        for (uint64_t d = d0; d < d1; ++d) {
+            int32_t n = ndk[d * K + k];
+            if (n) acc += (double)tmt::digamma_approx_f(__fadd_rn((float)n, ak));
+            else ++zeros;
+        }
+        acc += (double)zeros * (double)tmt::digamma_approx_f(ak);
+        part_nom[(uint64_t)blockIdx.x * K + k] = acc;
+    }
+    if (blockIdx.y == 0) {
+        const float as = *asum_p;
+        double acc = 0;
+        for (uint64_t d = d0 + threadIdx.x; d < d1; d += blockDim.x)
+            acc += (double)tmt::digamma_approx_f(__fadd_rn((float)doc_len[d], as));
+        acc = warp_sum(acc);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) s_red[warp] = acc;
+        __syncthreads();
+        if (warp == 0) {
+            double x = lane < (int)(blockDim.x >> 5) ? s_red[lane] : 0.0;
+            x = warp_sum(x);
+            if (lane == 0) part_den[blockIdx.x] = x;
+        }
+    }
+}
+
+// One fixed-point step for every k, then the new sum(alpha) for the next step.
+__global__ void k_alpha_update(const double* __restrict__ part_nom, const double* __restrict__ part_den,
+                               uint32_t nparts, uint32_t K, uint64_t D, float* __restrict__ alpha,
+                               float* __restrict__ asum_p, const float* __restrict__ dg_points)
+{
+    __shared__ double s_den;
+    tmt::DigammaTable dg{ dg_points };
+    if (threadIdx.x == 0) {
+        double den = 0;
+        for (uint32_t i = 0; i < nparts; ++i) den += part_den[i];
+        s_den = den - (double)D * (double)dg(*asum_p);
+    }
+    __syncthreads();
+    const double den = s_den;
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+        double nom = 0;
+        for (uint32_t i = 0; i < nparts; ++i) nom += part_nom[(uint64_t)i * K + k];
+        const float ak = alpha[k];
+        nom -= (double)D * (double)dg(ak);
+        const float na = __fmul_rn(__fdiv_rn((float)nom, (float)den), ak);
+        alpha[k] = na > 1e-5f ? na : 1e-5f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (uint32_t k = 0; k < K; ++k) s = __fadd_rn(s, alpha[k]);
+        *asum_p = s;
+    }
+}
+
+__global__ void k_sum_alpha(const float* __restrict__ alpha, uint32_t K, float* __restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        float s = 0.f;
+        for (uint32_t k = 0; k < K; ++k) s = __fadd_rn(s, alpha[k]);
+        *out = s;
+    }
+}
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct OomError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// the handle
+// ---------------------------------------------------------------------------
+struct tmt_handle {
+    tmt_config cfg{};
+    std::vector<float> alpha;        // host copy (after optimisation when downloaded)
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // around the sweep kernel only
+    double sweep_kernel_ms = 0;                   // summed over the last train() call
+    uint32_t sweeps_timed = 0;
+    int num_sms = 0;
+    std::string err;
+
+    uint64_t D = 0, N_all = 0, N = 0, global_step = 0, bytes = 0, launches = 0;
+    int sampler_used = 0;
+    float last_ms = 0.f;
+    bool uploaded = false;
+
+    // device buffers
+    std::vector<void*> allocs;
+    uint64_t* d_doc_off = nullptr;
+    uint32_t* d_words = nullptr;
+    uint16_t* d_z = nullptr;
+    int32_t* d_ndk = nullptr;
+    int32_t* d_nkw[2] = { nullptr, nullptr };
+    int32_t* d_nk[2] = { nullptr, nullptr };
+    int cur = 0;
+    int32_t* d_doc_len = nullptr;
+    uint32_t* d_doc_order = nullptr;
+    uint32_t* d_counter = nullptr;
+    float* d_alpha = nullptr;
+    float* d_asum = nullptr;
+    double* d_lg_alpha = nullptr;
+    double* d_asum_ll = nullptr;     // sum(alpha), lgamma(sum(alpha)) in FP64
+    double* d_llv = nullptr;         // tmt_ll output (2)
+    double* d_partials = nullptr;
+    uint32_t n_partials = 0;
+    double* d_ll = nullptr;          // ll history for one train() call (2 per point)
+    uint32_t ll_cap = 0;
+    float* d_dg_points = nullptr;
+    double* d_part_nom = nullptr;
+    double* d_part_den = nullptr;
+    uint32_t n_apart = 0;
+
+    template <class T>
+    T* dalloc(size_t count)
+    {
+        size_t b = count * sizeof(T);
+        if (b == 0) b = 16;
+        if (cfg.hbm_budget && bytes + b > cfg.hbm_budget)
+            throw OomError("HBM budget exceeded: need " + std::to_string(bytes + b) + " bytes, budget " +
+                           std::to_string(cfg.hbm_budget));
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw OomError(std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        }
+        allocs.push_back(p);
+        bytes += b;
+        return static_cast<T*>(p);
+    }
+
+    void release()
+    {
+        if (device >= 0) cudaSetDevice(device);
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        bytes = 0;
+    }
+
+    ~tmt_handle()
+    {
+        release();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (kev0) cudaEventDestroy(kev0);
+        if (kev1) cudaEventDestroy(kev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+tmt_status fail(tmt_handle* h, tmt_status s, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+template <class F>
+tmt_status guarded(tmt_handle* h, F&& f)
+{
+    try {
+        if (h) {
+            h->err.clear();
+            CK(cudaSetDevice(h->device));
+        }
+        f();
+        return TMT_OK;
+    } catch (const ArgError& e) {
+        return fail(h, TMT_ERR_INVALID_ARGUMENT, e.what());
+    } catch (const OomError& e) {
+        return fail(h, TMT_ERR_OUT_OF_MEMORY, e.what());
+    } catch (const StateError& e) {
+        return fail(h, TMT_ERR_STATE, e.what());
+    } catch (const CudaError& e) {
+        return fail(h, TMT_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(h, TMT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(h, TMT_ERR_INTERNAL, e.what());
+    }
+}
+
+void launch_check(tmt_handle* h)
+{
+    ++h->launches;
+    CK(cudaGetLastError());
+}
+
+uint32_t sweep_smem_bytes(uint32_t K)
+{
+    uint32_t KS = K + (K >> 5) + 1;
+    return (2 * KS + K + kSweepWarps * KS) * 4;
+}
+
+template <int CMAX, bool VEC>
+void launch_sweep_t(tmt_handle* h, const SweepArgs& a, uint32_t smem)
+{
+    auto kern = k_sweep_doc<CMAX, VEC>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepWarps * 32, smem));
+    if (per_sm < 1) throw CudaError("sweep kernel does not fit on an SM");
+    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms,
+                                                 (h->D + kSweepWarps - 1) / kSweepWarps);
+    if (grid == 0) grid = 1;
+    kern<<<grid, kSweepWarps * 32, smem, h->stream>>>(a);
+    launch_check(h);
+}
+
+void launch_sweep(tmt_handle* h, const SweepArgs& a)
+{
+    const uint32_t K = a.K, c = a.c;
+    const uint32_t smem = sweep_smem_bytes(K);
+    const bool vec = (K % 4 == 0) && (c % 4 == 0);
+    if (c <= 1) launch_sweep_t<1, false>(h, a, smem);
+    else if (c <= 2) launch_sweep_t<2, false>(h, a, smem);
+    else if (c <= 4) { if (vec) launch_sweep_t<4, true>(h, a, smem); else launch_sweep_t<4, false>(h, a, smem); }
+    else if (c <= 8) { if (vec) launch_sweep_t<8, true>(h, a, smem); else launch_sweep_t<8, false>(h, a, smem); }
+    else if (c <= 16) { if (vec) launch_sweep_t<16, true>(h, a, smem); else launch_sweep_t<16, false>(h, a, smem); }
+    else if (c <= 32) { if (vec) launch_sweep_t<32, true>(h, a, smem); else launch_sweep_t<32, false>(h, a, smem); }
+    else {
+        uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 8,
+                                                     (h->D + kSweepWarps - 1) / kSweepWarps);
+        if (grid == 0) grid = 1;
+        k_sweep_doc_large<<<grid, kSweepWarps * 32, 0, h->stream>>>(a);
+        launch_check(h);
+    }
+}
+
+void do_sweep(tmt_handle* h)
+{
+    const int cur = h->cur, nxt = cur ^ 1;
+    const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
+    CK(cudaMemcpyAsync(h->d_nkw[nxt], h->d_nkw[cur], kv * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_nk[nxt], h->d_nk[cur], h->cfg.K * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+    SweepArgs a{};
+    a.doc_off = h->d_doc_off;
+    a.words = h->d_words;
+    a.z = h->d_z;
+    a.ndk = h->d_ndk;
+    a.nkw = h->d_nkw[cur];
+    a.nk = h->d_nk[cur];
+    a.nkw_next = h->d_nkw[nxt];
+    a.nk_next = h->d_nk[nxt];
+    a.alpha = h->d_alpha;
+    a.doc_order = h->d_doc_order;
+    a.doc_counter = h->d_counter;
+    a.D = h->D;
+    a.K = h->cfg.K;
+    a.V = h->cfg.V;
+    a.c = (h->cfg.K + 31) / 32;
+    a.eta = h->cfg.eta;
+    a.veta = h->cfg.eta * (float)h->cfg.V;
+    a.seed = h->cfg.seed;
+    a.iter = (uint32_t)h->global_step;
+    CK(cudaEventRecord(h->kev0, h->stream));
+    launch_sweep(h, a);
+    CK(cudaEventRecord(h->kev1, h->stream));
+    h->cur = nxt;
+    h->sampler_used = TMT_SAMPLER_DENSE;
+}
+
+void do_optimize(tmt_handle* h)
+{
+    const uint32_t K = h->cfg.K;
+    dim3 grid(h->n_apart, (K + 255) / 256);
+    k_sum_alpha<<<1, 32, 0, h->stream>>>(h->d_alpha, K, h->d_asum);
+    launch_check(h);
+    for (int it = 0; it < 10; ++it) {
+        k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_alpha, h->d_doc_len, h->d_asum,
+                                                  h->d_part_nom, h->d_part_den);
+        launch_check(h);
+        k_alpha_update<<<1, 1024, 0, h->stream>>>(h->d_part_nom, h->d_part_den, h->n_apart, K, h->D,
+                                                  h->d_alpha, h->d_asum, h->d_dg_points);
+        launch_check(h);
+    }
+}
+
+// FP64 ll into d_out[0..1]; alpha read from the device copy.
+// FP64 ll into d_out[0..1] (docs, rest); stream-ordered, no host sync.
+void do_ll(tmt_handle* h, double* d_out)
+{
+    const uint32_t K = h->cfg.K;
+    const double eta = (double)h->cfg.eta;
+    const double veta = (double)h->cfg.V * eta;
+    k_ll_prep<<<1, 256, 0, h->stream>>>(h->d_alpha, K, h->d_lg_alpha, h->d_asum_ll);
+    launch_check(h);
+    k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
+                                                        h->d_doc_len, h->d_asum_ll,
+                                                        h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
+                                                        h->d_partials);
+    launch_check(h);
+    k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out);
+    launch_check(h);
+}
+
+void validate_config(const tmt_config& c)
+{
+    if (c.K == 0 || c.K > 32767) throw ArgError("wrong K value (K = " + std::to_string(c.K) + ")");
+    if (!(c.eta > 0)) throw ArgError("wrong eta value (eta = " + std::to_string(c.eta) + ")");
+    if (c.alpha) {
+        for (uint32_t k = 0; k < c.K; ++k)
+            if (!(c.alpha[k] > 0)) throw ArgError("wrong alpha value");
+    } else if (!(c.alpha_scalar > 0)) {
+        throw ArgError("wrong alpha value");
+    }
+    if (c.sampler < TMT_SAMPLER_AUTO || c.sampler > TMT_SAMPLER_SPARSE) throw ArgError("unknown sampler");
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out)
+{
+    if (!cfg || !out) return TMT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    tmt_handle* h = nullptr;
+    try {
+        h = new tmt_handle();
+    } catch (...) {
+        return TMT_ERR_OUT_OF_MEMORY;
+    }
+    h->cfg = *cfg;
+    h->cfg.alpha = nullptr;
+    h->device = cfg->device;
+    try {
+        validate_config(*cfg);   // the ctor's argument checks, before any CUDA call
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        *out = h;
+        return TMT_ERR_INVALID_ARGUMENT;
+    }
+    tmt_status s = guarded(h, [&] {
+        h->alpha.assign(cfg->K, cfg->alpha_scalar);
+        if (cfg->alpha) std::copy(cfg->alpha, cfg->alpha + cfg->K, h->alpha.begin());
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&h->ev0));
+        CK(cudaEventCreate(&h->ev1));
+        CK(cudaEventCreate(&h->kev0));
+        CK(cudaEventCreate(&h->kev1));
+        CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    });
+    if (s != TMT_OK) {
+        // keep the handle so the caller can read the message
+        *out = h;
+        return s;
+    }
+    *out = h;
+    return TMT_OK;
+}
+
+tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                             const uint16_t* z0)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!doc_off) throw ArgError("doc_off is NULL");
+        if (D >= 0xFFFFFFFFull) throw ArgError("too many documents");
+        const uint64_t n_all = doc_off[D];
+        if (n_all && !wid) throw ArgError("wid is NULL");
+        for (uint64_t d = 0; d < D; ++d)
+            if (doc_off[d + 1] < doc_off[d]) throw ArgError("doc_off is not non-decreasing");
+        const uint32_t K = h->cfg.K, V = h->cfg.V;
+        if (z0) {
+            for (uint64_t i = 0; i < n_all; ++i)
+                if (wid[i] < V && z0[i] >= K) throw ArgError("z0 holds a topic id >= K");
+        }
+        h->release();
+        h->uploaded = false;
+        h->D = D;
+        h->N_all = n_all;
+        h->global_step = 0;
+        h->cur = 0;
+        // host-side facts: valid-token count per doc, doc order (longest first)
+        std::vector<int32_t> len(D);
+        uint64_t N = 0;
+        for (uint64_t d = 0; d < D; ++d) {
+            int32_t c = 0;
+            for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) c += wid[i] < V;
+            len[d] = c;
+            N += c;
+        }
+        h->N = N;
+        std::vector<uint32_t> order(D);
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            return doc_off[a + 1] - doc_off[a] > doc_off[b + 1] - doc_off[b];
+        });
+
+        h->d_doc_off = h->dalloc<uint64_t>(D + 1);
+        h->d_words = h->dalloc<uint32_t>(n_all);
+        h->d_z = h->dalloc<uint16_t>(n_all);
+        h->d_ndk = h->dalloc<int32_t>(D * (uint64_t)K);
+        h->d_nkw[0] = h->dalloc<int32_t>((uint64_t)K * V);
+        h->d_nkw[1] = h->dalloc<int32_t>((uint64_t)K * V);
+        h->d_nk[0] = h->dalloc<int32_t>(K);
+        h->d_nk[1] = h->dalloc<int32_t>(K);
+        h->d_doc_len = h->dalloc<int32_t>(D);
+        h->d_doc_order = h->dalloc<uint32_t>(D);
+        h->d_counter = h->dalloc<uint32_t>(1);
+        h->d_alpha = h->dalloc<float>(K);
+        h->d_asum = h->dalloc<float>(1);
+        h->d_lg_alpha = h->dalloc<double>(K);
+        h->d_asum_ll = h->dalloc<double>(2);
+        h->d_llv = h->dalloc<double>(2);
+        h->n_partials = (uint32_t)std::max(1, h->num_sms * 8);
+        h->d_partials = h->dalloc<double>(2 * (size_t)h->n_partials);
+        h->ll_cap = 0;
+        h->d_ll = nullptr;
+        std::vector<float> dg = tmt::build_digamma_points();
+        h->d_dg_points = h->dalloc<float>(dg.size());
+        h->n_apart = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 4, (D + 63) / 64));
+        h->d_part_nom = h->dalloc<double>((size_t)h->n_apart * K);
+        h->d_part_den = h->dalloc<double>(h->n_apart);
+
+        cudaStream_t st = h->stream;
+        CK(cudaMemcpyAsync(h->d_doc_off, doc_off, (D + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        if (n_all) CK(cudaMemcpyAsync(h->d_words, wid, n_all * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(h->d_doc_order, order.data(), D * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(h->d_alpha, h->alpha.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(h->d_dg_points, dg.data(), dg.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(h->d_ndk, 0, D * (uint64_t)K * sizeof(int32_t), st));
+        CK(cudaMemsetAsync(h->d_nkw[0], 0, (uint64_t)K * V * sizeof(int32_t), st));
+        CK(cudaMemsetAsync(h->d_nk[0], 0, K * sizeof(int32_t), st));
+        if (z0) {
+            if (n_all) CK(cudaMemcpyAsync(h->d_z, z0, n_all * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+        } else if (n_all) {
+            std::vector<float> acum(K);
+            float s = 0.f;
+            for (uint32_t k = 0; k < K; ++k) { s = s + h->alpha[k]; acum[k] = s; }
+            float* d_acum = h->dalloc<float>(K);
+            CK(cudaMemcpyAsync(d_acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
+            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (n_all + 255) / 256);
+            k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->d_z);
+            launch_check(h);
+        }
+        if (D) {
+            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D * 32 + 255) / 256);
+            k_counts<<<grid, 256, 0, st>>>(h->d_doc_off, h->d_words, h->d_z, D, K, V, h->d_ndk, h->d_nkw[0],
+                                           h->d_nk[0], h->d_doc_len);
+            launch_check(h);
+        }
+        CK(cudaStreamSynchronize(st));
+        h->uploaded = true;
+    });
+}
+
+tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* ll_out)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("train() before the corpus was uploaded");
+        if (h->D == 0 || h->N == 0) {
+            h->global_step += iters;
+            return;
+        }
+        const uint32_t npts = (ll_every && ll_out) ? iters / ll_every : 0;
+        if (npts > h->ll_cap) {
+            h->d_ll = h->dalloc<double>(2 * (size_t)npts);
+            h->ll_cap = npts;
+        }
+        uint32_t pt = 0;
+        h->sweep_kernel_ms = 0;
+        h->sweeps_timed = 0;
+        for (uint32_t i = 0; i < iters; ++i) {
+            CK(cudaEventRecord(h->ev0, h->stream));
+            do_sweep(h);
+            CK(cudaEventRecord(h->ev1, h->stream));
+            // the events of this sweep's kernel are complete before the next
+            // sweep records them again: read them now
+            {
+                CK(cudaEventSynchronize(h->kev1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, h->kev0, h->kev1));
+                h->sweep_kernel_ms += ms;
+                ++h->sweeps_timed;
+            }
+            const uint64_t gs = h->global_step;
+            if (gs >= h->cfg.burn_in && h->cfg.optim_interval && (gs + 1) % h->cfg.optim_interval == 0)
+                do_optimize(h);
+            ++h->global_step;
+            if (npts && (i + 1) % ll_every == 0 && pt < npts) do_ll(h, h->d_ll + 2 * pt++);
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+        if (npts) {
+            std::vector<double> tmp(2 * (size_t)npts);
+            CK(cudaMemcpy(tmp.data(), h->d_ll, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (uint32_t p = 0; p < npts; ++p) ll_out[p] = tmp[2 * p] + tmp[2 * p + 1];
+        }
+    });
+}
+
+tmt_status tmt_ll(tmt_handle* h, double* ll_docs, double* ll_rest)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("ll before the corpus was uploaded");
+        double out[2] = { 0, 0 };
+        if (h->D) {
+            do_ll(h, h->d_llv);
+            CK(cudaMemcpyAsync(out, h->d_llv, sizeof(out), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        if (ll_docs) *ll_docs = out[0];
+        if (ll_rest) *ll_rest = out[1];
+    });
+}
+
+tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t* n_k, float* alpha)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("no corpus uploaded");
+        const uint32_t K = h->cfg.K, V = h->cfg.V;
+        if (z && h->N_all) CK(cudaMemcpyAsync(z, h->d_z, h->N_all * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream));
+        if (n_kw) CK(cudaMemcpyAsync(n_kw, h->d_nkw[h->cur], (uint64_t)K * V * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        if (n_k) CK(cudaMemcpyAsync(n_k, h->d_nk[h->cur], K * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->alpha.data(), h->d_alpha, K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (alpha) std::copy(h->alpha.begin(), h->alpha.end(), alpha);
+    });
+}
+
+tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("no corpus uploaded");
+        if (!n_dk) throw ArgError("n_dk is NULL");
+        if (h->D)
+            CK(cudaMemcpyAsync(n_dk, h->d_ndk, h->D * (uint64_t)h->cfg.K * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
+{
+    if (!h || !out) return TMT_ERR_INVALID_ARGUMENT;
+    out->D = h->D;
+    out->N_all = h->N_all;
+    out->N = h->N;
+    out->global_step = h->global_step;
+    out->device_bytes = h->bytes;
+    out->K = h->cfg.K;
+    out->V = h->cfg.V;
+    out->sampler = h->sampler_used;
+    out->last_sweep_ms = h->last_ms;
+    out->kernel_launches = h->launches;
+    out->sweep_kernel_ms = h->sweep_kernel_ms;
+    out->sweeps_timed = h->sweeps_timed;
+    return TMT_OK;
+}
+
+const char* tmt_last_error(const tmt_handle* h)
+{
+    return h ? h->err.c_str() : "null handle";
+}
+
+void tmt_destroy(tmt_handle* h)
+{
+    delete h;
+}
+
+} // extern "C"

@@ -1,0 +1,121 @@
+"""Thin Python wrapper over the engine's C ABI (tmt_create / tmt_upload_corpus /
+tmt_train / tmt_ll / tmt_download_state ...).  Host buffers are numpy arrays;
+the handle owns the device buffers."""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import lib, check, TmtConfig, TmtInfo, TmtSynthSpec, SAMPLER_AUTO, LEN_POISSON, LEN_LOGNORMAL
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class Engine:
+    """One model state on one GPU (tmt_handle)."""
+
+    def __init__(self, K, V, alpha=0.1, eta=0.01, seed=0, optim_interval=10, burn_in=0, device=0,
+                 sampler=SAMPLER_AUTO, hbm_budget=0):
+        self.K, self.V = int(K), int(V)
+        a = np.broadcast_to(np.asarray(alpha, dtype=np.float32), (self.K,)).copy() \
+            if np.ndim(alpha) else None
+        self._alpha_buf = a
+        cfg = TmtConfig(K=self.K, V=self.V,
+                        alpha=a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None,
+                        alpha_scalar=float(alpha) if a is None else 0.0, eta=float(eta), seed=int(seed),
+                        optim_interval=int(optim_interval), burn_in=int(burn_in), device=int(device),
+                        sampler=int(sampler), hbm_budget=int(hbm_budget))
+        h = C.c_void_p()
+        st = lib.tmt_create(C.byref(cfg), C.byref(h))
+        self.h = h
+        if st != 0:
+            msg = lib.tmt_last_error(h).decode() if h.value else "tmt_create failed"
+            self.close()
+            check(st, None, msg)
+        self.D = 0
+        self.n_all = 0
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib.tmt_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def upload(self, doc_off, words, z0=None):
+        self._doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
+        self._words = np.ascontiguousarray(words, dtype=np.uint32)
+        zz = np.ascontiguousarray(z0, dtype=np.uint16) if z0 is not None else None
+        self.D = len(self._doc_off) - 1
+        self.n_all = int(self._doc_off[-1]) if self.D >= 0 else 0
+        check(lib.tmt_upload_corpus(self.h, _p(self._words), _p(self._doc_off), self.D, _p(zz)), self.h)
+
+    def train(self, iters, ll_every=0):
+        n = iters // ll_every if ll_every else 0
+        out = np.zeros(max(n, 1), dtype=np.float64)
+        check(lib.tmt_train(self.h, int(iters), int(ll_every), _p(out) if n else None), self.h)
+        return out[:n]
+
+    def ll(self):
+        a, b = C.c_double(), C.c_double()
+        check(lib.tmt_ll(self.h, C.byref(a), C.byref(b)), self.h)
+        return a.value, b.value
+
+    def ll_per_word(self):
+        a, b = self.ll()
+        n = self.info().N
+        return (a + b) / n if n else 0.0
+
+    def state(self):
+        z = np.zeros(max(self.n_all, 1), dtype=np.uint16)
+        nkw = np.zeros((self.V, self.K), dtype=np.int32)
+        nk = np.zeros(self.K, dtype=np.int32)
+        alpha = np.zeros(self.K, dtype=np.float32)
+        check(lib.tmt_download_state(self.h, _p(z), _p(nkw), _p(nk), _p(alpha)), self.h)
+        return z[:self.n_all], nkw, nk, alpha
+
+    def doc_topic(self):
+        ndk = np.zeros((max(self.D, 1), self.K), dtype=np.int32)
+        check(lib.tmt_download_doc_topic(self.h, _p(ndk)), self.h)
+        return ndk[:self.D]
+
+    def info(self):
+        i = TmtInfo()
+        check(lib.tmt_get_info(self.h, C.byref(i)), self.h)
+        return i
+
+
+def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1.07, threads=0):
+    """Seeded synthetic corpus (tmt_synth_corpus).  length = ("poisson", mean, lo, hi)
+    or ("lognormal", mu, sigma, lo, hi).  Returns (doc_off uint64[D+1], words uint32[N])."""
+    if length[0] == "poisson":
+        kind, a, b, lo, hi = LEN_POISSON, float(length[1]), 0.0, int(length[2]), int(length[3])
+    else:
+        kind, a, b, lo, hi = LEN_LOGNORMAL, float(length[1]), float(length[2]), int(length[3]), int(length[4])
+    spec = TmtSynthSpec(V=V, T=T, D=D, len_kind=kind, len_a=a, len_b=b, len_min=lo, len_max=hi,
+                        doc_alpha=doc_alpha, topic_beta=topic_beta, zipf_s=zipf_s, seed=seed, threads=threads)
+    off = np.zeros(D + 1, dtype=np.uint64)
+    n = C.c_uint64()
+    check(lib.tmt_synth_corpus(C.byref(spec), _p(off), None, 0, C.byref(n)), None, "synth lengths")
+    words = np.zeros(max(n.value, 1), dtype=np.uint32)
+    check(lib.tmt_synth_corpus(C.byref(spec), _p(off), _p(words), n.value, C.byref(n)), None, "synth words")
+    return off, words[:n.value]
+
+
+def prepare_ids(doc_off, words, min_cf=0, min_df=0, rm_top=0):
+    """Integer-id corpus preparation as tomotopy's prepare() does it: vocab
+    reorder by (cf, df) descending with the stop-word rules (removeStopwords,
+    TopicModel.hpp:526-571), then each document sorted by id (prepareDoc,
+    LDAModel.hpp:716-722).  Returns (doc_off, words, realV, order)."""
+    doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
+    words = np.ascontiguousarray(words, dtype=np.uint32)
+    D = len(doc_off) - 1
+    nv = int(words.max()) + 1 if len(words) else 0
+    out = np.zeros(max(len(words), 1), dtype=np.uint32)
+    order = np.zeros(max(nv, 1), dtype=np.uint32)
+    rv = C.c_uint32()
+    check(lib.tmt_prepare_corpus(D, _p(doc_off), _p(words), nv, min_cf, min_df, rm_top, _p(out), None,
+                                 _p(order), None, None, C.byref(rv)), None, "tmt_prepare_corpus")
+    return doc_off, out[:len(words)], int(rv.value), order[:nv]
