@@ -63,6 +63,8 @@ typedef struct tmt_config {
     int32_t device;          /* CUDA device ordinal */
     int32_t sampler;         /* tmt_sampler */
     uint64_t hbm_budget;     /* bytes this handle may allocate; 0 = unlimited */
+    uint32_t sweep_groups;   /* documents per sweep are sampled in this many groups, the
+                                n_kw / n_k snapshot refreshed between groups; 0 = 1 */
 } tmt_config;
 
 /* Read-only facts about a handle. */

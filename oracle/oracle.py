@@ -56,6 +56,8 @@ def _load():
         "orc_conditional_f64": (None, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, C.c_uint16, V]),
         "orc_sweep_doc_live": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32,
                                       C.c_uint64, V, V, V, V, V, V, V, V]),
+        "orc_sweep_doc_live_subset": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32,
+                                             C.c_uint64] + [V] * 9 + [C.c_uint64]),
         "orc_apply_sweep": (None, [C.c_uint32, C.c_uint32, V, V, V, V, V, V, V]),
         "orc_gibbs_none": (None, [C.c_uint64, V, V, C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, V]),
         "orc_partition_create": (V, [C.c_uint64, V, V, C.c_uint32, C.c_uint32, V, C.c_float,
@@ -204,17 +206,41 @@ class State:
         if c.N:
             self.z[tok_pos.astype(np.int64)] = zw[:c.N]
 
-    def doc_live_sweeps(self, iters, start_step=0):
-        """Doc-major sweeps: live n_dk, snapshot n_kw / n_k (AD-LDA limit)."""
+    def group_bounds(self, groups):
+        """Document groups of a sweep: the documents ordered longest first
+        (stable), cut into `groups` contiguous ranges holding equal shares of
+        the tokens -- position p is in group g when prefix(p) * G lies in
+        [g * total, (g + 1) * total)."""
         c = self.c
+        lens = np.diff(c.doc_off.astype(np.int64))
+        order = np.argsort(-lens, kind="stable").astype(np.uint64)
+        total = int(lens.sum())
+        prefix = np.concatenate([[0], np.cumsum(lens[order.astype(np.int64)])[:-1]]) if c.D else np.zeros(0)
+        bounds = [0]
+        for g in range(1, groups):
+            bounds.append(int(np.sum(prefix * groups < g * total)))
+        bounds.append(c.D)
+        return order, bounds
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+        """The device sweep: doc-major, live n_dk, snapshot n_kw / n_k,
+        sampled group by group (see group_bounds), the snapshot refreshed
+        between groups."""
+        c = self.c
+        order, b = self.group_bounds(groups)
+        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
         for it in range(iters):
-            nkw2 = self.nkw.copy()
-            nk2 = self.nk.copy()
-            lib.orc_sweep_doc_live(self.K, c.V, _ptr(self.alpha), self.eta, self.seed, start_step + it,
-                                   c.D, _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk), _ptr(self.nkw),
-                                   _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z))
-            self.nkw = nkw2
-            self.nk = nk2
+            for part in parts:
+                if len(part) == 0:
+                    continue
+                nkw2 = self.nkw.copy()
+                nk2 = self.nk.copy()
+                lib.orc_sweep_doc_live_subset(self.K, c.V, _ptr(self.alpha), self.eta, self.seed, start_step + it,
+                                              c.D, _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk), _ptr(self.nkw),
+                                              _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z), _ptr(part),
+                                              len(part))
+                self.nkw = nkw2
+                self.nk = nk2
 
     def optimize_alpha(self):
         lib.orc_optimize_alpha(self.c.D, self.K, _ptr(self.ndk), _ptr(self.c.doc_len), _ptr(self.alpha))

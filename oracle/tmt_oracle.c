@@ -916,43 +916,138 @@ double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
 }
 
 /* ------------------------------------------------------------------------ */
-/* Doc-major sweep: live n_dk, snapshot n_kw / n_k                          */
+/* Doc-major sweep: live n_dk, snapshot n_kw / n_k  (the device semantics)  */
 /* ------------------------------------------------------------------------ */
 /* tomotopy's COPY_MERGE with one worker per document (LDAModel.hpp:401-423,
  * 555-570): each document is sampled sequentially with its own n_dk live;
  * n_kw and n_k are the start-of-sweep copy with the token's own assignment
  * removed; every count delta lands in the next state after the sweep.
- * Draw counter: (doc-major token index, iter).  Same segmented scan as the
- * snapshot sweep. */
-void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
+ *
+ * Arithmetic (each operation rounded to nearest, no contraction unless fma):
+ *   R_k      = 1 / ((float)n_k[k] + V*eta)
+ *   phi_k    = ((float)n_kw[k,v] + eta) * R_k             (per word, per sweep)
+ *   phi_own  = ((float)(n_kw[zo,v]-1) + eta) * (1 / ((float)(n_k[zo]-1) + V*eta))
+ *   A_k      = (float)n_dk[k] + alpha_k                    (own token removed)
+ * Topics are dealt to 32 lanes in blocks of four: lane l owns the topics
+ * k = 128*j + 4*l + i (j = 0, 1, ..., i = 0..3, k < K), in that order.
+ * Pass 1: T_l = fma-chain of A_k * phi_k over lane l's topics (s = fma(A, phi,
+ * s) from s = 0); the lane owning zo then sets T_l = max((T_l - A_zo*phi_zo)
+ * + A_zo*phi_own, 0).  X = Hillis-Steele inclusive scan of T over 32 lanes,
+ * E_l = X_{l-1} (E_0 = 0), r = u * X_31, u = Philox(token index, step).
+ * h = first lane owning a topic with r < E_h + T_h (none: K-1).
+ * Pass 2: x_t = A_k * phi_k (phi_own at zo) over lane h's topics in order,
+ * in chunks of 32, each Hillis-Steele scanned and offset by the running
+ * sum of the previous chunks: P_t; result = lane h's t-th topic for the
+ * first t with r < E_h + P_t, else lane h's last topic.  Any fixed topic
+ * order draws from the same distribution; this one makes each warp-wide
+ * load a contiguous 512-byte run. */
+static void hs32(float* x)   /* Hillis-Steele inclusive scan of 32 values */
+{
+    float y[32];
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+        for (uint32_t l = 0; l < 32; ++l) y[l] = (l >= off) ? x[l] + x[l - off] : x[l];
+        memcpy(x, y, sizeof(y));
+    }
+}
+
+/* the t-th topic of lane l, or -1 */
+static inline int64_t lane_topic(uint32_t l, uint32_t t, uint32_t K)
+{
+    uint64_t k = 128ull * (t >> 2) + 4ull * l + (t & 3);
+    return k < K ? (int64_t)k : -1;
+}
+
+static inline uint32_t lane_count(uint32_t l, uint32_t K)
+{
+    uint32_t n = 0;
+    for (uint32_t j = 0; 128 * j + 4 * l < K; ++j) {
+        uint32_t b = 128 * j + 4 * l;
+        n += (K - b) >= 4 ? 4 : (K - b);
+    }
+    return n;
+}
+
+/* A: doc row A_k; phi: word weights; zo, phi_own: the own topic */
+static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own, float u)
+{
+    float T[32], X[32];
+    uint32_t cl[32];
+    for (uint32_t l = 0; l < 32; ++l) {
+        float s = 0.f;
+        cl[l] = lane_count(l, K);
+        for (uint32_t t = 0; t < cl[l]; ++t) {
+            int64_t k = lane_topic(l, t, K);
+            s = fmaf(A[k], phi[k], s);
+        }
+        if (((zo >> 2) & 31) == l) {
+            float wu = A[zo] * phi[zo];
+            float wo = A[zo] * phi_own;
+            s = (s - wu) + wo;
+            if (!(s > 0.f)) s = 0.f;
+        }
+        T[l] = s;
+        X[l] = s;
+    }
+    hs32(X);
+    float total = X[31];
+    float r = u * total;
+    int h = -1;
+    float E = 0.f;
+    for (uint32_t l = 0; l < 32; ++l) {
+        float El = l ? X[l - 1] : 0.f;
+        if (cl[l] && r < El + T[l]) { h = (int)l; E = El; break; }
+    }
+    if (h < 0) return K - 1;
+    uint32_t n = cl[h];
+    float carry = 0.f;
+    for (uint32_t m = 0; m < n; m += 32) {
+        float x[32];
+        for (uint32_t t = 0; t < 32; ++t) {
+            if (m + t < n) {
+                int64_t k = lane_topic((uint32_t)h, m + t, K);
+                x[t] = A[k] * ((uint32_t)k == zo ? phi_own : phi[k]);
+            } else {
+                x[t] = 0.f;
+            }
+        }
+        hs32(x);
+        for (uint32_t t = 0; t < 32 && m + t < n; ++t)
+            if (r < E + (carry + x[t])) return (uint32_t)lane_topic((uint32_t)h, m + t, K);
+        carry = carry + x[31];
+    }
+    return (uint32_t)lane_topic((uint32_t)h, n - 1, K);
+}
+
+void orc_sweep_doc_live_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
                         uint64_t seed, uint32_t iter, uint64_t D, const uint64_t* doc_off,
                         const uint32_t* words, int32_t* ndk,
                         const int32_t* nkw, const int32_t* nk,
-                        int32_t* nkw_next, int32_t* nk_next, uint16_t* z)
+                        int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                        const uint64_t* docs, uint64_t n_docs)
 {
+    (void)D;
     float veta = eta * (float)V;
     float* R = (float*)malloc(K * sizeof(float));
-    float* w = (float*)malloc(K * sizeof(float));
-    float* loc = (float*)malloc(K * sizeof(float));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* phi = (float*)malloc(K * sizeof(float));
     for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / ((float)nk[k] + veta);
-    for (uint64_t d = 0; d < D; ++d) {
+    for (uint64_t di = 0; di < n_docs; ++di) {
+        uint64_t d = docs ? docs[di] : di;
         int32_t* row = ndk + d * K;
+        for (uint32_t k = 0; k < K; ++k) A[k] = (float)row[k] + alpha[k];
         for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
             uint32_t v = words[i];
             if (v >= V) continue;
             uint16_t zo = z[i];
             const int32_t* col = nkw + (size_t)v * K;
             row[zo]--;
-            for (uint32_t k = 0; k < K; ++k) {
-                int own = (k == zo);
-                float a = (float)row[k] + alpha[k];
-                float b = (float)(col[k] - own) + eta;
-                float r = own ? 1.0f / ((float)(nk[k] - 1) + veta) : R[k];
-                w[k] = (a * b) * r;
-            }
+            A[zo] = (float)row[zo] + alpha[zo];
+            for (uint32_t k = 0; k < K; ++k) phi[k] = ((float)col[k] + eta) * R[k];
+            float phi_own = ((float)(col[zo] - 1) + eta) * (1.0f / ((float)(nk[zo] - 1) + veta));
             float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, iter, seed));
-            uint16_t zn = (uint16_t)seg_scan_draw(w, K, u, loc);
+            uint16_t zn = (uint16_t)blocked_draw(A, phi, K, zo, phi_own, u);
             row[zn]++;
+            A[zn] = (float)row[zn] + alpha[zn];
             z[i] = zn;
             if (zn != zo) {
                 nkw_next[(size_t)v * K + zo]--; nkw_next[(size_t)v * K + zn]++;
@@ -960,5 +1055,15 @@ void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
             }
         }
     }
-    free(R); free(w); free(loc);
+    free(R); free(A); free(phi);
+}
+
+void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
+                        uint64_t seed, uint32_t iter, uint64_t D, const uint64_t* doc_off,
+                        const uint32_t* words, int32_t* ndk,
+                        const int32_t* nkw, const int32_t* nk,
+                        int32_t* nkw_next, int32_t* nk_next, uint16_t* z)
+{
+    orc_sweep_doc_live_subset(K, V, alpha, eta, seed, iter, D, doc_off, words, ndk, nkw, nk,
+                              nkw_next, nk_next, z, NULL, D);
 }

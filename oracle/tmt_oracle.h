@@ -117,6 +117,14 @@ void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
                         const uint32_t* words, int32_t* ndk,
                         const int32_t* nkw, const int32_t* nk,
                         int32_t* nkw_next, int32_t* nk_next, uint16_t* z);
+/* the same over a subset of documents (docs[0..n_docs), in that order); the
+ * device splits a sweep into G groups of documents this way */
+void orc_sweep_doc_live_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
+                               uint64_t seed, uint32_t iter, uint64_t D, const uint64_t* doc_off,
+                               const uint32_t* words, int32_t* ndk,
+                               const int32_t* nkw, const int32_t* nk,
+                               int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                               const uint64_t* docs, uint64_t n_docs);
 
 /* ---- the reference's sequential sampler (ParallelScheme::NONE) ---------- */
 /* Doc-major; live counts; forShuffled doc order; SSE prefix sum; strict

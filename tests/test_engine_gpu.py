@@ -19,6 +19,8 @@ from tomotopy_b200._lib import TmtError
 
 pytestmark = pytest.mark.gpu
 
+G = 8   # the engine's default number of document groups per sweep
+
 
 def corpus(V=800, Tt=8, D=120, mean=60, seed=1, min_cf=0, rm_top=0, lognormal=False):
     if lognormal:
@@ -52,18 +54,19 @@ def test_init_and_counts_bitexact(K):
     assert eng.info().N == st.c.N
 
 
-@pytest.mark.parametrize("K", [1, 5, 20, 33, 100, 250, 1000, 1100])
-def test_sweeps_bitexact(K):
+@pytest.mark.parametrize("K,groups", [(1, 1), (5, 1), (20, 1), (33, 3), (100, 1), (100, 4), (250, 1), (1000, 1),
+                                      (1000, 2), (1100, 1), (3000, 1)])
+def test_sweeps_bitexact(K, groups):
     """Every sweep's z and counts equal the oracle's doc-major sweep exactly."""
     off, w, V = corpus(V=600, D=90, mean=50, seed=K, min_cf=2, rm_top=3)
     alpha = np.float32(0.1) if K != 20 else (0.05 * (np.arange(K) + 1)).astype(np.float32)
-    eng = T.Engine(K, V, alpha=alpha, eta=0.01, seed=7, optim_interval=0)
+    eng = T.Engine(K, V, alpha=alpha, eta=0.01, seed=7, optim_interval=0, sweep_groups=groups)
     eng.upload(off, w)
     st = oracle_state(off, w, V, K, alpha, 0.01, 7)
     step = 0
     for n in (1, 2):
         eng.train(n)
-        st.doc_live_sweeps(n, start_step=step)
+        st.doc_live_sweeps(n, start_step=step, groups=groups)
         step += n
         assert_same_state(eng, st)
 
@@ -103,14 +106,15 @@ def test_ll_fp64_matches_oracle(K):
     eng.upload(off, w)
     eng.train(3)
     st = oracle_state(off, w, V, K, 0.1, 0.01, 3)
-    st.doc_live_sweeps(3)
+    st.doc_live_sweeps(3, groups=G)
     ld, lr = eng.ll()
     od, orr = st.ll_f64()
     assert ld == pytest.approx(od, rel=1e-11, abs=1e-7)
     assert lr == pytest.approx(orr, rel=1e-11, abs=1e-7)
-    # the reference's float-LUT likelihood agrees to LUT accuracy
+    # the reference's float-LUT likelihood agrees to the table's accuracy
+    # (linear interpolation of lgamma, step 1/1024 below 1: ~1e-5 per term)
     lut = sum(st.ll_lut())
-    assert (ld + lr) == pytest.approx(lut, rel=2e-5)
+    assert (ld + lr) == pytest.approx(lut, rel=1e-4)
 
 
 @pytest.mark.parametrize("asym", [False, True])
@@ -123,7 +127,7 @@ def test_alpha_optimisation_matches_oracle(asym):
     st = oracle_state(off, w, V, K, alpha, 0.01, 8)
     for step in range(3):
         eng.train(1)
-        st.doc_live_sweeps(1, start_step=step)
+        st.doc_live_sweeps(1, start_step=step, groups=G)
         st.optimize_alpha()
         _, _, _, a_dev = eng.state()
         np.testing.assert_allclose(a_dev, st.alpha, rtol=2e-4)
@@ -194,24 +198,29 @@ def test_chi_square_on_draws():
     assert p > 1e-4, (chi2, p)
 
 
-@pytest.mark.parametrize("K", [10, 40])
-def test_ll_per_word_matches_sequential_sampler(K):
-    """(d) at the same iteration count, the device's ll_per_word is within 1%
-    of the reference's sequential sampler (ParallelScheme::NONE restated),
-    averaged over 3 seeds."""
-    off, w, V = corpus(V=2000, Tt=10, D=300, mean=200, seed=31)
-    iters = 150
-    gpu, seq = [], []
-    for seed in (1, 2, 3):
-        eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
+@pytest.mark.parametrize("K,V,Tt,D,mean,iters", [(20, 5000, 20, 400, 500, 200), (100, 8000, 50, 1500, 200, 150)])
+def test_ll_per_word_matches_reference_train(K, V, Tt, D, mean, iters):
+    """(d) At the same iteration count, the device's ll_per_word is within 1%
+    of tomotopy's train() -- its default ParallelScheme::PARTITION on every
+    host thread, restated in the oracle -- averaged over 5 seeds."""
+    import os
+    off, w = T.synth_corpus(V, Tt, D, ("poisson", mean, 1, 20 * mean), seed=K + 1)
+    off, w, Vr, _ = T.prepare_ids(off, w)
+    c = O.Corpus(off, w, Vr)
+    cf = np.bincount(w[w < Vr], minlength=Vr).astype(np.uint64)
+    gpu, ref = [], []
+    for seed in (1, 2, 3, 4, 5):
+        eng = T.Engine(K, Vr, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
         eng.upload(off, w)
         eng.train(iters)
         gpu.append(eng.ll_per_word())
-        st = oracle_state(off, w, V, K, 0.1, 0.01, seed)
-        st.gibbs_none(iters, 1000 + seed)
-        seq.append(st.ll_per_word())
-    g, s = np.mean(gpu), np.mean(seq)
-    assert abs(g - s) / abs(s) < 0.01, (gpu, seq)
+        st = O.State(c, K, 0.1, 0.01, seed)
+        p = O.Partition(st, os.cpu_count() or 1, vocab_cf=cf, seed=seed)
+        p.train(iters)
+        p.close()
+        ref.append(st.ll_per_word())
+    g, r = np.mean(gpu), np.mean(ref)
+    assert abs(g - r) / abs(r) < 0.01, (gpu, ref)
 
 
 def test_edge_cases():
@@ -228,7 +237,7 @@ def test_edge_cases():
     st = oracle_state(off, words, 10, 3, 0.1, 0.01, 2)
     assert_same_state(eng, st)
     eng.train(4)
-    st.doc_live_sweeps(4)
+    st.doc_live_sweeps(4, groups=G)
     assert_same_state(eng, st)
     z = eng.state()[0]
     assert z[3] == 0xFFFF and z[4] == 0xFFFF

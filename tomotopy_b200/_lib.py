@@ -23,7 +23,7 @@ class TmtConfig(C.Structure):
     _fields_ = [("K", C.c_uint32), ("V", C.c_uint32), ("alpha", C.POINTER(C.c_float)),
                 ("alpha_scalar", C.c_float), ("eta", C.c_float), ("seed", C.c_uint64),
                 ("optim_interval", C.c_uint32), ("burn_in", C.c_uint32), ("device", C.c_int32),
-                ("sampler", C.c_int32), ("hbm_budget", C.c_uint64)]
+                ("sampler", C.c_int32), ("hbm_budget", C.c_uint64), ("sweep_groups", C.c_uint32)]
 
 
 class TmtInfo(C.Structure):

@@ -38,7 +38,6 @@ namespace {
 constexpr unsigned FULL = 0xFFFFFFFFu;
 constexpr int kSweepWarps = 8;           // warps per sweep block
 
-__device__ __forceinline__ int sk(int k) { return k + (k >> 5); }   // bank skew
 
 // ---------------------------------------------------------------------------
 // initialisation: z0 ~ Discrete(alpha) (initializeDocState, LDAModel.hpp:781-813)
@@ -89,13 +88,47 @@ __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* _
 // ---------------------------------------------------------------------------
 // the training sweep
 // ---------------------------------------------------------------------------
+// Per-sweep word table: phi[v*KP + k] = ((float)n_kw[k,v] + eta) * R_k with
+// R_k = 1 / ((float)n_k[k] + V*eta) and KP = K rounded up to a multiple of
+// 4 (entries K..KP-1 are 0); the same pass copies n_kw and n_k into the
+// next state, which the sweep then updates with the count deltas.
+__global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __restrict__ nk, uint32_t V, uint32_t K,
+                           uint32_t KP, float eta, float veta, float* __restrict__ phi, int32_t* __restrict__ nkw_next,
+                           int32_t* __restrict__ nk_next, uint32_t smem_k)
+{
+    extern __shared__ float s_R[];
+    const bool r_smem = K <= smem_k;
+    if (r_smem)
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+    if (blockIdx.x == 0)
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) nk_next[k] = nk[k];
+    __syncthreads();
+    for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
+        const int32_t* src = nkw + v * K;
+        int32_t* dst = nkw_next + v * K;
+        float* ph = phi + v * KP;
+        for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
+            float val = 0.f;
+            if (k < K) {
+                const int32_t n = src[k];
+                dst[k] = n;
+                const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+                val = __fmul_rn(__fadd_rn((float)n, eta), R);
+            }
+            ph[k] = val;
+        }
+    }
+}
+
 struct SweepArgs {
     const uint64_t* doc_off;
     const uint32_t* words;
     uint16_t* z;
     int32_t* ndk;
-    const int32_t* nkw;
+    const int32_t* nkw;     // start-of-sweep snapshot (own-topic weight)
     const int32_t* nk;
+    const float* phi;       // per-word topic weights of the snapshot
     int32_t* nkw_next;
     int32_t* nk_next;
     const float* alpha;
@@ -106,223 +139,225 @@ struct SweepArgs {
     float eta, veta;
     uint64_t seed;
     uint32_t iter;
+    uint64_t pos_begin, pos_end;  // this launch samples doc_order positions [pos_begin, pos_end)
+    uint32_t rowi_smem;      // 1: the int n_dk row lives in shared memory
+    uint32_t dnk_smem;       // 1: n_k deltas aggregate in shared memory
 };
 
-// Segment loads of an int32 K-vector: lane owns [k0, k0 + c).
-template <int CMAX, bool VEC>
-__device__ __forceinline__ void load_segment(const int32_t* __restrict__ p, int k0, int c, int K, int (&out)[CMAX])
+__device__ __forceinline__ float hs_scan32(float x, int lane)
 {
-    if (VEC) {
 #pragma unroll
-        for (int j = 0; j < CMAX; j += 4) {
-            if (j < c && k0 + j < K) {
-                int4 q = __ldg(reinterpret_cast<const int4*>(p + k0 + j));
-                out[j] = q.x; out[j + 1] = q.y; out[j + 2] = q.z; out[j + 3] = q.w;
-            }
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < CMAX; ++j)
-            if (j < c && k0 + j < K) out[j] = __ldg(p + k0 + j);
+    for (int off = 1; off < 32; off <<= 1) {
+        const float y = __shfl_up_sync(FULL, x, off);
+        if (lane >= off) x = __fadd_rn(x, y);
     }
+    return x;
 }
 
-template <int CMAX, bool VEC>
-__global__ void __launch_bounds__(kSweepWarps * 32)
+// Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
+// aligned regions): [n_k deltas: KP ints] [per warp: (float)n_dk + alpha, KP
+// floats, zero padded] [per warp: n_dk, KP ints].
+__host__ __device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
+
+// Topics are dealt to lanes in blocks of four: lane l owns k = 128*j + 4*l + i.
+// Every warp-wide float4 load of a K-vector is one contiguous 512-byte run
+// and shared-memory float4 reads are conflict-free.
+//   CH > 0: at most CH blocks per lane (KP <= 128*CH <= 4096), unrolled.
+//   CH == 0: any K, runtime loops.
+//   PF: the next token's word weights are loaded while the current token is
+//       sampled (the loads do not depend on the document row).
+template <int CH, int MINB, bool PF>
+__global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
-    extern __shared__ int smem[];
+    constexpr int CHR = CH > 0 ? CH : 1;
+    extern __shared__ __align__(16) int smem[];
     const int K = (int)a.K;
-    const int KS = K + (K >> 5) + 1;
-    float* s_alpha = reinterpret_cast<float*>(smem);
-    float* s_R = s_alpha + KS;
-    int* s_dnk = reinterpret_cast<int*>(s_R + KS);
-    int* s_rows = s_dnk + K;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int* row = s_rows + warp * KS;
-
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        s_alpha[sk(k)] = a.alpha[k];
-        s_R[sk(k)] = __fdiv_rn(1.0f, __fadd_rn((float)a.nk[k], a.veta));
-        s_dnk[k] = 0;
+    const int KP = (int)round4(a.K);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int* s_dnk = smem;
+    float* s_rowf = reinterpret_cast<float*>(smem + (a.dnk_smem ? KP : 0));
+    float* rowf = s_rowf + warp * KP;
+    int* s_rowi = reinterpret_cast<int*>(s_rowf + nwarps * KP);
+    if (a.dnk_smem) {
+        for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
+        __syncthreads();
     }
-    __syncthreads();
-
-    const int c = (int)a.c;
-    const int k0 = lane * c;
+    // blocks of four owned by this lane
+    const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
     const float eta = a.eta, veta = a.veta;
+
+    auto load_word = [&](uint32_t v, int zo, float4 (&pv)[CHR], int& nkw_o, int& nk_o, float& phu) {
+        const float* ph = a.phi + (uint64_t)v * KP;
+        if (CH > 0) {
+#pragma unroll
+            for (int jj = 0; jj < CHR; ++jj)
+                if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
+        }
+        nkw_o = __ldg(a.nkw + (uint64_t)v * K + zo);
+        nk_o = __ldg(a.nk + zo);
+        phu = __ldg(ph + zo);
+    };
 
     for (;;) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
         q = __shfl_sync(FULL, q, 0);
-        if (q >= a.D) break;
-        const uint64_t d = a.doc_order[q];
+        const uint64_t pos = a.pos_begin + q;
+        if (pos >= a.pos_end) break;
+        const uint64_t d = a.doc_order[pos];
         int32_t* grow = a.ndk + d * (uint64_t)K;
-        for (int k = lane; k < K; k += 32) row[sk(k)] = grow[k];
+        int* rowi = a.rowi_smem ? (s_rowi + warp * KP) : grow;
+        for (int k = lane; k < KP; k += 32) {
+            float f = 0.f;
+            if (k < K) {
+                const int n = grow[k];
+                if (a.rowi_smem) rowi[k] = n;
+                f = __fadd_rn((float)n, __ldg(a.alpha + k));
+            }
+            rowf[k] = f;
+        }
         __syncwarp();
         const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
         for (uint64_t base = b; base < e; base += 32) {
             const uint64_t my_i = base + lane;
-            uint32_t my_w = 0xFFFFFFFFu;
-            uint32_t my_z = 0xFFFF;
-            if (my_i < e) { my_w = a.words[my_i]; my_z = a.z[my_i]; }
+            uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
+            float my_u = 0.f;
+            if (my_i < e) {
+                my_w = a.words[my_i];
+                my_z = a.z[my_i];
+                my_u = tmt::u01(tmt::philox_u32((uint32_t)my_i, (uint32_t)(my_i >> 32), tmt::kStreamSweep,
+                                                a.iter, a.seed));
+            }
             uint32_t my_new = my_z;
-            const int nb = (int)min((uint64_t)32, e - base);
-            for (int j = 0; j < nb; ++j) {
-                const uint32_t v = __shfl_sync(FULL, my_w, j);
-                const int zo = (int)__shfl_sync(FULL, my_z, j);
-                if (v >= a.V) continue;
-                if (lane == 0) row[sk(zo)] -= 1;
-                __syncwarp();
-                const int32_t* col = a.nkw + (uint64_t)v * K;
-                int cv[CMAX];
-                load_segment<CMAX, VEC>(col, k0, c, K, cv);
-                float loc[CMAX];
-                float s = 0.f;
-#pragma unroll
-                for (int jj = 0; jj < CMAX; ++jj) {
-                    const int k = k0 + jj;
-                    if (jj < c && k < K) {
-                        const int own = (k == zo);
-                        const float A = __fadd_rn((float)row[sk(k)], s_alpha[sk(k)]);
-                        const float B = __fadd_rn((float)(cv[jj] - own), eta);
-                        const float R = own ? __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + k) - 1), veta))
-                                            : s_R[sk(k)];
-                        s = __fadd_rn(s, __fmul_rn(__fmul_rn(A, B), R));
+            unsigned vm = __ballot_sync(FULL, my_i < e && my_w < a.V);
+            if (vm) {
+                int j = __ffs(vm) - 1;
+                vm &= vm - 1;
+                uint32_t v = __shfl_sync(FULL, my_w, j);
+                int zo = (int)__shfl_sync(FULL, my_z, j);
+                float4 pv[CHR];
+                int nkw_o, nk_o;
+                float phu;
+                load_word(v, zo, pv, nkw_o, nk_o, phu);
+                for (;;) {
+                    const int jn = vm ? __ffs(vm) - 1 : -1;
+                    uint32_t vn = 0;
+                    int zon = 0;
+                    float4 pvn[CHR];
+                    int nkw_on = 0, nk_on = 0;
+                    float phun = 0.f;
+                    if (PF && jn >= 0) {
+                        vn = __shfl_sync(FULL, my_w, jn);
+                        zon = (int)__shfl_sync(FULL, my_z, jn);
+                        load_word(vn, zon, pvn, nkw_on, nk_on, phun);
                     }
-                    loc[jj] = s;
-                }
-                float x = s;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const float y = __shfl_up_sync(FULL, x, off);
-                    if (lane >= off) x = __fadd_rn(x, y);
-                }
-                float excl = __shfl_up_sync(FULL, x, 1);
-                if (lane == 0) excl = 0.f;
-                const float total = __shfl_sync(FULL, x, 31);
-                const uint64_t ti = base + j;
-                const float u = tmt::u01(tmt::philox_u32((uint32_t)ti, (uint32_t)(ti >> 32), tmt::kStreamSweep,
-                                                         a.iter, a.seed));
-                const float r = __fmul_rn(u, total);
-                const bool has = (k0 < K) && (r < __fadd_rn(excl, s));
-                const unsigned m = __ballot_sync(FULL, has);
-                int zn = K - 1;
-                if (m) {
-                    const int hl = __ffs(m) - 1;
-                    int hit = 0;
-                    if (lane == hl) {
-                        hit = c - 1;
-#pragma unroll
-                        for (int jj = CMAX - 1; jj >= 0; --jj)
-                            if (jj < c && k0 + jj < K && r < __fadd_rn(excl, loc[jj])) hit = jj;
+                    const float u = __shfl_sync(FULL, my_u, j);
+                    const float* ph = a.phi + (uint64_t)v * KP;
+                    if (lane == 0) {          // remove the token from its document
+                        const int n = rowi[zo] - 1;
+                        rowi[zo] = n;
+                        rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
                     }
-                    hit = __shfl_sync(FULL, hit, hl);
-                    zn = hl * c + hit;
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    row[sk(zn)] += 1;
-                    if (zn != zo) {
-                        atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
-                        atomicAdd(&a.nkw_next[(uint64_t)v * K + zn], 1);
-                        atomicSub(&s_dnk[zo], 1);
-                        atomicAdd(&s_dnk[zn], 1);
+                    __syncwarp();
+                    const float phi_own = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eta),
+                                                    __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), veta)));
+                    // pass 1: fma chain over this lane's topics
+                    float s = 0.f;
+                    if (CH > 0) {
+#pragma unroll
+                        for (int jj = 0; jj < CHR; ++jj) {
+                            if (jj < nch) {
+                                const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
+                                s = __fmaf_rn(A4.x, pv[jj].x, s);
+                                s = __fmaf_rn(A4.y, pv[jj].y, s);
+                                s = __fmaf_rn(A4.z, pv[jj].z, s);
+                                s = __fmaf_rn(A4.w, pv[jj].w, s);
+                            }
+                        }
+                    } else {
+                        for (int jj = 0; jj < nch; ++jj) {
+                            const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
+                            const float4 P4 = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
+                            s = __fmaf_rn(A4.x, P4.x, s);
+                            s = __fmaf_rn(A4.y, P4.y, s);
+                            s = __fmaf_rn(A4.z, P4.z, s);
+                            s = __fmaf_rn(A4.w, P4.w, s);
+                        }
+                    }
+                    if (lane == ((zo >> 2) & 31)) {   // the own topic: exclude the token from n_kw, n_k
+                        const float Ao = rowf[zo];
+                        s = fmaxf(__fadd_rn(__fsub_rn(s, __fmul_rn(Ao, phu)), __fmul_rn(Ao, phi_own)), 0.f);
+                    }
+                    const float x = hs_scan32(s, lane);
+                    float E = __shfl_up_sync(FULL, x, 1);
+                    if (lane == 0) E = 0.f;
+                    const float total = __shfl_sync(FULL, x, 31);
+                    const float r = __fmul_rn(u, total);
+                    const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
+                    int znew = K - 1;
+                    if (m) {
+                        // pass 2: position among lane h's topics, 32 at a time
+                        const int h = __ffs(m) - 1;
+                        const float Eh = __shfl_sync(FULL, E, h);
+                        const int mh = K - 4 * h;
+                        const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
+                        float carry = 0.f;
+                        int found = nh - 1;
+                        for (int mm = 0; mm < nh; mm += 32) {
+                            const int t = mm + lane;
+                            const int k = 128 * (t >> 2) + 4 * h + (t & 3);
+                            float x2 = 0.f;
+                            if (t < nh) x2 = __fmul_rn(rowf[k], k == zo ? phi_own : __ldg(ph + k));
+                            x2 = hs_scan32(x2, lane);
+                            const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
+                            if (mb) { found = mm + __ffs(mb) - 1; break; }
+                            carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                        }
+                        znew = 128 * (found >> 2) + 4 * h + (found & 3);
+                    }
+                    if (lane == 0) {
+                        const int n = rowi[znew] + 1;
+                        rowi[znew] = n;
+                        rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
+                        if (znew != zo) {
+                            atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
+                            atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
+                            if (a.dnk_smem) { atomicSub(&s_dnk[zo], 1); atomicAdd(&s_dnk[znew], 1); }
+                            else { atomicSub(&a.nk_next[zo], 1); atomicAdd(&a.nk_next[znew], 1); }
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == j) my_new = (uint32_t)znew;
+                    if (jn < 0) break;
+                    j = jn;
+                    vm &= vm - 1;
+                    if (PF) {
+                        v = vn;
+                        zo = zon;
+#pragma unroll
+                        for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
+                        nkw_o = nkw_on;
+                        nk_o = nk_on;
+                        phu = phun;
+                    } else {
+                        v = __shfl_sync(FULL, my_w, j);
+                        zo = (int)__shfl_sync(FULL, my_z, j);
+                        load_word(v, zo, pv, nkw_o, nk_o, phu);
                     }
                 }
-                if (lane == j) my_new = (uint32_t)zn;
             }
             if (my_i < e && my_w < a.V) a.z[my_i] = (uint16_t)my_new;
         }
         __syncwarp();
-        for (int k = lane; k < K; k += 32) grow[k] = row[sk(k)];
+        if (a.rowi_smem)
+            for (int k = lane; k < K; k += 32) grow[k] = rowi[k];
         __syncwarp();
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < K; k += blockDim.x)
-        if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
-}
-
-// K > 1024: two passes per token -- lane totals first, then the hit lane
-// recomputes its segment with identical arithmetic.  The doc row stays in
-// global memory (only its own warp touches it during the sweep).
-__global__ void __launch_bounds__(kSweepWarps * 32)
-k_sweep_doc_large(SweepArgs a)
-{
-    const int K = (int)a.K;
-    const int lane = threadIdx.x & 31;
-    const int c = (int)a.c;
-    const int k0 = lane * c;
-    const float eta = a.eta, veta = a.veta;
-    for (;;) {
-        uint32_t q = 0;
-        if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
-        q = __shfl_sync(FULL, q, 0);
-        if (q >= a.D) break;
-        const uint64_t d = a.doc_order[q];
-        int32_t* row = a.ndk + d * (uint64_t)K;
-        const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
-        for (uint64_t i = b; i < e; ++i) {
-            const uint32_t v = a.words[i];
-            if (v >= a.V) continue;
-            const int zo = a.z[i];
-            if (lane == 0) row[zo] -= 1;
-            __syncwarp();
-            __threadfence_block();
-            const int32_t* col = a.nkw + (uint64_t)v * K;
-            auto weight = [&](int k) -> float {
-                const int own = (k == zo);
-                const float A = __fadd_rn((float)row[k], a.alpha[k]);
-                const float B = __fadd_rn((float)(col[k] - own), eta);
-                const float R = __fdiv_rn(1.0f, __fadd_rn((float)(a.nk[k] - own), veta));
-                return __fmul_rn(__fmul_rn(A, B), R);
-            };
-            float s = 0.f;
-            for (int jj = 0; jj < c && k0 + jj < K; ++jj) s = __fadd_rn(s, weight(k0 + jj));
-            float x = s;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const float y = __shfl_up_sync(FULL, x, off);
-                if (lane >= off) x = __fadd_rn(x, y);
-            }
-            float excl = __shfl_up_sync(FULL, x, 1);
-            if (lane == 0) excl = 0.f;
-            const float total = __shfl_sync(FULL, x, 31);
-            const float u = tmt::u01(tmt::philox_u32((uint32_t)i, (uint32_t)(i >> 32), tmt::kStreamSweep,
-                                                     a.iter, a.seed));
-            const float r = __fmul_rn(u, total);
-            const bool has = (k0 < K) && (r < __fadd_rn(excl, s));
-            const unsigned m = __ballot_sync(FULL, has);
-            int zn = K - 1;
-            if (m) {
-                const int hl = __ffs(m) - 1;
-                int hit = 0;
-                if (lane == hl) {
-                    float t = 0.f;
-                    hit = c - 1;
-                    for (int jj = 0; jj < c && k0 + jj < K; ++jj) {
-                        t = __fadd_rn(t, weight(k0 + jj));
-                        if (r < __fadd_rn(excl, t)) { hit = jj; break; }
-                    }
-                }
-                hit = __shfl_sync(FULL, hit, hl);
-                zn = hl * c + hit;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                row[zn] += 1;
-                a.z[i] = (uint16_t)zn;
-                if (zn != zo) {
-                    atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
-                    atomicAdd(&a.nkw_next[(uint64_t)v * K + zn], 1);
-                    atomicSub(&a.nk_next[zo], 1);
-                    atomicAdd(&a.nk_next[zn], 1);
-                }
-            }
-            __syncwarp();
-            __threadfence_block();
-        }
+    if (a.dnk_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < K; k += blockDim.x)
+            if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
     }
 }
 
@@ -546,6 +581,15 @@ struct tmt_handle {
     int32_t* d_ndk = nullptr;
     int32_t* d_nkw[2] = { nullptr, nullptr };
     int32_t* d_nk[2] = { nullptr, nullptr };
+    float* d_phi = nullptr;          // per-word topic weights of the current snapshot
+    uint32_t groups = 1;             // document groups per sweep
+    std::vector<uint64_t> group_bounds;   // doc_order positions: group g = [b[g], b[g+1])
+    // sweep-kernel autotuner: variants give bit-identical results, so the
+    // first sweeps each time one variant and the fastest is kept
+    int variant = 0;
+    int n_variants = 1;
+    int tuned = -1;                  // chosen variant, -1 while tuning
+    std::vector<float> variant_ms;
     int cur = 0;
     int32_t* d_doc_len = nullptr;
     uint32_t* d_doc_order = nullptr;
@@ -641,78 +685,116 @@ void launch_check(tmt_handle* h)
     CK(cudaGetLastError());
 }
 
-uint32_t sweep_smem_bytes(uint32_t K)
+struct SweepShape {
+    uint32_t warps;      // warps per block
+    uint32_t smem;       // dynamic shared memory bytes
+    uint32_t rowi_smem, dnk_smem;
+};
+
+SweepShape sweep_shape(uint32_t K)
 {
-    uint32_t KS = K + (K >> 5) + 1;
-    return (2 * KS + K + kSweepWarps * KS) * 4;
+    const uint32_t KP = round4(K);
+    const uint32_t budget = 200 * 1024;
+    SweepShape s{};
+    s.dnk_smem = K <= 16384;
+    s.rowi_smem = K <= 8192;
+    const uint32_t per_warp = 4 * KP + (s.rowi_smem ? 4 * KP : 0);
+    const uint32_t fixed = s.dnk_smem ? 4 * KP : 0;
+    uint32_t w = (budget - fixed) / per_warp;
+    s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
+    s.smem = fixed + s.warps * per_warp;
+    return s;
 }
 
-template <int CMAX, bool VEC>
-void launch_sweep_t(tmt_handle* h, const SweepArgs& a, uint32_t smem)
+template <int CH, int MINB, bool PF>
+void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CMAX, VEC>;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = k_sweep_doc<CH, MINB, PF>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepWarps * 32, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.warps * 32, sh.smem));
     if (per_sm < 1) throw CudaError("sweep kernel does not fit on an SM");
-    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms,
-                                                 (h->D + kSweepWarps - 1) / kSweepWarps);
+    const uint64_t docs = a.pos_end - a.pos_begin;
+    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms, (docs + sh.warps - 1) / sh.warps);
     if (grid == 0) grid = 1;
-    kern<<<grid, kSweepWarps * 32, smem, h->stream>>>(a);
+    kern<<<grid, sh.warps * 32, sh.smem, h->stream>>>(a);
     launch_check(h);
+}
+
+// Variants (identical results, different speed): 0 = prefetch (up to 1024
+// topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM.
+template <int CH>
+void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
+{
+    constexpr bool kPrefetch = CH <= 8;   // above, the prefetch registers spill
+    if (h->variant == 1) launch_sweep_t<CH, 3, false>(h, a, sh);
+    else launch_sweep_t<CH, 2, kPrefetch>(h, a, sh);
 }
 
 void launch_sweep(tmt_handle* h, const SweepArgs& a)
 {
-    const uint32_t K = a.K, c = a.c;
-    const uint32_t smem = sweep_smem_bytes(K);
-    const bool vec = (K % 4 == 0) && (c % 4 == 0);
-    if (c <= 1) launch_sweep_t<1, false>(h, a, smem);
-    else if (c <= 2) launch_sweep_t<2, false>(h, a, smem);
-    else if (c <= 4) { if (vec) launch_sweep_t<4, true>(h, a, smem); else launch_sweep_t<4, false>(h, a, smem); }
-    else if (c <= 8) { if (vec) launch_sweep_t<8, true>(h, a, smem); else launch_sweep_t<8, false>(h, a, smem); }
-    else if (c <= 16) { if (vec) launch_sweep_t<16, true>(h, a, smem); else launch_sweep_t<16, false>(h, a, smem); }
-    else if (c <= 32) { if (vec) launch_sweep_t<32, true>(h, a, smem); else launch_sweep_t<32, false>(h, a, smem); }
-    else {
-        uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 8,
-                                                     (h->D + kSweepWarps - 1) / kSweepWarps);
-        if (grid == 0) grid = 1;
-        k_sweep_doc_large<<<grid, kSweepWarps * 32, 0, h->stream>>>(a);
-        launch_check(h);
-    }
+    const uint32_t KP = round4(a.K);
+    const uint32_t ch = (KP + 127) / 128;
+    const SweepShape sh = sweep_shape(a.K);
+    SweepArgs b = a;
+    b.rowi_smem = sh.rowi_smem;
+    b.dnk_smem = sh.dnk_smem;
+    if (ch <= 1) launch_sweep_ch<1>(h, b, sh);
+    else if (ch <= 2) launch_sweep_ch<2>(h, b, sh);
+    else if (ch <= 4) launch_sweep_ch<4>(h, b, sh);
+    else if (ch <= 8) launch_sweep_ch<8>(h, b, sh);
+    else if (ch <= 16) launch_sweep_ch<16>(h, b, sh);
+    else if (ch <= 32) launch_sweep_ch<32>(h, b, sh);
+    else launch_sweep_t<0, 3, false>(h, b, sh);
 }
 
+// One sweep = one launch per document group (contiguous ranges of the
+// longest-first order holding equal shares of the tokens); before each, the
+// word table and the next-state copy are rebuilt from the current state.
 void do_sweep(tmt_handle* h)
 {
-    const int cur = h->cur, nxt = cur ^ 1;
-    const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
-    CK(cudaMemcpyAsync(h->d_nkw[nxt], h->d_nkw[cur], kv * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_nk[nxt], h->d_nk[cur], h->cfg.K * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
-    SweepArgs a{};
-    a.doc_off = h->d_doc_off;
-    a.words = h->d_words;
-    a.z = h->d_z;
-    a.ndk = h->d_ndk;
-    a.nkw = h->d_nkw[cur];
-    a.nk = h->d_nk[cur];
-    a.nkw_next = h->d_nkw[nxt];
-    a.nk_next = h->d_nk[nxt];
-    a.alpha = h->d_alpha;
-    a.doc_order = h->d_doc_order;
-    a.doc_counter = h->d_counter;
-    a.D = h->D;
-    a.K = h->cfg.K;
-    a.V = h->cfg.V;
-    a.c = (h->cfg.K + 31) / 32;
-    a.eta = h->cfg.eta;
-    a.veta = h->cfg.eta * (float)h->cfg.V;
-    a.seed = h->cfg.seed;
-    a.iter = (uint32_t)h->global_step;
-    CK(cudaEventRecord(h->kev0, h->stream));
-    launch_sweep(h, a);
+    const uint32_t K = h->cfg.K, V = h->cfg.V;
+    const float veta = h->cfg.eta * (float)V;
+    bool recorded = false;
+    const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
+    for (uint32_t g = 0; g < G; ++g) {
+        if (h->group_bounds[g] == h->group_bounds[g + 1]) continue;
+        const int cur = h->cur, nxt = cur ^ 1;
+        const uint32_t smem_k = K <= 12288 ? K : 0;
+        uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
+        k_phi_copy<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[cur], h->d_nk[cur], V, K, round4(K), h->cfg.eta,
+                                                        veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k);
+        launch_check(h);
+        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+        SweepArgs a{};
+        a.doc_off = h->d_doc_off;
+        a.words = h->d_words;
+        a.z = h->d_z;
+        a.ndk = h->d_ndk;
+        a.nkw = h->d_nkw[cur];
+        a.nk = h->d_nk[cur];
+        a.phi = h->d_phi;
+        a.nkw_next = h->d_nkw[nxt];
+        a.nk_next = h->d_nk[nxt];
+        a.alpha = h->d_alpha;
+        a.doc_order = h->d_doc_order;
+        a.doc_counter = h->d_counter;
+        a.D = h->D;
+        a.K = K;
+        a.V = V;
+        a.c = (K + 31) / 32;
+        a.eta = h->cfg.eta;
+        a.veta = veta;
+        a.seed = h->cfg.seed;
+        a.iter = (uint32_t)h->global_step;
+        a.pos_begin = h->group_bounds[g];
+        a.pos_end = h->group_bounds[g + 1];
+        if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
+        launch_sweep(h, a);
+        h->cur = nxt;
+    }
     CK(cudaEventRecord(h->kev1, h->stream));
-    h->cur = nxt;
+    if (!recorded) CK(cudaEventRecord(h->kev0, h->stream));
     h->sampler_used = TMT_SAMPLER_DENSE;
 }
 
@@ -791,6 +873,7 @@ tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out)
         return TMT_ERR_INVALID_ARGUMENT;
     }
     tmt_status s = guarded(h, [&] {
+        h->groups = cfg->sweep_groups ? cfg->sweep_groups : 8;
         h->alpha.assign(cfg->K, cfg->alpha_scalar);
         if (cfg->alpha) std::copy(cfg->alpha, cfg->alpha + cfg->K, h->alpha.begin());
         CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -847,6 +930,20 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
             return doc_off[a + 1] - doc_off[a] > doc_off[b + 1] - doc_off[b];
         });
 
+        // groups: contiguous ranges of the order with equal shares of the tokens;
+        // position p is in group g when prefix(p) * G lies in [g * total, (g+1) * total)
+        {
+            const uint64_t G = std::max<uint64_t>(1, h->groups);
+            h->group_bounds.assign(G + 1, 0);
+            h->group_bounds[G] = D;
+            uint64_t prefix = 0;
+            uint64_t g = 1;
+            for (uint64_t p = 0; p < D; ++p) {
+                while (g < G && prefix * G >= g * n_all) h->group_bounds[g++] = p;
+                prefix += doc_off[order[p] + 1] - doc_off[order[p]];
+            }
+            while (g < G) h->group_bounds[g++] = D;
+        }
         h->d_doc_off = h->dalloc<uint64_t>(D + 1);
         h->d_words = h->dalloc<uint32_t>(n_all);
         h->d_z = h->dalloc<uint16_t>(n_all);
@@ -855,6 +952,13 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
         h->d_nkw[1] = h->dalloc<int32_t>((uint64_t)K * V);
         h->d_nk[0] = h->dalloc<int32_t>(K);
         h->d_nk[1] = h->dalloc<int32_t>(K);
+        h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
+        {
+            h->n_variants = round4(K) <= 4096 ? 2 : 1;
+            h->variant = 0;
+            h->tuned = h->n_variants > 1 ? -1 : 0;
+            h->variant_ms.clear();
+        }
         h->d_doc_len = h->dalloc<int32_t>(D);
         h->d_doc_order = h->dalloc<uint32_t>(D);
         h->d_counter = h->dalloc<uint32_t>(1);
@@ -934,6 +1038,16 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
                 CK(cudaEventElapsedTime(&ms, h->kev0, h->kev1));
                 h->sweep_kernel_ms += ms;
                 ++h->sweeps_timed;
+                if (h->tuned < 0) {
+                    h->variant_ms.push_back(ms);
+                    if ((int)h->variant_ms.size() >= h->n_variants) {
+                        h->tuned = (int)(std::min_element(h->variant_ms.begin(), h->variant_ms.end()) -
+                                         h->variant_ms.begin());
+                        h->variant = h->tuned;
+                    } else {
+                        h->variant = (int)h->variant_ms.size();
+                    }
+                }
             }
             const uint64_t gs = h->global_step;
             if (gs >= h->cfg.burn_in && h->cfg.optim_interval && (gs + 1) % h->cfg.optim_interval == 0)

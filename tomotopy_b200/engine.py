@@ -16,7 +16,7 @@ class Engine:
     """One model state on one GPU (tmt_handle)."""
 
     def __init__(self, K, V, alpha=0.1, eta=0.01, seed=0, optim_interval=10, burn_in=0, device=0,
-                 sampler=SAMPLER_AUTO, hbm_budget=0):
+                 sampler=SAMPLER_AUTO, hbm_budget=0, sweep_groups=0):
         self.K, self.V = int(K), int(V)
         a = np.broadcast_to(np.asarray(alpha, dtype=np.float32), (self.K,)).copy() \
             if np.ndim(alpha) else None
@@ -25,7 +25,7 @@ class Engine:
                         alpha=a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None,
                         alpha_scalar=float(alpha) if a is None else 0.0, eta=float(eta), seed=int(seed),
                         optim_interval=int(optim_interval), burn_in=int(burn_in), device=int(device),
-                        sampler=int(sampler), hbm_budget=int(hbm_budget))
+                        sampler=int(sampler), hbm_budget=int(hbm_budget), sweep_groups=int(sweep_groups))
         h = C.c_void_p()
         st = lib.tmt_create(C.byref(cfg), C.byref(h))
         self.h = h
