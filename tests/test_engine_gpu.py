@@ -177,7 +177,8 @@ def test_chi_square_on_draws():
     off = np.arange(D + 1, dtype=np.uint64) * L
     words = np.tile(doc, D)
     z0 = np.tile(z_doc, D)
-    eng = T.Engine(K, V, alpha=0.3, eta=0.05, seed=99, optim_interval=0)
+    # one document group: every first token sees the same start-of-sweep snapshot
+    eng = T.Engine(K, V, alpha=0.3, eta=0.05, seed=99, optim_interval=0, sweep_groups=1)
     eng.upload(off, words, z0=z0)
     st = oracle_state(off, words, V, K, 0.3, 0.05, 99, z0=z0)
     p64 = np.zeros(K)
