@@ -130,6 +130,29 @@ tmt_status tmt_prepare_corpus(uint64_t D, const uint64_t* doc_off, const uint32_
                               uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
                               uint64_t* vocab_cf, uint64_t* vocab_df, uint32_t* real_v);
 
+/* No counterpart in tomotopy.  The FP64 log-likelihood of tmt_ll computed
+ * from caller-owned DEVICE arrays -- n_dk (D x K), doc_len (D valid-token
+ * counts), alpha (K), n_kw (K x V column-major), n_k (K) -- into ll_out (2
+ * doubles on the device: ll_docs, ll_rest), on `stream` (a cudaStream_t;
+ * NULL = the legacy default stream), without allocating any memory.  For
+ * callers that may not call cudaMalloc: a serving process whose device
+ * memory is handed out up front by its own pool, a plug-in inside a host
+ * framework that owns every device allocation, or a pipelined stream that
+ * must not pick up the implicit device synchronisation cudaMalloc/cudaFree
+ * can cause.  Its scratch is one static device array of 281 KB, held by
+ * every GPU that loads this library until the process exits; it supports
+ * K <= 32767 and rejects larger K with TMT_ERR_INVALID_ARGUMENT.  The first
+ * call on a device looks up that array's device address (with the device
+ * current) and caches it; make that first call before any stream capture.
+ * All calls on a device share the scratch: calls that overlap on the GPU
+ * race and give wrong sums -- serialise them (one stream, or events).  Each
+ * call overwrites every scratch slot it reads, so no clearing is needed.
+ * The launches are asynchronous on `stream`.  A message for a non-OK status
+ * is written to err (err_len bytes, may be NULL). */
+tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, const int32_t* doc_len,
+                                 const float* alpha, const int32_t* n_kw, uint32_t V, const int32_t* n_k,
+                                 float eta, double* ll_out, void* stream, char* err, size_t err_len);
+
 tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out);
 const char* tmt_last_error(const tmt_handle* h);
 void tmt_destroy(tmt_handle* h);

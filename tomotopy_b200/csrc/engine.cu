@@ -29,6 +29,7 @@
 #include <numeric>
 #include <algorithm>
 #include <stdexcept>
+#include <mutex>
 #include "philox.cuh"
 #include "special.cuh"
 #include "../../include/tomotopy_b200.h"
@@ -448,6 +449,16 @@ __global__ void k_ll_final(const double* __restrict__ partials, uint32_t nparts,
         if (lane == 0) { out[0] = x; out[1] = y; }
     }
 }
+
+// ---------------------------------------------------------------------------
+// log-likelihood without device allocation (tmt_ll_counts_noalloc)
+// ---------------------------------------------------------------------------
+// Scratch of tmt_ll_counts_noalloc: 2 partial sums per block of the partial
+// kernel, lgamma(alpha_k) for up to 32767 topics, sum(alpha) and its lgamma.
+// 281 KB; every GPU that loads this library holds it until the process exits.
+constexpr uint32_t kNoAllocMaxBlocks = 1184;
+constexpr uint32_t kNoAllocMaxK = 32767;
+static __device__ __align__(256) double g_ll_scratch[2 * kNoAllocMaxBlocks + kNoAllocMaxK + 2];
 
 // ---------------------------------------------------------------------------
 // alpha optimisation (optimizeParameters / calcDigammaSum, LDAModel.hpp:221-265)
@@ -1125,6 +1136,64 @@ tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
     out->sweep_kernel_ms = h->sweep_kernel_ms;
     out->sweeps_timed = h->sweeps_timed;
     return TMT_OK;
+}
+
+/* Allocation-free FP64 log-likelihood over caller-owned device counts.
+ * Host code may not pass g_ll_scratch itself (its host-side name is not a
+ * device address): the device address is looked up once per device with
+ * cudaGetSymbolAddress, with that device current, and reused. */
+tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, const int32_t* doc_len,
+                                 const float* alpha, const int32_t* n_kw, uint32_t V, const int32_t* n_k,
+                                 float eta, double* ll_out, void* stream, char* err, size_t err_len)
+{
+    auto say = [&](tmt_status st, const std::string& msg) {
+        if (err && err_len) {
+            const size_t n = std::min(err_len - 1, msg.size());
+            std::memcpy(err, msg.data(), n);
+            err[n] = '\0';
+        }
+        return st;
+    };
+    if (K == 0 || K > kNoAllocMaxK)
+        return say(TMT_ERR_INVALID_ARGUMENT, "K = " + std::to_string(K) + " is outside 1.." +
+                                                 std::to_string(kNoAllocMaxK) + ", the size of the static scratch");
+    if (!ll_out || !alpha || !n_k || (D && (!n_dk || !doc_len)) || (V && !n_kw))
+        return say(TMT_ERR_INVALID_ARGUMENT, "a required device pointer is NULL");
+    if (!(eta > 0)) return say(TMT_ERR_INVALID_ARGUMENT, "eta must be > 0");
+    static std::mutex mu;
+    static double* scratch[64] = {};
+    static int sms[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return say(TMT_ERR_UNSUPPORTED, "device ordinal above 63");
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!scratch[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_ll_scratch);
+            if (e != cudaSuccess)
+                return say(TMT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess)
+                return say(TMT_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
+            scratch[dev] = static_cast<double*>(p);
+        }
+    }
+    // the same grid as tmt_ll on this device, so both give the same sums
+    const uint32_t blocks = std::min<uint32_t>(kNoAllocMaxBlocks, (uint32_t)std::max(1, sms[dev] * 8));
+    double* partials = scratch[dev];                     // 2 * blocks, every slot overwritten
+    double* lg_alpha = partials + 2 * kNoAllocMaxBlocks; // K, every slot overwritten
+    double* asum = lg_alpha + kNoAllocMaxK;              // 2, overwritten
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double etad = (double)eta;
+    k_ll_prep<<<1, 256, 0, st>>>(alpha, K, lg_alpha, asum);
+    k_ll_partials<<<blocks, 256, 0, st>>>(n_dk, D, K, lg_alpha, alpha, doc_len, asum, n_kw, V, etad,
+                                          std::lgamma(etad), partials);
+    k_ll_final<<<1, 256, 0, st>>>(partials, blocks, n_k, K, (double)V * etad, ll_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return say(TMT_OK, "");
 }
 
 const char* tmt_last_error(const tmt_handle* h)
