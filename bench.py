@@ -291,7 +291,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
             "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1),
-                       "tokens": int(N), "alpha": ALPHA, "eta": ETA, "sweep_groups": max(1, args.groups), "parallelism": f"dp{world} (independent chains)",
+                       "tokens": int(N), "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups), "parallelism": f"dp{world} (independent chains)",
                        "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,

@@ -80,6 +80,7 @@ typedef struct tmt_info {
     uint64_t kernel_launches;/* kernels launched by this handle so far */
     double sweep_kernel_ms;  /* device time of the sweep kernels of the last tmt_train call */
     uint32_t sweeps_timed;   /* sweeps in that sum */
+    uint32_t sweep_groups;   /* document groups per sweep in use */
 } tmt_info;
 
 /* Replaces ILDAModel::create (LDAModel.cpp:10-13) + the LDAModel ctor checks

@@ -30,7 +30,7 @@ class TmtInfo(C.Structure):
     _fields_ = [("D", C.c_uint64), ("N_all", C.c_uint64), ("N", C.c_uint64), ("global_step", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("K", C.c_uint32), ("V", C.c_uint32), ("sampler", C.c_int32),
                 ("last_sweep_ms", C.c_float), ("kernel_launches", C.c_uint64),
-                ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32)]
+                ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32), ("sweep_groups", C.c_uint32)]
 
 
 class TmtSynthSpec(C.Structure):

@@ -1135,6 +1135,7 @@ tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
     out->kernel_launches = h->launches;
     out->sweep_kernel_ms = h->sweep_kernel_ms;
     out->sweeps_timed = h->sweeps_timed;
+    out->sweep_groups = h->groups;
     return TMT_OK;
 }
 
