@@ -117,6 +117,22 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
 /* Downloads n_dk (D x K row-major int32; DocumentLDA::numByTopic). */
 tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
 
+/* Replaces LDAModel::_infer<together = false> (LDAModel.hpp:920-953) behind
+ * TopicModel::infer (TopicModel.hpp:842-875): each of the D documents
+ * (doc-major ids in the model's vocabulary; ids >= V are carried but not
+ * sampled) gets a private copy of the handle's current model with its own
+ * tokens added, z0 ~ Discrete(alpha), then `iters` sequential Gibbs sweeps.
+ * Outputs (host, may be NULL): theta[D x K] = (n_dk + alpha) / (N_d +
+ * sum(alpha)) (_getTopicsByDoc, LDAModel.hpp:1145-1159) and ll[D] =
+ * LLRest(model + doc) - LLRest(model) + LLDocs(doc) in FP64.  Documents are
+ * sorted by id internally, as prepareDoc does.  Draws are keyed by seed and
+ * doc_keys[d] (NULL: key 0 for every document, as tomotopy starts every
+ * document's chain from a freshly seeded generator), so a document's result
+ * does not depend on the other documents of the call.  The model is not
+ * changed. */
+tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                           uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll);
+
 /* Host-side preparation of an integer-id corpus, replacing the vocabulary
  * part of LDAModel::prepare (LDAModel.hpp:1073-1138): removeStopwords
  * (TopicModel.hpp:526-571) reorders ids by (cf, df) descending with the

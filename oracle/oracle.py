@@ -70,7 +70,7 @@ def _load():
         "orc_ll_rest_f64": (C.c_double, [C.c_uint32, C.c_uint32, V, V, C.c_float]),
         "orc_optimize_alpha": (None, [C.c_uint64, C.c_uint32, V, V, V]),
         "orc_infer_doc": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, C.c_uint32,
-                                       C.c_uint32, C.c_uint64, C.c_uint64, V, V]),
+                                       C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -289,9 +289,13 @@ class Partition:
 
 
 def infer_doc(K, V, alpha, eta, nkw, nk, words, iters, seed, doc_key):
+    """Infer one document (ids sorted ascending) against a frozen model."""
     words = np.ascontiguousarray(words, dtype=np.uint32)
     z = np.zeros(max(len(words), 1), dtype=np.uint16)
     ndk = np.zeros(K, dtype=np.int32)
-    ll = lib.orc_infer_doc(K, V, _ptr(f32(alpha)), float(np.float32(eta)), _ptr(nkw), _ptr(nk),
-                           _ptr(words), len(words), iters, seed, doc_key, _ptr(z), _ptr(ndk))
-    return ll, z[:len(words)], ndk
+    theta = np.zeros(K, dtype=np.float32)
+    a = f32(np.broadcast_to(np.asarray(alpha, dtype=np.float32), (K,)).copy())
+    ll = lib.orc_infer_doc(K, V, _ptr(a), float(np.float32(eta)), _ptr(np.ascontiguousarray(nkw, np.int32)),
+                           _ptr(np.ascontiguousarray(nk, np.int32)), _ptr(words), len(words), iters, seed,
+                           doc_key, _ptr(z), _ptr(ndk), _ptr(theta))
+    return ll, z[:len(words)], ndk, theta

@@ -836,82 +836,105 @@ void orc_optimize_alpha(uint64_t D, uint32_t K, const int32_t* ndk, const int32_
 /* ------------------------------------------------------------------------ */
 /* Per-document infer (LDAModel.hpp:920-953)                                */
 /* ------------------------------------------------------------------------ */
+static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own, float u);
+
+/* The device's infer semantics for one (vid-sorted) document:
+ *   z0 ~ Discrete(alpha) (u = Philox(j, 0xFFFFFFFF, doc_key)), added to the doc's counts;
+ *   `iters` sweeps over the tokens in order; for token j of word v (own assignment removed):
+ *     A_k = (float)n_dk[k] + alpha_k
+ *     B_k = (float)(n_kw[k,v] + own[k]) + eta      own = the doc's other tokens of word v
+ *     R_k = 1 / ((float)(n_k[k] + n_dk[k]) + V*eta)
+ *     weight A_k * (B_k * R_k), drawn with blocked_draw (no own-topic term),
+ *     u = Philox(j, sweep, doc_key) under key seed ^ 'INFR';
+ *   theta_k = ((float)n_dk[k] + alpha_k) / ((float)N_d + sum(alpha))   (_getTopicsByDoc)
+ *   ll = LLRest(model + doc) - LLRest(model) + LLDocs(doc) in FP64 (only touched cells). */
 double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
                      const int32_t* nkw, const int32_t* nk,
                      const uint32_t* words, uint32_t len, uint32_t iters,
-                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk)
+                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk, float* theta)
 {
     float veta = eta * (float)V;
-    /* own[k, j] = count of this doc's tokens of word words[j] at topic k,
-     * kept per run of equal words (the doc is vid-sorted). */
-    int32_t* own = (int32_t*)calloc((size_t)len * K + 1, sizeof(int32_t));
-    int32_t* dnk = (int32_t*)calloc(K, sizeof(int32_t));
-    uint32_t* run0 = (uint32_t*)malloc((len + 1) * sizeof(uint32_t));
-    float* w = (float*)malloc(K * sizeof(float));
-    float* loc = (float*)malloc(K * sizeof(float));
-    float acum[32768];
+    uint64_t key = seed ^ (uint64_t)ORC_STREAM_INFER;
+    uint32_t klo = (uint32_t)doc_key, khi = (uint32_t)(doc_key >> 32);
+    int32_t* own = (int32_t*)calloc(K, sizeof(int32_t));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* BR = (float*)malloc(K * sizeof(float));
+    float* acum = (float*)malloc(K * sizeof(float));
     float s = 0.f;
     for (uint32_t k = 0; k < K; ++k) { s = s + alpha[k]; acum[k] = s; }
     memset(ndk, 0, K * sizeof(int32_t));
-    for (uint32_t j = 0; j < len; ++j)
-        run0[j] = (j && words[j] == words[j - 1]) ? run0[j - 1] : j;
-    /* initializeDocState<true>: z ~ Discrete(alpha), added to the private state */
     for (uint32_t j = 0; j < len; ++j) {
         if (words[j] >= V) { z[j] = 0xFFFF; continue; }
-        float u = orc_u01(philox_first(j, 0xFFFFFFFFu, (uint32_t)doc_key, (uint32_t)(doc_key >> 32),
-                                       seed ^ ORC_STREAM_INFER));
+        float u = orc_u01(philox_first(j, 0xFFFFFFFFu, klo, khi, key));
         uint16_t k = (uint16_t)orc_sample_acc(acum, K, u);
         z[j] = k;
         ndk[k]++;
-        own[(size_t)run0[j] * K + k]++;
     }
     for (uint32_t it = 0; it < iters; ++it) {
-        for (uint32_t j = 0; j < len; ++j) {
-            uint32_t v = words[j];
-            if (v >= V) continue;
-            uint16_t k0 = z[j];
-            int32_t* o = own + (size_t)run0[j] * K;
-            const int32_t* g = nkw + (size_t)v * K;
-            ndk[k0]--; o[k0]--;
-            for (uint32_t k = 0; k < K; ++k) {
-                float a = (float)ndk[k] + alpha[k];
-                float b = (float)(g[k] + o[k]) + eta;
-                float c = (float)(nk[k] + ndk[k]) + veta;
-                w[k] = (a * b) / c;
+        uint32_t rb = 0;
+        while (rb < len) {
+            uint32_t re = rb + 1;
+            while (re < len && words[re] == words[rb]) ++re;
+            uint32_t v = words[rb];
+            if (v < V) {
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+                const int32_t* g = nkw + (size_t)v * K;
+                for (uint32_t j = rb; j < re; ++j) {
+                    uint16_t zo = z[j];
+                    own[zo]--;
+                    ndk[zo]--;
+                    for (uint32_t k = 0; k < K; ++k) {
+                        A[k] = (float)ndk[k] + alpha[k];
+                        float B = (float)(g[k] + own[k]) + eta;
+                        float R = 1.0f / ((float)(nk[k] + ndk[k]) + veta);
+                        BR[k] = B * R;
+                    }
+                    float u = orc_u01(philox_first(j, it, klo, khi, key));
+                    uint16_t zn = (uint16_t)blocked_draw(A, BR, K, 0xFFFFFFFFu, 0.f, u);
+                    z[j] = zn;
+                    ndk[zn]++;
+                    own[zn]++;
+                }
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]--;
             }
-            float u = orc_u01(philox_first(j, it, (uint32_t)doc_key, (uint32_t)(doc_key >> 32),
-                                           seed ^ ORC_STREAM_INFER));
-            uint16_t k1 = (uint16_t)seg_scan_draw(w, K, u, loc);
-            z[j] = k1;
-            ndk[k1]++; o[k1]++;
+            rb = re;
         }
     }
-    /* ll = LLRest(tmp) - LLRest(global) + LLDocs(doc), FP64, only touched cells */
+    /* ll over touched cells, FP64 */
     double e = (double)eta, vd = (double)V * (double)eta, ll = 0, as = 0;
-    for (uint32_t k = 0; k < K; ++k) as += (double)alpha[k];
+    float asf = 0.f;
+    uint32_t n = 0;
+    for (uint32_t k = 0; k < K; ++k) { as += (double)alpha[k]; asf = asf + alpha[k]; }
+    for (uint32_t j = 0; j < len; ++j) n += words[j] < V;
     for (uint32_t k = 0; k < K; ++k) {
         if (!ndk[k]) continue;
         ll += lgamma((double)nk[k] + vd) - lgamma((double)(nk[k] + ndk[k]) + vd);
+        ll += lgamma((double)ndk[k] + alpha[k]) - lgamma((double)alpha[k]);
     }
-    for (uint32_t j = 0; j < len; ++j) {
-        if (words[j] >= V || run0[j] != j) continue;
-        const int32_t* o = own + (size_t)j * K;
-        const int32_t* g = nkw + (size_t)words[j] * K;
-        for (uint32_t k = 0; k < K; ++k) {
-            if (!o[k]) continue;
-            double after = lgamma((double)(g[k] + o[k]) + e) - lgamma(e);
-            double before = g[k] ? lgamma((double)g[k] + e) - lgamma(e) : 0.0;
-            ll += after - before;
+    ll -= lgamma((double)n + as) - lgamma(as);
+    uint32_t rb = 0;
+    while (rb < len) {
+        uint32_t re = rb + 1;
+        while (re < len && words[re] == words[rb]) ++re;
+        uint32_t v = words[rb];
+        if (v < V) {
+            const int32_t* g = nkw + (size_t)v * K;
+            for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+            for (uint32_t j = rb; j < re; ++j) {
+                uint32_t k = z[j];
+                int32_t c = own[k];
+                if (!c) continue;          /* cell already counted */
+                double after = lgamma((double)(g[k] + c) + e);
+                double before = g[k] ? lgamma((double)g[k] + e) : lgamma(e);
+                ll += after - before;
+                own[k] = 0;
+            }
         }
+        rb = re;
     }
-    uint32_t n = 0;
-    for (uint32_t j = 0; j < len; ++j) n += words[j] < V;
-    double ld = 0;
-    for (uint32_t k = 0; k < K; ++k)
-        if (ndk[k]) ld += lgamma((double)ndk[k] + alpha[k]) - lgamma((double)alpha[k]);
-    ld -= lgamma((double)n + as) - lgamma(as);
-    ll += ld;
-    free(own); free(dnk); free(run0); free(w); free(loc);
+    if (theta)
+        for (uint32_t k = 0; k < K; ++k) theta[k] = ((float)ndk[k] + alpha[k]) / ((float)n + asf);
+    free(own); free(A); free(BR); free(acum);
     return ll;
 }
 
@@ -979,7 +1002,7 @@ static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint3
             int64_t k = lane_topic(l, t, K);
             s = fmaf(A[k], phi[k], s);
         }
-        if (((zo >> 2) & 31) == l) {
+        if (zo < K && ((zo >> 2) & 31) == l) {
             float wu = A[zo] * phi[zo];
             float wo = A[zo] * phi_own;
             s = (s - wu) + wo;
@@ -1005,7 +1028,7 @@ static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint3
         for (uint32_t t = 0; t < 32; ++t) {
             if (m + t < n) {
                 int64_t k = lane_topic((uint32_t)h, m + t, K);
-                x[t] = A[k] * ((uint32_t)k == zo ? phi_own : phi[k]);
+                x[t] = A[k] * ((zo < K && (uint32_t)k == zo) ? phi_own : phi[k]);
             } else {
                 x[t] = 0.f;
             }

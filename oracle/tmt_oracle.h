@@ -161,14 +161,14 @@ void orc_optimize_alpha(uint64_t D, uint32_t K, const int32_t* ndk, const int32_
                         float* alpha);
 
 /* ---- per-document infer (together=False) -------------------------------- */
-/* Runs `iters` sequential Gibbs sweeps over one (prepared, vid-sorted) doc on
- * a private copy of the frozen model, as LDAModel::_infer does.  Draws come
- * from Philox stream INFER keyed by (seed, doc_key).  Writes the doc's topic
- * counts and returns ll = LLRest(tmp) - LLRest(global) + LLDocs(doc) in FP64. */
+/* The device infer semantics for one prepared (vid-sorted) document against
+ * a frozen model (LDAModel.hpp:920-953, _getTopicsByDoc :1145-1159): writes
+ * z, the doc's topic counts and theta (may be NULL); returns the FP64 ll =
+ * LLRest(model + doc) - LLRest(model) + LLDocs(doc). */
 double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
                      const int32_t* nkw, const int32_t* nk,
                      const uint32_t* words, uint32_t len, uint32_t iters,
-                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk_out);
+                     uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk_out, float* theta);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,7 @@ SIGNATURES = {
     "tmt_upload_corpus": (C.c_int, [_H, _P, _P, C.c_uint64, _P]),
     "tmt_train": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P]),
     "tmt_ll": (C.c_int, [_H, _P, _P]),
+    "tmt_infer_batch": (C.c_int, [_H, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P]),
     "tmt_download_state": (C.c_int, [_H, _P, _P, _P, _P]),
     "tmt_download_doc_topic": (C.c_int, [_H, _P]),
     "tmt_get_info": (C.c_int, [_H, C.POINTER(TmtInfo)]),

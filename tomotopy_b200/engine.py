@@ -58,6 +58,18 @@ class Engine:
         check(lib.tmt_train(self.h, int(iters), int(ll_every), _p(out) if n else None), self.h)
         return out[:n]
 
+    def infer(self, doc_off, words, iters=100, seed=0, doc_keys=None):
+        """tmt_infer_batch: returns (theta [D x K] float32, ll [D] float64)."""
+        doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        D = len(doc_off) - 1
+        theta = np.zeros((max(D, 1), self.K), dtype=np.float32)
+        ll = np.zeros(max(D, 1), dtype=np.float64)
+        keys = np.ascontiguousarray(doc_keys, dtype=np.uint64) if doc_keys is not None else None
+        check(lib.tmt_infer_batch(self.h, _p(words), _p(doc_off), D, int(iters), int(seed), _p(keys),
+                                  _p(theta), _p(ll)), self.h)
+        return theta[:D], ll[:D]
+
     def ll(self):
         a, b = C.c_double(), C.c_double()
         check(lib.tmt_ll(self.h, C.byref(a), C.byref(b)), self.h)
