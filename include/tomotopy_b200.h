@@ -133,6 +133,48 @@ tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
 tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
                            uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll);
 
+/* ---- served inference: continuous batching over resident frozen models ----
+ * No single tomotopy counterpart: it serves tomotopy's infer() (models.py:354,
+ * LDAModel.hpp:920-953) as a request loop.  A worker thread admits submitted
+ * documents into free slots of their model and into free space of the token
+ * arena (token_budget tokens: the HBM budget for documents in flight), and
+ * each step advances every active document by ceil(step_token_sweeps /
+ * length) sweeps on the device; requests that arrive while others run join
+ * at the next step.  A finished document's theta and ll are those of
+ * tmt_infer_batch for the same model, words, iters, seed and key, whatever
+ * else shares the GPU.  All functions are thread-safe. */
+typedef struct tmt_server tmt_server;
+typedef struct tmt_server_config {
+    int32_t device;
+    uint32_t max_slots;          /* documents in flight per model */
+    uint64_t token_budget;       /* tokens in flight over all models */
+    uint32_t step_token_sweeps;  /* work per document per step, in token-sweeps (0: 4096) */
+    uint32_t max_doc_len;        /* longer documents are rejected */
+} tmt_server_config;
+typedef struct tmt_server_stats {
+    uint64_t steps, completed, queued;
+    double mean_active;          /* documents per step, averaged over steps */
+    uint64_t tokens_in_flight_max;
+} tmt_server_stats;
+
+tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out);
+/* Makes a frozen model resident: host arrays n_kw (K x V column-major), n_k,
+ * alpha; returns its id.  Call before submitting to it. */
+tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
+                                const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id);
+/* Queues one document (ids in the model's vocabulary); returns at once. */
+tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* wid, uint32_t len, uint32_t iters,
+                             uint64_t seed, uint64_t key, uint64_t* request_id);
+/* Waits up to wait_ms for a finished document; TMT_ERR_TIMEOUT when none.
+ * theta gets the model's K values (theta_cap >= K); latency_ms is submit to
+ * completion. */
+tmt_status tmt_server_poll(tmt_server* s, uint32_t wait_ms, uint64_t* request_id, uint32_t* model_id,
+                           float* theta, uint32_t theta_cap, double* ll, double* latency_ms);
+tmt_status tmt_server_get_stats(tmt_server* s, tmt_server_stats* out);
+const char* tmt_server_last_error(const tmt_server* s);
+/* Stops the worker (queued and running documents are dropped) and frees the server. */
+tmt_status tmt_server_stop(tmt_server* s);
+
 /* Host-side preparation of an integer-id corpus, replacing the vocabulary
  * part of LDAModel::prepare (LDAModel.hpp:1073-1138): removeStopwords
  * (TopicModel.hpp:526-571) reorders ids by (cf, df) descending with the

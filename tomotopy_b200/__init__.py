@@ -1,5 +1,5 @@
 """tomotopy_b200 -- tomotopy's LDA collapsed-Gibbs path on NVIDIA B200 (sm_100a)."""
 from ._lib import lib as _native, TmtError  # noqa: F401  (loads the CUDA library or raises)
-from .engine import Engine, synth_corpus, prepare_ids  # noqa: F401
+from .engine import Engine, Server, synth_corpus, prepare_ids  # noqa: F401
 
 __version__ = "0.1.0"

@@ -33,6 +33,16 @@ class TmtInfo(C.Structure):
                 ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32), ("sweep_groups", C.c_uint32)]
 
 
+class TmtServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_slots", C.c_uint32), ("token_budget", C.c_uint64),
+                ("step_token_sweeps", C.c_uint32), ("max_doc_len", C.c_uint32)]
+
+
+class TmtServerStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("completed", C.c_uint64), ("queued", C.c_uint64),
+                ("mean_active", C.c_double), ("tokens_in_flight_max", C.c_uint64)]
+
+
 class TmtSynthSpec(C.Structure):
     _fields_ = [("V", C.c_uint32), ("T", C.c_uint32), ("D", C.c_uint64), ("len_kind", C.c_int32),
                 ("len_a", C.c_double), ("len_b", C.c_double), ("len_min", C.c_uint32), ("len_max", C.c_uint32),
@@ -57,6 +67,15 @@ SIGNATURES = {
                                      _P, _P, _P, _P, _P, C.POINTER(C.c_uint32)]),
     "tmt_ll_counts_noalloc": (C.c_int, [_P, C.c_uint64, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_float, _P, _P,
                                         C.c_char_p, C.c_size_t]),
+    "tmt_server_start": (C.c_int, [C.POINTER(TmtServerConfig), C.POINTER(_H)]),
+    "tmt_server_add_model": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P, C.c_float, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_server_submit": (C.c_int, [_H, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64,
+                                    C.POINTER(C.c_uint64)]),
+    "tmt_server_poll": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), _P, C.c_uint32,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "tmt_server_get_stats": (C.c_int, [_H, C.POINTER(TmtServerStats)]),
+    "tmt_server_last_error": (C.c_char_p, [_H]),
+    "tmt_server_stop": (C.c_int, [_H]),
     "tmt_synth_corpus": (C.c_int, [C.POINTER(TmtSynthSpec), _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 

@@ -32,11 +32,13 @@
 #include <mutex>
 #include "philox.cuh"
 #include "special.cuh"
+#include "common.cuh"
+#include "infer.cuh"
 #include "../../include/tomotopy_b200.h"
 
 namespace {
 
-constexpr unsigned FULL = 0xFFFFFFFFu;
+using namespace tmtk;
 constexpr int kSweepWarps = 8;           // warps per sweep block
 
 
@@ -145,27 +147,10 @@ struct SweepArgs {
     uint32_t dnk_smem;       // 1: n_k deltas aggregate in shared memory
 };
 
-__device__ __forceinline__ float hs_scan32(float x, int lane)
-{
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const float y = __shfl_up_sync(FULL, x, off);
-        if (lane >= off) x = __fadd_rn(x, y);
-    }
-    return x;
-}
-
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
 // aligned regions): [n_k deltas: KP ints] [per warp: (float)n_dk + alpha, KP
 // floats, zero padded] [per warp: n_dk, KP ints].
-__host__ __device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
 
-__device__ __forceinline__ double warp_sum(double x)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
-    return x;
-}
 
 
 // Topics are dealt to lanes in blocks of four: lane l owns k = 128*j + 4*l + i.
@@ -371,251 +356,6 @@ k_sweep_doc(SweepArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// inference: per-document Gibbs chains against a frozen model
-// ---------------------------------------------------------------------------
-// tomotopy's _infer<together = false> (LDAModel.hpp:920-953): each document
-// gets a private copy of the model with its own tokens added, z0 ~
-// Discrete(alpha), then `iters` sequential sweeps.  Only the document's
-// cells differ from the frozen model, so the warp keeps them on chip:
-//   A_k = (float)n_dk[k] + alpha_k, R_k = 1 / ((float)(n_k[k] + n_dk[k]) + V*eta),
-//   B_k = (float)(n_kw[k,v] + own[k]) + eta (own: the doc's other tokens of word v),
-//   weight A_k * (B_k * R_k), the blocked two-pass draw of the training sweep.
-// Documents must be sorted by word id (prepareDoc does this): tokens of a
-// word form one run, whose topic histogram is `own`.
-struct InferArgs {
-    const uint64_t* doc_off;
-    const uint32_t* words;
-    uint16_t* z;
-    const int32_t* nkw;
-    const int32_t* nk;
-    const float* alpha;
-    const float* acum;
-    const uint64_t* doc_keys;   // NULL: every document uses key 0
-    float* theta;               // D x K or NULL
-    double* ll;                 // D or NULL
-    int32_t* ndk_out;           // D x K or NULL
-    uint32_t* counter;
-    uint64_t D;
-    uint32_t K, V, iters;
-    float eta, veta, asum_f;
-    double veta_d, asum_d, lg_asum, lg_eta;
-    uint64_t key;               // seed ^ 'INFR'
-};
-
-template <int CH>
-__global__ void __launch_bounds__(256)
-k_infer_docs(InferArgs a)
-{
-    constexpr int CHR = CH > 0 ? CH : 1;
-    extern __shared__ __align__(16) int smem[];
-    const int K = (int)a.K;
-    const int KP = (int)round4(a.K);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int* rowi = smem + warp * 4 * KP;
-    float* rowf = reinterpret_cast<float*>(rowi + KP);
-    float* rr = rowf + KP;
-    int* own = reinterpret_cast<int*>(rr + KP);
-    const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
-    const float eta = a.eta, veta = a.veta;
-
-    for (;;) {
-        uint32_t q = 0;
-        if (lane == 0) q = atomicAdd(a.counter, 1u);
-        q = __shfl_sync(FULL, q, 0);
-        if (q >= a.D) break;
-        const uint64_t d = q;
-        const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
-        const uint32_t L = (uint32_t)(e - b);
-        const uint64_t dk = a.doc_keys ? a.doc_keys[d] : 0;
-        const uint32_t klo = (uint32_t)dk, khi = (uint32_t)(dk >> 32);
-        for (int k = lane; k < KP; k += 32) { rowi[k] = 0; own[k] = 0; }
-        __syncwarp();
-        // z0 ~ Discrete(alpha)
-        int nvalid = 0;
-        for (uint32_t j = lane; j < L; j += 32) {
-            const uint32_t w = a.words[b + j];
-            uint16_t zz = 0xFFFF;
-            if (w < a.V) {
-                const float u = tmt::u01(tmt::philox_u32(j, 0xFFFFFFFFu, klo, khi, a.key));
-                const float r = __fmul_rn(u, a.acum[K - 1]);
-                uint32_t lo = 0, hi = K - 1;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (r < a.acum[mid]) hi = mid; else lo = mid + 1;
-                }
-                zz = (uint16_t)lo;
-                atomicAdd(&rowi[lo], 1);
-                ++nvalid;
-            }
-            a.z[b + j] = zz;
-        }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) nvalid += __shfl_xor_sync(FULL, nvalid, o);
-        __syncwarp();
-        for (int k = lane; k < KP; k += 32) {
-            float f = 0.f, g = 0.f;
-            if (k < K) {
-                const int n = rowi[k];
-                f = __fadd_rn((float)n, __ldg(a.alpha + k));
-                g = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + k) + n), veta));
-            }
-            rowf[k] = f;
-            rr[k] = g;
-        }
-        __syncwarp();
-        for (uint32_t it = 0; it < a.iters; ++it) {
-            uint32_t rb = 0;
-            while (rb < L) {
-                const uint32_t v = a.words[b + rb];
-                // end of the run of word v
-                uint32_t re = rb + 1;
-                for (;;) {
-                    const uint32_t j = re + lane;
-                    const bool diff = j >= L || a.words[b + j] != v;
-                    const unsigned mm = __ballot_sync(FULL, diff);
-                    if (mm) { re += __ffs(mm) - 1; break; }
-                    re += 32;
-                }
-                if (v < a.V) {
-                    for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
-                    __syncwarp();
-                    const int32_t* gcol = a.nkw + (uint64_t)v * K;
-                    for (uint32_t j = rb; j < re; ++j) {
-                        const int zo = a.z[b + j];
-                        if (lane == 0) {
-                            own[zo] -= 1;
-                            const int n = rowi[zo] - 1;
-                            rowi[zo] = n;
-                            rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
-                            rr[zo] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + zo) + n), veta));
-                        }
-                        __syncwarp();
-                        // pass 1
-                        float s = 0.f;
-#pragma unroll
-                        for (int jj = 0; jj < CHR; ++jj) {
-                            if (CH > 0 ? jj < nch : false) {
-                                const int k0 = 128 * jj + 4 * lane;
-                                const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
-                                const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
-                                const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
-                                int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
-                                if (k0 + 3 < K) {
-                                    g0 = __ldg(gcol + k0); g1 = __ldg(gcol + k0 + 1);
-                                    g2 = __ldg(gcol + k0 + 2); g3 = __ldg(gcol + k0 + 3);
-                                } else {
-                                    g0 = __ldg(gcol + k0);
-                                    if (k0 + 1 < K) g1 = __ldg(gcol + k0 + 1);
-                                    if (k0 + 2 < K) g2 = __ldg(gcol + k0 + 2);
-                                }
-                                s = __fmaf_rn(A4.x, __fmul_rn(__fadd_rn((float)(g0 + O4.x), eta), R4.x), s);
-                                s = __fmaf_rn(A4.y, __fmul_rn(__fadd_rn((float)(g1 + O4.y), eta), R4.y), s);
-                                s = __fmaf_rn(A4.z, __fmul_rn(__fadd_rn((float)(g2 + O4.z), eta), R4.z), s);
-                                s = __fmaf_rn(A4.w, __fmul_rn(__fadd_rn((float)(g3 + O4.w), eta), R4.w), s);
-                            }
-                        }
-                        if (CH == 0) {
-                            for (int jj = 0; jj < nch; ++jj) {
-                                for (int i = 0; i < 4; ++i) {
-                                    const int k = 128 * jj + 4 * lane + i;
-                                    if (k < K)
-                                        s = __fmaf_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]), s);
-                                }
-                            }
-                        }
-                        const float x = hs_scan32(s, lane);
-                        float E = __shfl_up_sync(FULL, x, 1);
-                        if (lane == 0) E = 0.f;
-                        const float total = __shfl_sync(FULL, x, 31);
-                        const float u = tmt::u01(tmt::philox_u32(j, it, klo, khi, a.key));
-                        const float r = __fmul_rn(u, total);
-                        const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
-                        int znew = K - 1;
-                        if (m) {
-                            const int h = __ffs(m) - 1;
-                            const float Eh = __shfl_sync(FULL, E, h);
-                            const int mh = K - 4 * h;
-                            const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
-                            float carry = 0.f;
-                            int found = nh - 1;
-                            for (int mm = 0; mm < nh; mm += 32) {
-                                const int t = mm + lane;
-                                const int k = 128 * (t >> 2) + 4 * h + (t & 3);
-                                float x2 = 0.f;
-                                if (t < nh)
-                                    x2 = __fmul_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]));
-                                x2 = hs_scan32(x2, lane);
-                                const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
-                                if (mb) { found = mm + __ffs(mb) - 1; break; }
-                                carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
-                            }
-                            znew = 128 * (found >> 2) + 4 * h + (found & 3);
-                        }
-                        __syncwarp();
-                        if (lane == 0) {
-                            own[znew] += 1;
-                            const int n = rowi[znew] + 1;
-                            rowi[znew] = n;
-                            rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
-                            rr[znew] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + znew) + n), veta));
-                            a.z[b + j] = (uint16_t)znew;
-                        }
-                        __syncwarp();
-                    }
-                    for (uint32_t j = rb + lane; j < re; j += 32) atomicSub(&own[a.z[b + j]], 1);
-                    __syncwarp();
-                }
-                rb = re;
-            }
-        }
-        // outputs: theta, counts, FP64 ll over the touched cells
-        double acc = 0;
-        const float denom = __fadd_rn((float)nvalid, a.asum_f);
-        for (int k = lane; k < K; k += 32) {
-            const int n = rowi[k];
-            if (a.theta) a.theta[d * K + k] = __fdiv_rn(__fadd_rn((float)n, __ldg(a.alpha + k)), denom);
-            if (a.ndk_out) a.ndk_out[d * K + k] = n;
-            if (n) {
-                const double gk = (double)__ldg(a.nk + k);
-                acc += lgamma(gk + a.veta_d) - lgamma(gk + (double)n + a.veta_d);
-                const double al = (double)__ldg(a.alpha + k);
-                acc += lgamma((double)n + al) - lgamma(al);
-            }
-        }
-        // word cells: per run, each distinct topic once
-        uint32_t rb = 0;
-        while (rb < L) {
-            const uint32_t v = a.words[b + rb];
-            uint32_t re = rb + 1;
-            for (;;) {
-                const uint32_t j = re + lane;
-                const bool diff = j >= L || a.words[b + j] != v;
-                const unsigned mm = __ballot_sync(FULL, diff);
-                if (mm) { re += __ffs(mm) - 1; break; }
-                re += 32;
-            }
-            if (v < a.V) {
-                for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
-                __syncwarp();
-                for (uint32_t j = rb + lane; j < re; j += 32) {
-                    const int k = a.z[b + j];
-                    const int c = atomicExch(&own[k], 0);
-                    if (c) {
-                        const int gk = __ldg(a.nkw + (uint64_t)v * K + k);
-                        acc += lgamma((double)(gk + c) + (double)a.eta) - (gk ? lgamma((double)gk + (double)a.eta) : a.lg_eta);
-                    }
-                }
-                __syncwarp();
-            }
-            rb = re;
-        }
-        acc = warp_sum(acc);
-        if (lane == 0 && a.ll) a.ll[d] = acc - (lgamma((double)nvalid + a.asum_d) - a.lg_asum);
-        __syncwarp();
-    }
-}
-
-// ---------------------------------------------------------------------------
 // log-likelihood in FP64 (getLLDocs / getLLRest, LDAModel.hpp:616-668)
 // ---------------------------------------------------------------------------
 
@@ -788,26 +528,6 @@ __global__ void k_sum_alpha(const float* __restrict__ alpha, uint32_t K, float* 
         *out = s;
     }
 }
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct ArgError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct OomError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct StateError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess)                                                                \
-            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));              \
-    } while (0)
 
 } // namespace
 
@@ -1118,45 +838,6 @@ void validate_config(const tmt_config& c)
 } // namespace
 
 // ---------------------------------------------------------------------------
-// inference launch
-// ---------------------------------------------------------------------------
-uint32_t infer_warps(uint32_t K)
-{
-    const uint32_t per_warp = 16 * round4(K);
-    const uint32_t budget = 200 * 1024;
-    return std::max(0u, std::min(8u, budget / per_warp));
-}
-
-template <int CH>
-void launch_infer_t(tmt_handle* h, const InferArgs& a, uint32_t warps)
-{
-    auto kern = k_infer_docs<CH>;
-    const uint32_t smem = warps * 16 * round4(a.K);
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem));
-    if (per_sm < 1) throw CudaError("infer kernel does not fit on an SM");
-    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms, (a.D + warps - 1) / warps);
-    if (grid == 0) grid = 1;
-    kern<<<grid, warps * 32, smem, h->stream>>>(a);
-    launch_check(h);
-}
-
-void launch_infer(tmt_handle* h, const InferArgs& a)
-{
-    const uint32_t warps = infer_warps(a.K);
-    if (warps == 0) throw ArgError("K too large for on-chip inference state");
-    const uint32_t ch = (round4(a.K) + 127) / 128;
-    if (ch <= 1) launch_infer_t<1>(h, a, warps);
-    else if (ch <= 2) launch_infer_t<2>(h, a, warps);
-    else if (ch <= 4) launch_infer_t<4>(h, a, warps);
-    else if (ch <= 8) launch_infer_t<8>(h, a, warps);
-    else if (ch <= 16) launch_infer_t<16>(h, a, warps);
-    else if (ch <= 32) launch_infer_t<32>(h, a, warps);
-    else launch_infer_t<0>(h, a, warps);
-}
-
-// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -1449,6 +1130,7 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         for (uint64_t d = 0; d < D; ++d)
             if (doc_off[d + 1] < doc_off[d]) throw ArgError("doc_off is not non-decreasing");
         if (infer_warps(h->cfg.K) == 0) throw ArgError("K too large for inference");
+        if (D >= 0xFFFFFFFFull) throw ArgError("too many documents");
         if (D == 0) return;
         const uint32_t K = h->cfg.K;
         // documents sorted by word id, as prepareDoc does (LDAModel.hpp:716-722)
@@ -1489,22 +1171,12 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         CK(cudaMemcpyAsync(B.acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(B.counter, 0, sizeof(uint32_t), st));
         InferArgs a{};
-        a.doc_off = B.doc_off;
-        a.words = B.words;
-        a.z = B.z;
         a.nkw = h->d_nkw[h->cur];
         a.nk = h->d_nk[h->cur];
         a.alpha = h->d_alpha;
         a.acum = B.acum;
-        a.doc_keys = doc_keys ? B.keys : nullptr;
-        a.theta = B.theta;
-        a.ll = B.ll;
-        a.ndk_out = nullptr;
-        a.counter = B.counter;
-        a.D = D;
         a.K = K;
         a.V = h->cfg.V;
-        a.iters = iters;
         a.eta = h->cfg.eta;
         a.veta = h->cfg.eta * (float)h->cfg.V;
         a.asum_f = sf;
@@ -1513,7 +1185,23 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         a.lg_asum = std::lgamma(sd);
         a.lg_eta = std::lgamma((double)h->cfg.eta);
         a.key = seed ^ (uint64_t)tmt::kStreamInfer;
-        launch_infer(h, a);
+        a.words = B.words;
+        a.z = B.z;
+        a.tok_begin = B.doc_off;          // slot d = document d: tokens [doc_off[d], doc_off[d+1])
+        a.tok_len = nullptr;
+        a.keys = doc_keys ? B.keys : nullptr;
+        a.it_begin = a.it_end = a.it_total = nullptr;
+        a.u_begin = 0;
+        a.u_end = iters;
+        a.u_total = iters;
+        a.ndk = nullptr;
+        a.theta = B.theta;
+        a.ll = B.ll;
+        a.work = nullptr;
+        a.n_work = (uint32_t)D;
+        a.counter = B.counter;
+        launch_infer(a, h->num_sms, h->stream);
+        ++h->launches;
         if (theta) CK(cudaMemcpyAsync(theta, B.theta, D * (uint64_t)K * sizeof(float), cudaMemcpyDeviceToHost, st));
         if (ll) CK(cudaMemcpyAsync(ll, B.ll, D * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

@@ -1,0 +1,313 @@
+// infer.cuh -- inference of unseen documents against a frozen model:
+// tomotopy's LDAModel::_infer<together = false> (LDAModel.hpp:920-953).
+//
+// Each document gets a private copy of the model with its own tokens added,
+// z0 ~ Discrete(alpha), then sequential Gibbs sweeps.  Only the document's
+// cells differ from the frozen model, so one warp keeps them on chip:
+//   A_k = (float)n_dk[k] + alpha_k
+//   R_k = 1 / ((float)(n_k[k] + n_dk[k]) + V*eta)
+//   B_k = (float)(n_kw[k,v] + own[k]) + eta   (own: the document's other tokens of word v)
+//   weight A_k * (B_k * R_k), drawn with the blocked two-pass draw of the training sweep.
+// Documents are sorted by word id (prepareDoc, LDAModel.hpp:716-722), so the
+// tokens of one word form a run and `own` is that run's topic histogram.
+//
+// The kernel works on "slots" and is resumable: one launch advances each
+// listed slot through sweeps [it_begin, it_end); z and n_dk persist in device
+// memory between launches.  Draws use the absolute (token, sweep) counter, so
+// a document's result does not depend on how its sweeps are split across
+// launches or on which other documents share them.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include "common.cuh"
+#include "philox.cuh"
+
+namespace tmtk {
+
+struct InferArgs {
+    // frozen model
+    const int32_t* nkw;          // K x V column-major
+    const int32_t* nk;
+    const float* alpha;
+    const float* acum;           // sequential float cumsum of alpha
+    uint32_t K, V;
+    float eta, veta, asum_f;
+    double veta_d, asum_d, lg_asum, lg_eta;
+    uint64_t key;                // seed ^ 'INFR'
+    // tokens, addressed by the slots
+    const uint32_t* words;       // sorted within each document
+    uint16_t* z;
+    // slots
+    const uint64_t* tok_begin;   // first token of each slot; with tok_len == NULL, tok_begin[s+1] ends slot s
+    const uint32_t* tok_len;
+    const uint64_t* keys;        // per-slot draw key; NULL: 0
+    const uint32_t* it_begin;    // per-slot sweep range of this launch; NULL: the uniform values below
+    const uint32_t* it_end;
+    const uint32_t* it_total;
+    uint32_t u_begin, u_end, u_total;
+    int32_t* ndk;                // slot x K counts kept between launches; NULL when every slot finishes here
+    float* theta;                // slot x K, written when a slot finishes (may be NULL)
+    double* ll;                  // slot, written when a slot finishes (may be NULL)
+    const uint32_t* work;        // slots advanced by this launch; NULL: 0 .. n_work-1
+    uint32_t n_work;
+    uint32_t* counter;           // zeroed before the launch
+};
+
+template <int CH>
+__global__ void __launch_bounds__(256)
+k_infer_slots(InferArgs a)
+{
+    constexpr int CHR = CH > 0 ? CH : 1;
+    extern __shared__ __align__(16) int smem[];
+    const int K = (int)a.K;
+    const int KP = (int)round4(a.K);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* rowi = smem + warp * 4 * KP;
+    float* rowf = reinterpret_cast<float*>(rowi + KP);
+    float* rr = rowf + KP;
+    int* own = reinterpret_cast<int*>(rr + KP);
+    const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
+    const float eta = a.eta, veta = a.veta;
+
+    for (;;) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(a.counter, 1u);
+        q = __shfl_sync(FULL, q, 0);
+        if (q >= a.n_work) break;
+        const uint32_t sl = a.work ? a.work[q] : q;
+        const uint64_t b = a.tok_begin[sl];
+        const uint32_t L = a.tok_len ? a.tok_len[sl] : (uint32_t)(a.tok_begin[sl + 1] - b);
+        const uint64_t dk = a.keys ? a.keys[sl] : 0;
+        const uint32_t klo = (uint32_t)dk, khi = (uint32_t)(dk >> 32);
+        const uint32_t it0 = a.it_begin ? a.it_begin[sl] : a.u_begin;
+        const uint32_t it1 = a.it_end ? a.it_end[sl] : a.u_end;
+        const uint32_t itT = a.it_total ? a.it_total[sl] : a.u_total;
+        for (int k = lane; k < KP; k += 32) own[k] = 0;
+        int nvalid = 0;
+        if (it0 == 0) {
+            // z0 ~ Discrete(alpha), added to the document's counts
+            for (int k = lane; k < KP; k += 32) rowi[k] = 0;
+            __syncwarp();
+            for (uint32_t j = lane; j < L; j += 32) {
+                const uint32_t w = a.words[b + j];
+                uint16_t zz = 0xFFFF;
+                if (w < a.V) {
+                    const float u = tmt::u01(tmt::philox_u32(j, 0xFFFFFFFFu, klo, khi, a.key));
+                    const float r = __fmul_rn(u, a.acum[K - 1]);
+                    uint32_t lo = 0, hi = K - 1;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (r < a.acum[mid]) hi = mid; else lo = mid + 1;
+                    }
+                    zz = (uint16_t)lo;
+                    atomicAdd(&rowi[lo], 1);
+                    ++nvalid;
+                }
+                a.z[b + j] = zz;
+            }
+        } else {
+            for (int k = lane; k < KP; k += 32) rowi[k] = k < K ? a.ndk[(uint64_t)sl * K + k] : 0;
+            for (uint32_t j = lane; j < L; j += 32) nvalid += a.words[b + j] < a.V;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) nvalid += __shfl_xor_sync(FULL, nvalid, o);
+        __syncwarp();
+        for (int k = lane; k < KP; k += 32) {
+            float f = 0.f, g = 0.f;
+            if (k < K) {
+                const int n = rowi[k];
+                f = __fadd_rn((float)n, __ldg(a.alpha + k));
+                g = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + k) + n), veta));
+            }
+            rowf[k] = f;
+            rr[k] = g;
+        }
+        __syncwarp();
+        for (uint32_t it = it0; it < it1; ++it) {
+            uint32_t rb = 0;
+            while (rb < L) {
+                const uint32_t v = a.words[b + rb];
+                uint32_t re = rb + 1;          // end of the run of word v
+                for (;;) {
+                    const uint32_t j = re + lane;
+                    const bool diff = j >= L || a.words[b + j] != v;
+                    const unsigned mm = __ballot_sync(FULL, diff);
+                    if (mm) { re += __ffs(mm) - 1; break; }
+                    re += 32;
+                }
+                if (v < a.V) {
+                    for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
+                    __syncwarp();
+                    const int32_t* gcol = a.nkw + (uint64_t)v * K;
+                    for (uint32_t j = rb; j < re; ++j) {
+                        const int zo = a.z[b + j];
+                        if (lane == 0) {
+                            own[zo] -= 1;
+                            const int n = rowi[zo] - 1;
+                            rowi[zo] = n;
+                            rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
+                            rr[zo] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + zo) + n), veta));
+                        }
+                        __syncwarp();
+                        // pass 1: fma chain over this lane's topics
+                        float s = 0.f;
+                        if (CH > 0) {
+#pragma unroll
+                            for (int jj = 0; jj < CHR; ++jj) {
+                                if (jj < nch) {
+                                    const int k0 = 128 * jj + 4 * lane;
+                                    const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
+                                    const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
+                                    const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
+                                    int g0 = __ldg(gcol + k0), g1 = 0, g2 = 0, g3 = 0;
+                                    if (k0 + 1 < K) g1 = __ldg(gcol + k0 + 1);
+                                    if (k0 + 2 < K) g2 = __ldg(gcol + k0 + 2);
+                                    if (k0 + 3 < K) g3 = __ldg(gcol + k0 + 3);
+                                    s = __fmaf_rn(A4.x, __fmul_rn(__fadd_rn((float)(g0 + O4.x), eta), R4.x), s);
+                                    s = __fmaf_rn(A4.y, __fmul_rn(__fadd_rn((float)(g1 + O4.y), eta), R4.y), s);
+                                    s = __fmaf_rn(A4.z, __fmul_rn(__fadd_rn((float)(g2 + O4.z), eta), R4.z), s);
+                                    s = __fmaf_rn(A4.w, __fmul_rn(__fadd_rn((float)(g3 + O4.w), eta), R4.w), s);
+                                }
+                            }
+                        } else {
+                            for (int jj = 0; jj < nch; ++jj)
+                                for (int i = 0; i < 4; ++i) {
+                                    const int k = 128 * jj + 4 * lane + i;
+                                    if (k < K)
+                                        s = __fmaf_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]), s);
+                                }
+                        }
+                        const float x = hs_scan32(s, lane);
+                        float E = __shfl_up_sync(FULL, x, 1);
+                        if (lane == 0) E = 0.f;
+                        const float total = __shfl_sync(FULL, x, 31);
+                        const float u = tmt::u01(tmt::philox_u32(j, it, klo, khi, a.key));
+                        const float r = __fmul_rn(u, total);
+                        const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
+                        int znew = K - 1;
+                        if (m) {
+                            // pass 2: position among lane h's topics, 32 at a time
+                            const int h = __ffs(m) - 1;
+                            const float Eh = __shfl_sync(FULL, E, h);
+                            const int mh = K - 4 * h;
+                            const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
+                            float carry = 0.f;
+                            int found = nh - 1;
+                            for (int mm = 0; mm < nh; mm += 32) {
+                                const int t = mm + lane;
+                                const int k = 128 * (t >> 2) + 4 * h + (t & 3);
+                                float x2 = 0.f;
+                                if (t < nh)
+                                    x2 = __fmul_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]));
+                                x2 = hs_scan32(x2, lane);
+                                const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
+                                if (mb) { found = mm + __ffs(mb) - 1; break; }
+                                carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                            }
+                            znew = 128 * (found >> 2) + 4 * h + (found & 3);
+                        }
+                        __syncwarp();
+                        if (lane == 0) {
+                            own[znew] += 1;
+                            const int n = rowi[znew] + 1;
+                            rowi[znew] = n;
+                            rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
+                            rr[znew] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + znew) + n), veta));
+                            a.z[b + j] = (uint16_t)znew;
+                        }
+                        __syncwarp();
+                    }
+                    for (uint32_t j = rb + lane; j < re; j += 32) atomicSub(&own[a.z[b + j]], 1);
+                    __syncwarp();
+                }
+                rb = re;
+            }
+        }
+        if (it1 < itT) {            // keep the document's counts for the next launch
+            for (int k = lane; k < K; k += 32) a.ndk[(uint64_t)sl * K + k] = rowi[k];
+            __syncwarp();
+            continue;
+        }
+        // finished: theta, FP64 ll over the touched cells
+        double acc = 0;
+        const float denom = __fadd_rn((float)nvalid, a.asum_f);
+        for (int k = lane; k < K; k += 32) {
+            const int n = rowi[k];
+            if (a.theta) a.theta[(uint64_t)sl * K + k] = __fdiv_rn(__fadd_rn((float)n, __ldg(a.alpha + k)), denom);
+            if (n) {
+                const double gk = (double)__ldg(a.nk + k);
+                acc += lgamma(gk + a.veta_d) - lgamma(gk + (double)n + a.veta_d);
+                const double al = (double)__ldg(a.alpha + k);
+                acc += lgamma((double)n + al) - lgamma(al);
+            }
+        }
+        uint32_t rb = 0;
+        while (rb < L) {            // word cells: per run, each distinct topic once
+            const uint32_t v = a.words[b + rb];
+            uint32_t re = rb + 1;
+            for (;;) {
+                const uint32_t j = re + lane;
+                const bool diff = j >= L || a.words[b + j] != v;
+                const unsigned mm = __ballot_sync(FULL, diff);
+                if (mm) { re += __ffs(mm) - 1; break; }
+                re += 32;
+            }
+            if (v < a.V) {
+                for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
+                __syncwarp();
+                for (uint32_t j = rb + lane; j < re; j += 32) {
+                    const int k = a.z[b + j];
+                    const int c = atomicExch(&own[k], 0);
+                    if (c) {
+                        const int gk = __ldg(a.nkw + (uint64_t)v * K + k);
+                        acc += lgamma((double)(gk + c) + (double)a.eta) - (gk ? lgamma((double)gk + (double)a.eta) : a.lg_eta);
+                    }
+                }
+                __syncwarp();
+            }
+            rb = re;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0 && a.ll) a.ll[sl] = acc - (lgamma((double)nvalid + a.asum_d) - a.lg_asum);
+        __syncwarp();
+    }
+}
+
+// warps per block so that 16 * KP bytes of state per warp fit in 200 KB; 0: too large
+inline uint32_t infer_warps(uint32_t K)
+{
+    const uint32_t per_warp = 16 * round4(K);
+    return std::min(8u, (200u * 1024u) / per_warp);
+}
+
+template <int CH>
+inline void launch_infer_t(const InferArgs& a, uint32_t warps, int num_sms, cudaStream_t st)
+{
+    auto kern = k_infer_slots<CH>;
+    const uint32_t smem = warps * 16 * round4(a.K);
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem));
+    if (per_sm < 1) throw CudaError("infer kernel does not fit on an SM");
+    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * num_sms, (a.n_work + warps - 1) / warps);
+    if (grid == 0) grid = 1;
+    kern<<<grid, warps * 32, smem, st>>>(a);
+    CK(cudaGetLastError());
+}
+
+// One launch of the slot kernel for this K (the counter must be zeroed first).
+inline void launch_infer(const InferArgs& a, int num_sms, cudaStream_t st)
+{
+    const uint32_t warps = infer_warps(a.K);
+    if (warps == 0) throw ArgError("K too large for on-chip inference state");
+    const uint32_t ch = (round4(a.K) + 127) / 128;
+    if (ch <= 1) launch_infer_t<1>(a, warps, num_sms, st);
+    else if (ch <= 2) launch_infer_t<2>(a, warps, num_sms, st);
+    else if (ch <= 4) launch_infer_t<4>(a, warps, num_sms, st);
+    else if (ch <= 8) launch_infer_t<8>(a, warps, num_sms, st);
+    else if (ch <= 16) launch_infer_t<16>(a, warps, num_sms, st);
+    else if (ch <= 32) launch_infer_t<32>(a, warps, num_sms, st);
+    else launch_infer_t<0>(a, warps, num_sms, st);
+}
+
+} // namespace tmtk

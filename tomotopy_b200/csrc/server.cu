@@ -1,0 +1,513 @@
+// server.cu -- continuous-batching inference over frozen models resident on
+// one GPU (tmt_server_* in include/tomotopy_b200.h).
+//
+// A worker thread runs steps.  Each step it admits queued requests into free
+// slots of their model's slot pool and into free space of the shared token
+// arena (the HBM budget for documents in flight), then launches the
+// resumable inference kernel (infer.cuh) once per model with active slots,
+// advancing every active document by ceil(step_token_sweeps / length) sweeps
+// (at least one), so long documents do not stall a step.  Documents that have
+// done all their sweeps leave with their theta and log-likelihood.  Requests
+// arriving while others are on the GPU join at the next step.  A document's
+// draws depend only on its model, words, seed and key, so its result is the
+// same alone or in any mix.  All waits are host-side and bounded.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+#include "common.cuh"
+#include "infer.cuh"
+#include "philox.cuh"
+#include "../../include/tomotopy_b200.h"
+
+using namespace tmtk;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Request {
+    uint64_t id;
+    uint32_t model;
+    std::vector<uint32_t> words;   // sorted by id
+    uint32_t iters;
+    uint64_t seed, key;
+    Clock::time_point t_submit;
+};
+
+struct Result {
+    uint64_t id;
+    uint32_t model;
+    std::vector<float> theta;
+    double ll;
+    double latency_ms, queue_ms;
+};
+
+// first-fit allocator over [0, cap) tokens
+struct Arena {
+    std::map<uint64_t, uint64_t> free_;   // begin -> length
+    uint64_t cap = 0, used = 0;
+    void init(uint64_t c) { cap = c; free_.clear(); if (c) free_[0] = c; used = 0; }
+    bool alloc(uint64_t n, uint64_t& at)
+    {
+        if (n == 0) { at = 0; return true; }
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                at = it->first;
+                const uint64_t rest = it->second - n;
+                free_.erase(it);
+                if (rest) free_[at + n] = rest;
+                used += n;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(uint64_t at, uint64_t n)
+    {
+        if (n == 0) return;
+        used -= n;
+        auto it = free_.emplace(at, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+struct Model {
+    uint32_t K = 0, V = 0;
+    float eta = 0;
+    std::vector<float> alpha;
+    float asum_f = 0;
+    double asum_d = 0;
+    int32_t* d_nkw = nullptr;
+    int32_t* d_nk = nullptr;
+    float* d_alpha = nullptr;
+    float* d_acum = nullptr;
+    // slot pool
+    uint32_t slots = 0;
+    std::vector<int> active;            // request index per slot, -1 free
+    std::vector<Request> req;           // request per slot
+    std::vector<uint64_t> h_tok_begin;
+    std::vector<uint32_t> h_tok_len, h_it_begin, h_it_end, h_it_total, h_done;
+    std::vector<uint64_t> h_keys;
+    uint64_t* d_tok_begin = nullptr;
+    uint32_t *d_tok_len = nullptr, *d_it_begin = nullptr, *d_it_end = nullptr, *d_it_total = nullptr;
+    uint64_t* d_keys = nullptr;
+    int32_t* d_ndk = nullptr;
+    float* d_theta = nullptr;
+    double* d_ll = nullptr;
+    uint32_t* d_work = nullptr;
+    uint32_t* d_counter = nullptr;
+};
+
+} // namespace
+
+struct tmt_server {
+    tmt_server_config cfg{};
+    int device = 0, num_sms = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    uint32_t* d_words = nullptr;
+    uint16_t* d_z = nullptr;
+    Arena arena;
+    std::vector<std::unique_ptr<Model>> models;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request> queue;
+    std::deque<Result> results;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    std::string err;
+    tmt_status worker_status = TMT_OK;
+    // statistics
+    uint64_t steps = 0, completed = 0, active_sum = 0, tokens_in_flight_max = 0;
+
+    template <class T>
+    T* dalloc(size_t n)
+    {
+        void* p = nullptr;
+        const size_t b = std::max<size_t>(16, n * sizeof(T));
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw OomError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        allocs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~tmt_server()
+    {
+        cudaSetDevice(device);
+        for (void* p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// One step of the worker; returns false when there was nothing to do.
+bool server_step(tmt_server* s)
+{
+    std::vector<std::pair<Model*, uint32_t>> admitted;   // (model, slot)
+    std::vector<Model*> models;                          // tmt_server_add_model may append meanwhile
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& mp : s->models) models.push_back(mp.get());
+        while (!s->queue.empty()) {
+            Request& r = s->queue.front();
+            Model* m = s->models[r.model].get();
+            auto it = std::find(m->active.begin(), m->active.end(), -1);
+            if (it == m->active.end()) break;            // no slot: wait (head of line)
+            uint64_t at = 0;
+            if (!s->arena.alloc(r.words.size(), at)) break;   // over the budget: wait
+            const uint32_t sl = (uint32_t)(it - m->active.begin());
+            m->active[sl] = 1;
+            m->h_tok_begin[sl] = at;
+            m->h_tok_len[sl] = (uint32_t)r.words.size();
+            m->h_keys[sl] = r.key;
+            m->h_it_total[sl] = r.iters;
+            m->h_done[sl] = 0;
+            m->req[sl] = std::move(r);
+            s->queue.pop_front();
+            admitted.emplace_back(m, sl);
+        }
+        s->tokens_in_flight_max = std::max<uint64_t>(s->tokens_in_flight_max, s->arena.used);
+    }
+    // copy the admitted documents into the arena
+    for (auto& [m, sl] : admitted) {
+        if (m->h_tok_len[sl])
+            CK(cudaMemcpyAsync(s->d_words + m->h_tok_begin[sl], m->req[sl].words.data(),
+                               m->h_tok_len[sl] * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    }
+    bool any = false;
+    std::vector<std::pair<Model*, uint32_t>> finishing;
+    for (Model* m : models) {
+        std::vector<uint32_t> work;
+        for (uint32_t sl = 0; sl < m->slots; ++sl) {
+            if (m->active[sl] < 0) continue;
+            const uint32_t len = std::max(1u, m->h_tok_len[sl]);
+            const uint32_t adv = std::max(1u, (s->cfg.step_token_sweeps + len - 1) / len);
+            m->h_it_begin[sl] = m->h_done[sl];
+            m->h_it_end[sl] = std::min(m->h_it_total[sl], m->h_done[sl] + adv);
+            work.push_back(sl);
+            if (m->h_it_end[sl] == m->h_it_total[sl]) finishing.emplace_back(m, sl);
+        }
+        if (work.empty()) continue;
+        any = true;
+        s->active_sum += work.size();
+        const size_t S = m->slots;
+        CK(cudaMemcpyAsync(m->d_tok_begin, m->h_tok_begin.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_tok_len, m->h_tok_len.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_keys, m->h_keys.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_begin, m->h_it_begin.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_end, m->h_it_end.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_total, m->h_it_total.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_work, work.data(), work.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
+        InferArgs a{};
+        a.nkw = m->d_nkw;
+        a.nk = m->d_nk;
+        a.alpha = m->d_alpha;
+        a.acum = m->d_acum;
+        a.K = m->K;
+        a.V = m->V;
+        a.eta = m->eta;
+        a.veta = m->eta * (float)m->V;
+        a.asum_f = m->asum_f;
+        a.veta_d = (double)m->V * (double)m->eta;
+        a.asum_d = m->asum_d;
+        a.lg_asum = std::lgamma(m->asum_d);
+        a.lg_eta = std::lgamma((double)m->eta);
+        a.words = s->d_words;
+        a.z = s->d_z;
+        a.tok_begin = m->d_tok_begin;
+        a.tok_len = m->d_tok_len;
+        a.keys = m->d_keys;
+        a.it_begin = m->d_it_begin;
+        a.it_end = m->d_it_end;
+        a.it_total = m->d_it_total;
+        a.ndk = m->d_ndk;
+        a.theta = m->d_theta;
+        a.ll = m->d_ll;
+        a.work = m->d_work;
+        a.n_work = (uint32_t)work.size();
+        a.counter = m->d_counter;
+        // every request of a model shares the draw key base; the per-request seed is folded in below
+        a.key = 0;
+        // requests may carry different seeds: launch per distinct seed (usually one)
+        std::map<uint64_t, std::vector<uint32_t>> by_seed;
+        for (uint32_t sl : work) by_seed[m->req[sl].seed].push_back(sl);
+        if (by_seed.size() == 1) {
+            a.key = by_seed.begin()->first ^ (uint64_t)tmt::kStreamInfer;
+            launch_infer(a, s->num_sms, s->stream);
+        } else {
+            for (auto& [seed, sls] : by_seed) {
+                CK(cudaMemcpyAsync(m->d_work, sls.data(), sls.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+                CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
+                a.n_work = (uint32_t)sls.size();
+                a.key = seed ^ (uint64_t)tmt::kStreamInfer;
+                launch_infer(a, s->num_sms, s->stream);
+            }
+        }
+    }
+    if (!any) return false;
+    // results of the finished documents
+    std::vector<Result> out(finishing.size());
+    for (size_t i = 0; i < finishing.size(); ++i) {
+        auto [m, sl] = finishing[i];
+        out[i].theta.resize(m->K);
+        CK(cudaMemcpyAsync(out[i].theta.data(), m->d_theta + (uint64_t)sl * m->K, m->K * sizeof(float),
+                           cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(&out[i].ll, m->d_ll + sl, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    const auto now = Clock::now();
+    ++s->steps;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (Model* m : models)
+            for (uint32_t sl = 0; sl < m->slots; ++sl)
+                if (m->active[sl] >= 0) m->h_done[sl] = m->h_it_end[sl];
+        for (size_t i = 0; i < finishing.size(); ++i) {
+            auto [m, sl] = finishing[i];
+            Request& r = m->req[sl];
+            out[i].id = r.id;
+            out[i].model = r.model;
+            out[i].latency_ms = std::chrono::duration<double, std::milli>(now - r.t_submit).count();
+            out[i].queue_ms = 0;
+            s->arena.release(m->h_tok_begin[sl], m->h_tok_len[sl]);
+            m->active[sl] = -1;
+            r.words.clear();
+            r.words.shrink_to_fit();
+            s->results.push_back(std::move(out[i]));
+            ++s->completed;
+        }
+    }
+    if (!finishing.empty()) s->cv_done.notify_all();
+    return true;
+}
+
+void server_loop(tmt_server* s)
+{
+    cudaSetDevice(s->device);
+    try {
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (s->stop) break;
+            }
+            if (!server_step(s)) {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (s->stop) break;
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+            }
+        }
+    } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->err = e.what();
+        s->worker_status = TMT_ERR_CUDA;
+        s->stop = true;
+        s->cv_done.notify_all();
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out)
+{
+    if (!cfg || !out) return TMT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (cfg->max_slots == 0 || cfg->token_budget == 0 || cfg->max_doc_len == 0 || cfg->max_doc_len > cfg->token_budget)
+        return TMT_ERR_INVALID_ARGUMENT;
+    auto* s = new (std::nothrow) tmt_server();
+    if (!s) return TMT_ERR_OUT_OF_MEMORY;
+    s->cfg = *cfg;
+    if (!s->cfg.step_token_sweeps) s->cfg.step_token_sweeps = 4096;
+    s->device = cfg->device;
+    try {
+        CK(cudaSetDevice(s->device));
+        CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
+        s->d_words = s->dalloc<uint32_t>(cfg->token_budget);
+        s->d_z = s->dalloc<uint16_t>(cfg->token_budget);
+        s->arena.init(cfg->token_budget);
+    } catch (const OomError&) {
+        delete s;
+        return TMT_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        delete s;
+        return TMT_ERR_CUDA;
+    }
+    s->worker = std::thread(server_loop, s);
+    *out = s;
+    return TMT_OK;
+}
+
+tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
+                                const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id)
+{
+    if (!s || !alpha || !n_k || (V && !n_kw) || !model_id || K == 0 || K > 32767 || !(eta > 0))
+        return TMT_ERR_INVALID_ARGUMENT;
+    if (infer_warps(K) == 0) return TMT_ERR_UNSUPPORTED;
+    auto m = std::make_unique<Model>();
+    m->K = K;
+    m->V = V;
+    m->eta = eta;
+    m->alpha.assign(alpha, alpha + K);
+    std::vector<float> acum(K);
+    float sf = 0.f;
+    double sd = 0;
+    for (uint32_t k = 0; k < K; ++k) {
+        if (!(alpha[k] > 0)) return TMT_ERR_INVALID_ARGUMENT;
+        sf = sf + alpha[k];
+        acum[k] = sf;
+        sd += (double)alpha[k];
+    }
+    m->asum_f = sf;
+    m->asum_d = sd;
+    const uint32_t S = s->cfg.max_slots;
+    m->slots = S;
+    m->active.assign(S, -1);
+    m->req.resize(S);
+    m->h_tok_begin.assign(S, 0);
+    m->h_keys.assign(S, 0);
+    m->h_tok_len.assign(S, 0);
+    m->h_it_begin.assign(S, 0);
+    m->h_it_end.assign(S, 0);
+    m->h_it_total.assign(S, 0);
+    m->h_done.assign(S, 0);
+    std::lock_guard<std::mutex> lk(s->mu);      // the worker does not allocate meanwhile
+    try {
+        CK(cudaSetDevice(s->device));
+        m->d_nkw = s->dalloc<int32_t>((uint64_t)K * V);
+        m->d_nk = s->dalloc<int32_t>(K);
+        m->d_alpha = s->dalloc<float>(K);
+        m->d_acum = s->dalloc<float>(K);
+        m->d_tok_begin = s->dalloc<uint64_t>(S);
+        m->d_tok_len = s->dalloc<uint32_t>(S);
+        m->d_keys = s->dalloc<uint64_t>(S);
+        m->d_it_begin = s->dalloc<uint32_t>(S);
+        m->d_it_end = s->dalloc<uint32_t>(S);
+        m->d_it_total = s->dalloc<uint32_t>(S);
+        m->d_ndk = s->dalloc<int32_t>((uint64_t)S * K);
+        m->d_theta = s->dalloc<float>((uint64_t)S * K);
+        m->d_ll = s->dalloc<double>(S);
+        m->d_work = s->dalloc<uint32_t>(S);
+        m->d_counter = s->dalloc<uint32_t>(1);
+        if ((uint64_t)K * V)
+            CK(cudaMemcpy(m->d_nkw, n_kw, (uint64_t)K * V * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_nk, n_k, K * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_alpha, alpha, K * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice));
+    } catch (const OomError&) {
+        return TMT_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return TMT_ERR_CUDA;
+    }
+    *model_id = (uint32_t)s->models.size();
+    s->models.push_back(std::move(m));
+    return TMT_OK;
+}
+
+tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* wid, uint32_t len, uint32_t iters,
+                             uint64_t seed, uint64_t key, uint64_t* request_id)
+{
+    if (!s || (len && !wid) || !request_id) return TMT_ERR_INVALID_ARGUMENT;
+    if (len > s->cfg.max_doc_len) return TMT_ERR_INVALID_ARGUMENT;
+    Request r;
+    r.words.assign(wid, wid + len);
+    std::stable_sort(r.words.begin(), r.words.end());
+    r.iters = iters;
+    r.seed = seed;
+    r.key = key;
+    r.t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
+        if (model_id >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
+        r.model = model_id;
+        r.id = s->next_id++;
+        *request_id = r.id;
+        s->queue.push_back(std::move(r));
+    }
+    s->cv_work.notify_one();
+    return TMT_OK;
+}
+
+tmt_status tmt_server_poll(tmt_server* s, uint32_t wait_ms, uint64_t* request_id, uint32_t* model_id,
+                           float* theta, uint32_t theta_cap, double* ll, double* latency_ms)
+{
+    if (!s || !request_id) return TMT_ERR_INVALID_ARGUMENT;
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !s->results.empty() || s->stop; });
+    if (s->results.empty()) {
+        if (s->worker_status != TMT_OK) return s->worker_status;
+        return TMT_ERR_TIMEOUT;
+    }
+    Result r = std::move(s->results.front());
+    s->results.pop_front();
+    lk.unlock();
+    *request_id = r.id;
+    if (model_id) *model_id = r.model;
+    if (theta) {
+        if (theta_cap < r.theta.size()) return TMT_ERR_INVALID_ARGUMENT;
+        std::memcpy(theta, r.theta.data(), r.theta.size() * sizeof(float));
+    }
+    if (ll) *ll = r.ll;
+    if (latency_ms) *latency_ms = r.latency_ms;
+    return TMT_OK;
+}
+
+tmt_status tmt_server_get_stats(tmt_server* s, tmt_server_stats* out)
+{
+    if (!s || !out) return TMT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->steps = s->steps;
+    out->completed = s->completed;
+    out->queued = s->queue.size();
+    out->mean_active = s->steps ? (double)s->active_sum / (double)s->steps : 0.0;
+    out->tokens_in_flight_max = s->tokens_in_flight_max;
+    return TMT_OK;
+}
+
+const char* tmt_server_last_error(const tmt_server* s)
+{
+    return s ? s->err.c_str() : "null server";
+}
+
+tmt_status tmt_server_stop(tmt_server* s)
+{
+    if (!s) return TMT_ERR_INVALID_ARGUMENT;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    s->cv_done.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    const tmt_status st = s->worker_status;
+    delete s;
+    return st;
+}
+
+} // extern "C"

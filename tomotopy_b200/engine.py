@@ -5,7 +5,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import lib, check, TmtConfig, TmtInfo, TmtSynthSpec, SAMPLER_AUTO, LEN_POISSON, LEN_LOGNORMAL
+from ._lib import (lib, check, TmtConfig, TmtInfo, TmtSynthSpec, TmtServerConfig, TmtServerStats, TmtError,
+                   SAMPLER_AUTO, LEN_POISSON, LEN_LOGNORMAL)
 
 
 def _p(a):
@@ -18,6 +19,7 @@ class Engine:
     def __init__(self, K, V, alpha=0.1, eta=0.01, seed=0, optim_interval=10, burn_in=0, device=0,
                  sampler=SAMPLER_AUTO, hbm_budget=0, sweep_groups=0):
         self.K, self.V = int(K), int(V)
+        self._eta = float(np.float32(eta))
         a = np.broadcast_to(np.asarray(alpha, dtype=np.float32), (self.K,)).copy() \
             if np.ndim(alpha) else None
         self._alpha_buf = a
@@ -69,6 +71,10 @@ class Engine:
         check(lib.tmt_infer_batch(self.h, _p(words), _p(doc_off), D, int(iters), int(seed), _p(keys),
                                   _p(theta), _p(ll)), self.h)
         return theta[:D], ll[:D]
+
+    @property
+    def eta(self):
+        return self._eta
 
     def ll(self):
         a, b = C.c_double(), C.c_double()
@@ -131,3 +137,63 @@ def prepare_ids(doc_off, words, min_cf=0, min_df=0, rm_top=0):
     check(lib.tmt_prepare_corpus(D, _p(doc_off), _p(words), nv, min_cf, min_df, rm_top, _p(out), None,
                                  _p(order), None, None, C.byref(rv)), None, "tmt_prepare_corpus")
     return doc_off, out[:len(words)], int(rv.value), order[:nv]
+
+
+class Server:
+    """Continuous-batching inference over resident frozen models (tmt_server_*)."""
+
+    def __init__(self, max_slots=4096, token_budget=1 << 24, step_token_sweeps=4096, max_doc_len=1 << 16, device=0):
+        cfg = TmtServerConfig(device=int(device), max_slots=int(max_slots), token_budget=int(token_budget),
+                              step_token_sweeps=int(step_token_sweeps), max_doc_len=int(max_doc_len))
+        h = C.c_void_p()
+        check(lib.tmt_server_start(C.byref(cfg), C.byref(h)), None, "tmt_server_start")
+        self.h = h
+        self.K = {}
+
+    def add_model(self, K, V, alpha, eta, n_kw, n_k):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(alpha, np.float32), (K,)))
+        nkw = np.ascontiguousarray(n_kw, dtype=np.int32)
+        nk = np.ascontiguousarray(n_k, dtype=np.int32)
+        mid = C.c_uint32()
+        check(lib.tmt_server_add_model(self.h, K, V, _p(a), float(eta), _p(nkw), _p(nk), C.byref(mid)), None,
+              "tmt_server_add_model")
+        self.K[mid.value] = int(K)
+        return mid.value
+
+    def add_engine_model(self, eng):
+        _, nkw, nk, alpha = eng.state()
+        return self.add_model(eng.K, eng.V, alpha, eng.eta, nkw, nk)
+
+    def submit(self, model_id, words, iters=100, seed=0, key=0):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        rid = C.c_uint64()
+        check(lib.tmt_server_submit(self.h, int(model_id), _p(w), len(w), int(iters), int(seed), int(key),
+                                    C.byref(rid)), None, "tmt_server_submit")
+        return rid.value
+
+    def poll(self, wait_ms=1000):
+        """(request_id, model_id, theta, ll, latency_ms) or None on timeout."""
+        rid, mid = C.c_uint64(), C.c_uint32()
+        cap = max(self.K.values()) if self.K else 1
+        theta = np.zeros(cap, dtype=np.float32)
+        ll, lat = C.c_double(), C.c_double()
+        st = lib.tmt_server_poll(self.h, int(wait_ms), C.byref(rid), C.byref(mid), _p(theta), cap, C.byref(ll),
+                                 C.byref(lat))
+        if st == -7:
+            return None
+        if st != 0:
+            raise TmtError(st, lib.tmt_server_last_error(self.h).decode())
+        return rid.value, mid.value, theta[:self.K[mid.value]].copy(), ll.value, lat.value
+
+    def stats(self):
+        s = TmtServerStats()
+        check(lib.tmt_server_get_stats(self.h, C.byref(s)), None, "tmt_server_get_stats")
+        return s
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib.tmt_server_stop(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
