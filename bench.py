@@ -200,18 +200,192 @@ def cpu_baseline_sample(w, off, words, V, seconds=10.0):
             "sample": f"first {D} docs ({c.N} tokens), {n} PARTITION sweeps on {cores} host threads"}
 
 
+INFER = {
+    # served infer(), single model: k=100 trained on config 1's corpus; requests lognormal(ln 150, 1.0)
+    "c4": dict(models=[dict(K=100, V=10000, T=20, D=1000, length=("poisson", 1500, 1, 100000),
+                            seed=20261204, sweeps=200)],
+               mix=[1.0], length=("lognormal", float(np.log(150)), 1.0, 10, 5000), iters=50,
+               rates=[1000, 5000, 20000, 50000, 100000]),
+    # served infer(), three resident models, traffic 60/30/10, 100 sweeps each
+    "c5": dict(models=[dict(K=50, V=20000, T=50, D=40000, length=("lognormal", float(np.log(100)), 1.2, 5, 10000),
+                            seed=20261207, sweeps=50),
+                       dict(K=200, V=50000, T=200, D=40000, length=("lognormal", float(np.log(100)), 1.2, 5, 10000),
+                            seed=20261208, sweeps=50),
+                       dict(K=1000, V=100000, T=1000, D=40000, length=("lognormal", float(np.log(100)), 1.2, 5, 10000),
+                            seed=20261209, sweeps=50)],
+               mix=[0.6, 0.3, 0.1], length=("lognormal", float(np.log(100)), 1.2, 5, 10000), iters=100,
+               rates=[1000, 5000, 20000, 50000]),
+}
+
+
+def infer_requests(mc, order, n, length, seed_off):
+    """n unseen documents from the model's generative process; words outside
+    the model's dictionary are dropped, as tomotopy's makeDoc does."""
+    import tomotopy_b200 as T
+    off, w = T.synth_corpus(mc["V"], mc["T"], n, length, seed=mc["seed"], doc_offset=10_000_000 + seed_off)
+    docs = []
+    for d in range(n):
+        ids = w[off[d]:off[d + 1]]
+        ids = ids[ids < len(order)]
+        docs.append(order[ids].astype(np.uint32))
+    return docs
+
+
+def run_infer(args):
+    import threading as th
+    import torch
+    import tomotopy_b200 as T
+    cfg = INFER[args.config]
+    torch.cuda.set_device(0)
+    engines, orders = [], []
+    for mc in cfg["models"]:
+        off, w = T.synth_corpus(mc["V"], mc["T"], mc["D"], mc["length"], seed=mc["seed"])
+        off, w, V, order = T.prepare_ids(off, w)
+        eng = T.Engine(mc["K"], V, alpha=ALPHA, eta=ETA, seed=1, optim_interval=0)
+        eng.upload(off, w)
+        eng.train(mc["sweeps"])
+        engines.append(eng)
+        orders.append(order)
+    rng = np.random.default_rng(7)
+    n_req = args.requests
+    which = rng.choice(len(engines), size=n_req, p=cfg["mix"])
+    docs = [None] * n_req
+    for m in range(len(engines)):
+        idx = np.nonzero(which == m)[0]
+        ds = infer_requests(cfg["models"][m], orders[m], len(idx), cfg["length"], seed_off=m * 1_000_000)
+        for i, d in zip(idx, ds):
+            docs[i] = d
+    iters = cfg["iters"]
+    ntok = sum(len(d) for d in docs)
+
+    # plain per-document GPU infer: one tmt_infer_batch call per document
+    n_plain = min(200, n_req)
+    t0 = time.perf_counter()
+    plain_ll = []
+    for i in range(n_plain):
+        d = docs[i]
+        th_, ll_ = engines[which[i]].infer(np.array([0, len(d)], np.uint64), d, iters=iters, seed=0)
+        plain_ll.append(ll_[0])
+    plain_dps = n_plain / (time.perf_counter() - t0)
+
+    srv = T.Server(max_slots=args.slots, token_budget=1 << 25, step_token_sweeps=args.step_tokens,
+                   max_doc_len=1 << 16)
+    mids = [srv.add_engine_model(e) for e in engines]
+
+    def serve(rate):
+        n = n_req if rate is None else int(min(n_req, max(200, 2.0 * rate)))
+        lat, got = [], {}
+        done = th.Event()
+
+        def collect():
+            while len(got) < n:
+                r = srv.poll(wait_ms=500)
+                if r is None:
+                    if done.is_set():
+                        break
+                    continue
+                got[r[0]] = r
+                lat.append(r[4])
+        c = th.Thread(target=collect, daemon=True)
+        c.start()
+        ids = {}
+        t0 = time.perf_counter()
+        if rate is None:
+            for i in range(n):
+                ids[srv.submit(mids[which[i]], docs[i], iters=iters, seed=0)] = i
+        else:
+            gaps = np.random.default_rng(11).exponential(1.0 / rate, n)
+            arrive = np.cumsum(gaps)
+            i = 0
+            while i < n:
+                now = time.perf_counter() - t0
+                while i < n and arrive[i] <= now:
+                    ids[srv.submit(mids[which[i]], docs[i], iters=iters, seed=0)] = i
+                    i += 1
+                if i < n:
+                    time.sleep(max(0.0, min(arrive[i] - (time.perf_counter() - t0), 0.002)))
+        c.join(timeout=600)
+        wall = time.perf_counter() - t0
+        done.set()
+        c.join(timeout=5)
+        lat_a = np.array(lat)
+        return {"offered_docs_per_s": rate, "docs_per_s": len(got) / wall, "p50_ms": float(np.percentile(lat_a, 50)),
+                "p99_ms": float(np.percentile(lat_a, 99)), "completed": len(got)}, got, ids
+
+    sat, got, ids = serve(None)
+    # same results as plain per-document infer (same seeds, keys 0)
+    served_ll = {ids[k]: v[3] for k, v in got.items()}
+    agree = all(served_ll[i] == plain_ll[i] for i in range(n_plain))
+    sweeps = [serve(r)[0] for r in cfg["rates"]]
+    st = srv.stats()
+    srv.close()
+    tok_per_doc = ntok / n_req
+    line = {
+        "metric": f"served infer docs/s ({args.config})", "value": sat["docs_per_s"], "unit": "docs/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
+        "config": {"workload": f"{args.config}: " + ", ".join(f"k={m['K']} V={m['V']}" for m in cfg["models"]) +
+                   f"; mix {cfg['mix']}; {iters} sweeps per document; {n_req} requests, {tok_per_doc:.1f} tokens/doc",
+                   "slots": args.slots, "step_token_sweeps": args.step_tokens},
+        "saturation": sat, "rate_sweep": sweeps,
+        "plain_per_document_docs_per_s": plain_dps, "speedup_vs_plain": sat["docs_per_s"] / plain_dps,
+        "token_sweeps_per_s": sat["docs_per_s"] * tok_per_doc * iters,
+        "results_identical_to_plain": bool(agree),
+        "mean_ll_per_word_plain": float(np.sum(plain_ll) / max(1, sum(len(docs[i]) for i in range(n_plain)))),
+        "server": {"steps": int(st.steps), "mean_active": st.mean_active},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_infer_baseline(engines, which, docs, iters)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_infer_baseline(engines, which, docs, iters, seconds=10.0):
+    """tomotopy's per-document infer (LDAModel.hpp:920-953) restated in the
+    oracle, one document per host thread."""
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    models = []
+    for e in engines:
+        _, nkw, nk, alpha = e.state()
+        models.append((e.K, e.V, alpha, e.eta, nkw, nk))
+    cores = os.cpu_count() or 1
+    n = 0
+    t0 = time.perf_counter()
+
+    def one(i):
+        K, V, alpha, eta, nkw, nk = models[which[i]]
+        O.infer_doc(K, V, alpha, eta, nkw, nk, np.sort(docs[i]), iters, 0, 0)
+
+    with ThreadPoolExecutor(cores) as ex:
+        while time.perf_counter() - t0 < seconds and n < len(docs):
+            batch = list(range(n, min(len(docs), n + 4 * cores)))
+            list(ex.map(one, batch))
+            n += len(batch)
+    t = time.perf_counter() - t0
+    return {"value": n / t, "unit": "docs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} request documents, per-document infer on {cores} host threads"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="c3", choices=sorted(set(WORKLOADS) | set(INFER)))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI pass")
     ap.add_argument("--docs", type=int, default=0, help="override the document count (smaller case)")
     ap.add_argument("--groups", type=int, default=0, help="document groups per sweep (0: engine default)")
+    ap.add_argument("--mode", default="train", choices=["train", "infer"])
+    ap.add_argument("--requests", type=int, default=20000, help="infer mode: documents per run")
+    ap.add_argument("--slots", type=int, default=8192, help="infer mode: server slots per model")
+    ap.add_argument("--step-tokens", type=int, default=4096, help="infer mode: token-sweeps per document per step")
     args = ap.parse_args()
+    if args.mode == "infer":
+        if args.config not in INFER:
+            args.config = "c4"
+        return run_infer(args)
     args.warmup = max(args.warmup, 3)
     w = dict(WORKLOADS[args.config])
     if args.docs:

@@ -229,6 +229,8 @@ typedef struct tmt_synth_spec {
     double zipf_s;
     uint64_t seed;
     uint32_t threads;        /* 0 = all hardware threads */
+    uint64_t doc_offset;     /* documents are drawn as numbers doc_offset .. doc_offset+D-1: with the
+                                same seed, a different offset gives new documents of the same topics */
 } tmt_synth_spec;
 
 /* Two calls: with words == NULL fills doc_off[D+1] and *n_tokens; then with

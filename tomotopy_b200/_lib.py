@@ -47,7 +47,7 @@ class TmtSynthSpec(C.Structure):
     _fields_ = [("V", C.c_uint32), ("T", C.c_uint32), ("D", C.c_uint64), ("len_kind", C.c_int32),
                 ("len_a", C.c_double), ("len_b", C.c_double), ("len_min", C.c_uint32), ("len_max", C.c_uint32),
                 ("doc_alpha", C.c_double), ("topic_beta", C.c_double), ("zipf_s", C.c_double),
-                ("seed", C.c_uint64), ("threads", C.c_uint32)]
+                ("seed", C.c_uint64), ("threads", C.c_uint32), ("doc_offset", C.c_uint64)]
 
 
 _P = C.c_void_p

@@ -158,7 +158,8 @@ extern "C" tmt_status tmt_synth_corpus(const tmt_synth_spec* spec, uint64_t* doc
         std::vector<uint32_t> len(s.D);
         parallel_for(s.D, threads, [&](uint64_t b, uint64_t e) {
             for (uint64_t d = b; d < e; ++d) {
-                Rng r(s.seed, (uint32_t)d, 0x4C454E00u | (uint32_t)(d >> 32));
+                const uint64_t dd = d + s.doc_offset;
+                Rng r(s.seed, (uint32_t)dd, 0x4C454E00u | (uint32_t)(dd >> 32));
                 len[d] = doc_length(s, r);
             }
         });
@@ -200,7 +201,8 @@ extern "C" tmt_status tmt_synth_corpus(const tmt_synth_spec* spec, uint64_t* doc
         parallel_for(s.D, threads, [&](uint64_t b, uint64_t e) {
             std::vector<uint32_t> zt;
             for (uint64_t d = b; d < e; ++d) {
-                Rng r(s.seed, (uint32_t)d, 0x544F4B00u | (uint32_t)(d >> 32));
+                const uint64_t dd = d + s.doc_offset;
+                Rng r(s.seed, (uint32_t)dd, 0x544F4B00u | (uint32_t)(dd >> 32));
                 uint32_t L = len[d];
                 zt.resize(L);
                 uint32_t* out = words + doc_off[d];

@@ -105,7 +105,7 @@ class Engine:
         return i
 
 
-def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1.07, threads=0):
+def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1.07, threads=0, doc_offset=0):
     """Seeded synthetic corpus (tmt_synth_corpus).  length = ("poisson", mean, lo, hi)
     or ("lognormal", mu, sigma, lo, hi).  Returns (doc_off uint64[D+1], words uint32[N])."""
     if length[0] == "poisson":
@@ -113,7 +113,8 @@ def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1
     else:
         kind, a, b, lo, hi = LEN_LOGNORMAL, float(length[1]), float(length[2]), int(length[3]), int(length[4])
     spec = TmtSynthSpec(V=V, T=T, D=D, len_kind=kind, len_a=a, len_b=b, len_min=lo, len_max=hi,
-                        doc_alpha=doc_alpha, topic_beta=topic_beta, zipf_s=zipf_s, seed=seed, threads=threads)
+                        doc_alpha=doc_alpha, topic_beta=topic_beta, zipf_s=zipf_s, seed=seed, threads=threads,
+                        doc_offset=doc_offset)
     off = np.zeros(D + 1, dtype=np.uint64)
     n = C.c_uint64()
     check(lib.tmt_synth_corpus(C.byref(spec), _p(off), None, 0, C.byref(n)), None, "synth lengths")
