@@ -68,6 +68,7 @@ k_infer_slots(InferArgs a)
     int* own = reinterpret_cast<int*>(rr + KP);
     const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
     const float eta = a.eta, veta = a.veta;
+    const bool vecg = (K & 3) == 0;      // n_kw columns 16-byte aligned: vector loads
 
     for (;;) {
         uint32_t q = 0;
@@ -117,110 +118,144 @@ k_infer_slots(InferArgs a)
             if (k < K) {
                 const int n = rowi[k];
                 f = __fadd_rn((float)n, __ldg(a.alpha + k));
-                g = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + k) + n), veta));
+                g = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + k) + n), veta));
             }
             rowf[k] = f;
             rr[k] = g;
         }
         __syncwarp();
+        // `own` holds the topics of the current run's other tokens; a word
+        // that occurs once in the document never touches it.
+        auto run_end = [&](uint32_t j0, uint32_t v) -> uint32_t {
+            uint32_t re = j0 + 1;
+            for (;;) {
+                const uint32_t j = re + lane;
+                const bool diff = j >= L || a.words[b + j] != v;
+                const unsigned mm = __ballot_sync(FULL, diff);
+                if (mm) return re + __ffs(mm) - 1;
+                re += 32;
+            }
+        };
         for (uint32_t it = it0; it < it1; ++it) {
-            uint32_t rb = 0;
-            while (rb < L) {
-                const uint32_t v = a.words[b + rb];
-                uint32_t re = rb + 1;          // end of the run of word v
-                for (;;) {
-                    const uint32_t j = re + lane;
-                    const bool diff = j >= L || a.words[b + j] != v;
-                    const unsigned mm = __ballot_sync(FULL, diff);
-                    if (mm) { re += __ffs(mm) - 1; break; }
-                    re += 32;
+            uint32_t run_b = 0, run_e = 0;      // the multi-token run whose histogram is in `own`
+            for (uint32_t base = 0; base < L; base += 32) {
+                const uint32_t jl = base + lane;
+                uint32_t my_w = 0xFFFFFFFFu, my_z = 0;
+                bool my_same = false;            // my token's word equals the next token's
+                float my_u = 0.f;
+                if (jl < L) {
+                    my_w = a.words[b + jl];
+                    my_z = a.z[b + jl];
+                    my_same = jl + 1 < L && a.words[b + jl + 1] == my_w;
+                    my_u = tmt::u01(tmt::philox_u32(jl, it, klo, khi, a.key));
                 }
-                if (v < a.V) {
-                    for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
-                    __syncwarp();
-                    const int32_t* gcol = a.nkw + (uint64_t)v * K;
-                    for (uint32_t j = rb; j < re; ++j) {
-                        const int zo = a.z[b + j];
-                        if (lane == 0) {
-                            own[zo] -= 1;
-                            const int n = rowi[zo] - 1;
-                            rowi[zo] = n;
-                            rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
-                            rr[zo] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + zo) + n), veta));
-                        }
+                const unsigned same_m = __ballot_sync(FULL, my_same);
+                const int nb = (int)min(32u, L - base);
+                for (int q2 = 0; q2 < nb; ++q2) {
+                    const uint32_t j = base + q2;
+                    const uint32_t v = __shfl_sync(FULL, my_w, q2);
+                    const int zo = (int)__shfl_sync(FULL, my_z, q2);
+                    const float u = __shfl_sync(FULL, my_u, q2);
+                    if (v >= a.V) continue;
+                    const bool in_run = j < run_e;
+                    if (!in_run && ((same_m >> q2) & 1u)) {
+                        // a multi-token run starts here: histogram of its tokens' topics
+                        run_b = j;
+                        run_e = run_end(j, v);
+                        for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicAdd(&own[a.z[b + t]], 1);
                         __syncwarp();
-                        // pass 1: fma chain over this lane's topics
-                        float s = 0.f;
-                        if (CH > 0) {
+                    }
+                    const bool multi = j < run_e;
+                    const int32_t* gcol = a.nkw + (uint64_t)v * K;
+                    if (lane == 0) {
+                        if (multi) own[zo] -= 1;
+                        const int n = rowi[zo] - 1;
+                        rowi[zo] = n;
+                        rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
+                        rr[zo] = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + zo) + n), veta));
+                    }
+                    __syncwarp();
+                    // pass 1: fma chain over this lane's topics
+                    float s = 0.f;
+                    if (CH > 0) {
 #pragma unroll
-                            for (int jj = 0; jj < CHR; ++jj) {
-                                if (jj < nch) {
-                                    const int k0 = 128 * jj + 4 * lane;
-                                    const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
-                                    const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
-                                    const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
-                                    int g0 = __ldg(gcol + k0), g1 = 0, g2 = 0, g3 = 0;
+                        for (int jj = 0; jj < CHR; ++jj) {
+                            if (jj < nch) {
+                                const int k0 = 128 * jj + 4 * lane;
+                                const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
+                                const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
+                                int g0, g1 = 0, g2 = 0, g3 = 0;
+                                if (vecg) {
+                                    const int4 G4 = __ldg(reinterpret_cast<const int4*>(gcol + k0));
+                                    g0 = G4.x; g1 = G4.y; g2 = G4.z; g3 = G4.w;
+                                } else {
+                                    g0 = __ldg(gcol + k0);
                                     if (k0 + 1 < K) g1 = __ldg(gcol + k0 + 1);
                                     if (k0 + 2 < K) g2 = __ldg(gcol + k0 + 2);
                                     if (k0 + 3 < K) g3 = __ldg(gcol + k0 + 3);
-                                    s = __fmaf_rn(A4.x, __fmul_rn(__fadd_rn((float)(g0 + O4.x), eta), R4.x), s);
-                                    s = __fmaf_rn(A4.y, __fmul_rn(__fadd_rn((float)(g1 + O4.y), eta), R4.y), s);
-                                    s = __fmaf_rn(A4.z, __fmul_rn(__fadd_rn((float)(g2 + O4.z), eta), R4.z), s);
-                                    s = __fmaf_rn(A4.w, __fmul_rn(__fadd_rn((float)(g3 + O4.w), eta), R4.w), s);
                                 }
-                            }
-                        } else {
-                            for (int jj = 0; jj < nch; ++jj)
-                                for (int i = 0; i < 4; ++i) {
-                                    const int k = 128 * jj + 4 * lane + i;
-                                    if (k < K)
-                                        s = __fmaf_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]), s);
+                                if (multi) {
+                                    const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
+                                    g0 += O4.x; g1 += O4.y; g2 += O4.z; g3 += O4.w;
                                 }
-                        }
-                        const float x = hs_scan32(s, lane);
-                        float E = __shfl_up_sync(FULL, x, 1);
-                        if (lane == 0) E = 0.f;
-                        const float total = __shfl_sync(FULL, x, 31);
-                        const float u = tmt::u01(tmt::philox_u32(j, it, klo, khi, a.key));
-                        const float r = __fmul_rn(u, total);
-                        const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
-                        int znew = K - 1;
-                        if (m) {
-                            // pass 2: position among lane h's topics, 32 at a time
-                            const int h = __ffs(m) - 1;
-                            const float Eh = __shfl_sync(FULL, E, h);
-                            const int mh = K - 4 * h;
-                            const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
-                            float carry = 0.f;
-                            int found = nh - 1;
-                            for (int mm = 0; mm < nh; mm += 32) {
-                                const int t = mm + lane;
-                                const int k = 128 * (t >> 2) + 4 * h + (t & 3);
-                                float x2 = 0.f;
-                                if (t < nh)
-                                    x2 = __fmul_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]));
-                                x2 = hs_scan32(x2, lane);
-                                const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
-                                if (mb) { found = mm + __ffs(mb) - 1; break; }
-                                carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                                s = __fmaf_rn(A4.x, __fmul_rn(__fadd_rn((float)g0, eta), R4.x), s);
+                                s = __fmaf_rn(A4.y, __fmul_rn(__fadd_rn((float)g1, eta), R4.y), s);
+                                s = __fmaf_rn(A4.z, __fmul_rn(__fadd_rn((float)g2, eta), R4.z), s);
+                                s = __fmaf_rn(A4.w, __fmul_rn(__fadd_rn((float)g3, eta), R4.w), s);
                             }
-                            znew = 128 * (found >> 2) + 4 * h + (found & 3);
                         }
-                        __syncwarp();
-                        if (lane == 0) {
-                            own[znew] += 1;
-                            const int n = rowi[znew] + 1;
-                            rowi[znew] = n;
-                            rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
-                            rr[znew] = __fdiv_rn(1.0f, __fadd_rn((float)(__ldg(a.nk + znew) + n), veta));
-                            a.z[b + j] = (uint16_t)znew;
+                    } else {
+                        for (int jj = 0; jj < nch; ++jj)
+                            for (int i = 0; i < 4; ++i) {
+                                const int k = 128 * jj + 4 * lane + i;
+                                if (k < K)
+                                    s = __fmaf_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]), s);
+                            }
+                    }
+                    const float x = hs_scan32(s, lane);
+                    float E = __shfl_up_sync(FULL, x, 1);
+                    if (lane == 0) E = 0.f;
+                    const float total = __shfl_sync(FULL, x, 31);
+                    const float r = __fmul_rn(u, total);
+                    const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
+                    int znew = K - 1;
+                    if (m) {
+                        // pass 2: position among lane h's topics, 32 at a time
+                        const int h = __ffs(m) - 1;
+                        const float Eh = __shfl_sync(FULL, E, h);
+                        const int mh = K - 4 * h;
+                        const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
+                        float carry = 0.f;
+                        int found = nh - 1;
+                        for (int mm = 0; mm < nh; mm += 32) {
+                            const int t = mm + lane;
+                            const int k = 128 * (t >> 2) + 4 * h + (t & 3);
+                            float x2 = 0.f;
+                            if (t < nh)
+                                x2 = __fmul_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + (multi ? own[k] : 0)), eta), rr[k]));
+                            x2 = hs_scan32(x2, lane);
+                            const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
+                            if (mb) { found = mm + __ffs(mb) - 1; break; }
+                            carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
                         }
+                        znew = 128 * (found >> 2) + 4 * h + (found & 3);
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (multi) own[znew] += 1;
+                        const int n = rowi[znew] + 1;
+                        rowi[znew] = n;
+                        rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
+                        rr[znew] = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + znew) + n), veta));
+                        a.z[b + j] = (uint16_t)znew;
+                    }
+                    __syncwarp();
+                    if (multi && j + 1 == run_e) {
+                        // the run is done: clear its histogram
+                        for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicSub(&own[a.z[b + t]], 1);
                         __syncwarp();
                     }
-                    for (uint32_t j = rb + lane; j < re; j += 32) atomicSub(&own[a.z[b + j]], 1);
-                    __syncwarp();
                 }
-                rb = re;
             }
         }
         if (it1 < itT) {            // keep the document's counts for the next launch

@@ -32,6 +32,38 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
+// copies admitted documents from the contiguous staging buffer into the arena
+__global__ void k_scatter_docs(const uint32_t* __restrict__ staging, const uint64_t* __restrict__ src,
+                               const uint64_t* __restrict__ dst, const uint32_t* __restrict__ len, uint32_t n,
+                               uint32_t* __restrict__ arena)
+{
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
+        for (uint32_t j = threadIdx.x; j < len[i]; j += blockDim.x) arena[dst[i] + j] = staging[src[i] + j];
+}
+
+// packs the outputs of finished slots: theta rows and ll
+__global__ void k_gather_results(const float* __restrict__ theta, const double* __restrict__ ll,
+                                 const uint32_t* __restrict__ slots, uint32_t n, uint32_t K,
+                                 float* __restrict__ out_theta, double* __restrict__ out_ll)
+{
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint32_t sl = slots[i];
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) out_theta[(uint64_t)i * K + k] = theta[(uint64_t)sl * K + k];
+        if (threadIdx.x == 0) out_ll[i] = ll[sl];
+    }
+}
+
+template <class T>
+T* pinned(size_t n)
+{
+    void* p = nullptr;
+    if (cudaMallocHost(&p, std::max<size_t>(16, n * sizeof(T))) != cudaSuccess) {
+        cudaGetLastError();
+        throw OomError("cudaMallocHost failed");
+    }
+    return static_cast<T*>(p);
+}
+
 struct Request {
     uint64_t id;
     uint32_t model;
@@ -103,9 +135,18 @@ struct Model {
     uint32_t slots = 0;
     std::vector<int> active;            // request index per slot, -1 free
     std::vector<Request> req;           // request per slot
-    std::vector<uint64_t> h_tok_begin;
-    std::vector<uint32_t> h_tok_len, h_it_begin, h_it_end, h_it_total, h_done;
-    std::vector<uint64_t> h_keys;
+    // per-slot metadata, pinned host mirrors of the device arrays
+    uint64_t* h_tok_begin = nullptr;
+    uint32_t *h_tok_len = nullptr, *h_it_begin = nullptr, *h_it_end = nullptr, *h_it_total = nullptr;
+    uint64_t* h_keys = nullptr;
+    uint32_t* h_work = nullptr;
+    uint32_t* h_fin = nullptr;
+    float* h_out_theta = nullptr;
+    double* h_out_ll = nullptr;
+    std::vector<uint32_t> h_done;
+    uint32_t* d_fin = nullptr;
+    float* d_out_theta = nullptr;
+    double* d_out_ll = nullptr;
     uint64_t* d_tok_begin = nullptr;
     uint32_t *d_tok_len = nullptr, *d_it_begin = nullptr, *d_it_end = nullptr, *d_it_total = nullptr;
     uint64_t* d_keys = nullptr;
@@ -125,6 +166,12 @@ struct tmt_server {
     std::vector<void*> allocs;
     uint32_t* d_words = nullptr;
     uint16_t* d_z = nullptr;
+    uint32_t* d_staging = nullptr;               // admitted documents of one step, contiguous
+    uint32_t* h_staging = nullptr;               // pinned
+    uint64_t *h_sc_src = nullptr, *h_sc_dst = nullptr, *d_sc_src = nullptr, *d_sc_dst = nullptr;
+    uint32_t *h_sc_len = nullptr, *d_sc_len = nullptr;
+    std::vector<void*> pinned_allocs;
+    uint64_t sc_cap = 0;                         // documents one step may admit
     Arena arena;
     std::vector<std::unique_ptr<Model>> models;
 
@@ -153,10 +200,19 @@ struct tmt_server {
         allocs.push_back(p);
         return static_cast<T*>(p);
     }
+    template <class T>
+    T* palloc(size_t n)
+    {
+        T* p = pinned<T>(n);
+        pinned_allocs.push_back(p);
+        return p;
+    }
     ~tmt_server()
     {
         cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
         for (void* p : allocs) cudaFree(p);
+        for (void* p : pinned_allocs) cudaFreeHost(p);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -171,7 +227,7 @@ bool server_step(tmt_server* s)
     {
         std::lock_guard<std::mutex> lk(s->mu);
         for (auto& mp : s->models) models.push_back(mp.get());
-        while (!s->queue.empty()) {
+        while (!s->queue.empty() && admitted.size() < s->sc_cap) {
             Request& r = s->queue.front();
             Model* m = s->models[r.model].get();
             auto it = std::find(m->active.begin(), m->active.end(), -1);
@@ -191,15 +247,35 @@ bool server_step(tmt_server* s)
         }
         s->tokens_in_flight_max = std::max<uint64_t>(s->tokens_in_flight_max, s->arena.used);
     }
-    // copy the admitted documents into the arena
-    for (auto& [m, sl] : admitted) {
-        if (m->h_tok_len[sl])
-            CK(cudaMemcpyAsync(s->d_words + m->h_tok_begin[sl], m->req[sl].words.data(),
-                               m->h_tok_len[sl] * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    // the admitted documents: packed into pinned staging, one copy, one scatter
+    if (!admitted.empty()) {
+        uint64_t off = 0;
+        uint32_t n = 0;
+        for (auto& [m, sl] : admitted) {
+            const uint32_t len = m->h_tok_len[sl];
+            if (!len) continue;
+            std::memcpy(s->h_staging + off, m->req[sl].words.data(), len * sizeof(uint32_t));
+            s->h_sc_src[n] = off;
+            s->h_sc_dst[n] = m->h_tok_begin[sl];
+            s->h_sc_len[n] = len;
+            off += len;
+            ++n;
+        }
+        if (n) {
+            CK(cudaMemcpyAsync(s->d_staging, s->h_staging, off * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+            CK(cudaMemcpyAsync(s->d_sc_src, s->h_sc_src, n * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+            CK(cudaMemcpyAsync(s->d_sc_dst, s->h_sc_dst, n * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+            CK(cudaMemcpyAsync(s->d_sc_len, s->h_sc_len, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+            k_scatter_docs<<<std::min<uint32_t>(n, 4096), 128, 0, s->stream>>>(s->d_staging, s->d_sc_src, s->d_sc_dst,
+                                                                              s->d_sc_len, n, s->d_words);
+            CK(cudaGetLastError());
+        }
     }
     bool any = false;
     std::vector<std::pair<Model*, uint32_t>> finishing;
-    for (Model* m : models) {
+    std::vector<uint32_t> nfin(models.size(), 0);
+    for (size_t mi = 0; mi < models.size(); ++mi) {
+        Model* m = models[mi];
         std::vector<uint32_t> work;
         for (uint32_t sl = 0; sl < m->slots; ++sl) {
             if (m->active[sl] < 0) continue;
@@ -208,19 +284,23 @@ bool server_step(tmt_server* s)
             m->h_it_begin[sl] = m->h_done[sl];
             m->h_it_end[sl] = std::min(m->h_it_total[sl], m->h_done[sl] + adv);
             work.push_back(sl);
-            if (m->h_it_end[sl] == m->h_it_total[sl]) finishing.emplace_back(m, sl);
+            if (m->h_it_end[sl] == m->h_it_total[sl]) {
+                finishing.emplace_back(m, sl);
+                m->h_fin[nfin[mi]++] = sl;
+            }
         }
         if (work.empty()) continue;
         any = true;
         s->active_sum += work.size();
         const size_t S = m->slots;
-        CK(cudaMemcpyAsync(m->d_tok_begin, m->h_tok_begin.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_tok_len, m->h_tok_len.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_keys, m->h_keys.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_begin, m->h_it_begin.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_end, m->h_it_end.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_total, m->h_it_total.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_work, work.data(), work.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_tok_begin, m->h_tok_begin, S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_tok_len, m->h_tok_len, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_keys, m->h_keys, S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_begin, m->h_it_begin, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_end, m->h_it_end, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_it_total, m->h_it_total, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        std::copy(work.begin(), work.end(), m->h_work);
+        CK(cudaMemcpyAsync(m->d_work, m->h_work, work.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
         CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
         InferArgs a{};
         a.nkw = m->d_nkw;
@@ -259,8 +339,12 @@ bool server_step(tmt_server* s)
             a.key = by_seed.begin()->first ^ (uint64_t)tmt::kStreamInfer;
             launch_infer(a, s->num_sms, s->stream);
         } else {
+            uint32_t at = 0;
             for (auto& [seed, sls] : by_seed) {
-                CK(cudaMemcpyAsync(m->d_work, sls.data(), sls.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+                std::copy(sls.begin(), sls.end(), m->h_work + at);
+                CK(cudaMemcpyAsync(m->d_work + at, m->h_work + at, sls.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+                a.work = m->d_work + at;
+                at += (uint32_t)sls.size();
                 CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
                 a.n_work = (uint32_t)sls.size();
                 a.key = seed ^ (uint64_t)tmt::kStreamInfer;
@@ -269,16 +353,30 @@ bool server_step(tmt_server* s)
         }
     }
     if (!any) return false;
-    // results of the finished documents
-    std::vector<Result> out(finishing.size());
-    for (size_t i = 0; i < finishing.size(); ++i) {
-        auto [m, sl] = finishing[i];
-        out[i].theta.resize(m->K);
-        CK(cudaMemcpyAsync(out[i].theta.data(), m->d_theta + (uint64_t)sl * m->K, m->K * sizeof(float),
-                           cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaMemcpyAsync(&out[i].ll, m->d_ll + sl, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    // results of the finished documents: packed per model, one copy each
+    for (size_t mi = 0; mi < models.size(); ++mi) {
+        Model* m = models[mi];
+        const uint32_t n = nfin[mi];
+        if (!n) continue;
+        CK(cudaMemcpyAsync(m->d_fin, m->h_fin, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        k_gather_results<<<std::min<uint32_t>(n, 4096), 128, 0, s->stream>>>(m->d_theta, m->d_ll, m->d_fin, n, m->K,
+                                                                             m->d_out_theta, m->d_out_ll);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(m->h_out_theta, m->d_out_theta, (uint64_t)n * m->K * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(m->h_out_ll, m->d_out_ll, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     }
     CK(cudaStreamSynchronize(s->stream));
+    std::vector<Result> out(finishing.size());
+    {
+        std::vector<uint32_t> seen(models.size(), 0);
+        for (size_t i = 0; i < finishing.size(); ++i) {
+            auto [m, sl] = finishing[i];
+            const size_t mi = std::find(models.begin(), models.end(), m) - models.begin();
+            const uint32_t r = seen[mi]++;
+            out[i].theta.assign(m->h_out_theta + (uint64_t)r * m->K, m->h_out_theta + (uint64_t)(r + 1) * m->K);
+            out[i].ll = m->h_out_ll[r];
+        }
+    }
     const auto now = Clock::now();
     ++s->steps;
     {
@@ -350,6 +448,16 @@ tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out)
         CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
         s->d_words = s->dalloc<uint32_t>(cfg->token_budget);
         s->d_z = s->dalloc<uint16_t>(cfg->token_budget);
+        s->d_staging = s->dalloc<uint32_t>(cfg->token_budget);
+        s->h_staging = s->palloc<uint32_t>(cfg->token_budget);
+        const uint64_t maxdocs = cfg->token_budget;
+        s->sc_cap = std::min<uint64_t>(maxdocs, 1u << 22);
+        s->h_sc_src = s->palloc<uint64_t>(std::min<uint64_t>(maxdocs, 1u << 22));
+        s->h_sc_dst = s->palloc<uint64_t>(std::min<uint64_t>(maxdocs, 1u << 22));
+        s->h_sc_len = s->palloc<uint32_t>(std::min<uint64_t>(maxdocs, 1u << 22));
+        s->d_sc_src = s->dalloc<uint64_t>(std::min<uint64_t>(maxdocs, 1u << 22));
+        s->d_sc_dst = s->dalloc<uint64_t>(std::min<uint64_t>(maxdocs, 1u << 22));
+        s->d_sc_len = s->dalloc<uint32_t>(std::min<uint64_t>(maxdocs, 1u << 22));
         s->arena.init(cfg->token_budget);
     } catch (const OomError&) {
         delete s;
@@ -389,16 +497,29 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
     m->slots = S;
     m->active.assign(S, -1);
     m->req.resize(S);
-    m->h_tok_begin.assign(S, 0);
-    m->h_keys.assign(S, 0);
-    m->h_tok_len.assign(S, 0);
-    m->h_it_begin.assign(S, 0);
-    m->h_it_end.assign(S, 0);
-    m->h_it_total.assign(S, 0);
     m->h_done.assign(S, 0);
     std::lock_guard<std::mutex> lk(s->mu);      // the worker does not allocate meanwhile
     try {
         CK(cudaSetDevice(s->device));
+        m->h_tok_begin = s->palloc<uint64_t>(S);
+        m->h_keys = s->palloc<uint64_t>(S);
+        m->h_tok_len = s->palloc<uint32_t>(S);
+        m->h_it_begin = s->palloc<uint32_t>(S);
+        m->h_it_end = s->palloc<uint32_t>(S);
+        m->h_it_total = s->palloc<uint32_t>(S);
+        m->h_work = s->palloc<uint32_t>(S);
+        m->h_fin = s->palloc<uint32_t>(S);
+        m->h_out_theta = s->palloc<float>((uint64_t)S * K);
+        m->h_out_ll = s->palloc<double>(S);
+        std::fill(m->h_tok_begin, m->h_tok_begin + S, 0);
+        std::fill(m->h_keys, m->h_keys + S, 0);
+        std::fill(m->h_tok_len, m->h_tok_len + S, 0);
+        std::fill(m->h_it_begin, m->h_it_begin + S, 0);
+        std::fill(m->h_it_end, m->h_it_end + S, 0);
+        std::fill(m->h_it_total, m->h_it_total + S, 0);
+        m->d_fin = s->dalloc<uint32_t>(S);
+        m->d_out_theta = s->dalloc<float>((uint64_t)S * K);
+        m->d_out_ll = s->dalloc<double>(S);
         m->d_nkw = s->dalloc<int32_t>((uint64_t)K * V);
         m->d_nk = s->dalloc<int32_t>(K);
         m->d_alpha = s->dalloc<float>(K);
