@@ -114,6 +114,17 @@ tmt_status tmt_ll(tmt_handle* h, double* ll_docs, double* ll_rest);
  * column-major), n_k (K), alpha (K, after optimisation). */
 tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t* n_k, float* alpha);
 
+/* Replaces the topic-word state with host arrays n_kw (K x V column-major)
+ * and n_k (K): the state a model loaded without its documents carries
+ * (TopicModel::_loadModel, TopicModel.hpp:361-395).  Later sweeps and
+ * inference use it. */
+tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k);
+/* Replaces alpha (K values > 0), e.g. the optimised alphas of a loaded model. */
+tmt_status tmt_set_alpha(tmt_handle* h, const float* alpha);
+/* Sets the sweep counter (TopicModel::globalStep), e.g. after a load; it keys
+ * the draws and the alpha-optimisation schedule. */
+tmt_status tmt_set_global_step(tmt_handle* h, uint64_t step);
+
 /* Downloads n_dk (D x K row-major int32; DocumentLDA::numByTopic). */
 tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
 
@@ -215,6 +226,79 @@ tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, co
 tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out);
 const char* tmt_last_error(const tmt_handle* h);
 void tmt_destroy(tmt_handle* h);
+
+/* ---- the host model: tomotopy's LDAModel over the engine ----------------
+ * One object per model (tomotopy's LDAModelObject -> ILDAModel,
+ * py_LDA.cpp:151-611, LDAModel.hpp): dictionary and documents on the host,
+ * sampling state on the device.  Word lists cross the ABI as NUL-separated
+ * UTF-8 strings.  Only TermWeight.ONE and symmetric eta. */
+typedef struct tmt_model tmt_model;
+typedef struct tmt_model_args {
+    uint32_t K;
+    const float* alpha;      /* n_alpha == 1 (symmetric) or n_alpha == K */
+    uint32_t n_alpha;
+    float eta;
+    uint64_t seed;
+    uint64_t min_cf, min_df, rm_top;
+    int32_t device;
+    uint32_t sweep_groups;   /* 0: engine default */
+} tmt_model_args;
+typedef struct tmt_model_info {
+    uint32_t K, V, n_vocab;  /* V = realV (used vocabulary); n_vocab = all words seen */
+    uint64_t n_docs, N, global_step;
+    int32_t prepared;
+    float alpha, eta;
+    uint32_t optim_interval, burn_in;
+    uint64_t seed, min_cf, min_df, rm_top;
+} tmt_model_info;
+
+/* LDAModel ctor checks (LDAModel.hpp:962-983). */
+tmt_status tmt_model_create(const tmt_model_args* args, tmt_model** out);
+/* add_doc (TopicModel.hpp:397-449): *doc_id = -1 for an empty document. */
+tmt_status tmt_model_add_doc(tmt_model* m, const char* words, uint32_t n_words, int64_t* doc_id);
+/* LDAModel::prepare (LDAModel.hpp:1073-1138); train() calls it when needed. */
+tmt_status tmt_model_prepare(tmt_model* m);
+/* TopicModel::train (TopicModel.hpp:684-755) for `iters` sweeps. */
+tmt_status tmt_model_train(tmt_model* m, uint32_t iters);
+/* optim_interval / burn_in properties (LDAModel.hpp:1000-1010); before train. */
+tmt_status tmt_model_set_optim(tmt_model* m, uint32_t optim_interval, uint32_t burn_in);
+tmt_status tmt_model_get_info(tmt_model* m, tmt_model_info* out);
+/* getLLDocs + getLLRest in FP64 (LDAModel.hpp:616-674). */
+tmt_status tmt_model_ll(tmt_model* m, double* ll_docs, double* ll_rest);
+/* current alphas (K). */
+tmt_status tmt_model_alpha(tmt_model* m, float* out);
+/* _getWidsByTopic (LDAModel.hpp:828-841): V floats. */
+tmt_status tmt_model_topic_word_dist(tmt_model* m, uint32_t topic, int normalize, float* out);
+/* _getTopicsCount (LDAModel.hpp:815-826): K counts. */
+tmt_status tmt_model_count_by_topics(tmt_model* m, uint64_t* out);
+/* the vocabulary as NUL-separated words (used_only: the first V); *need = bytes. */
+tmt_status tmt_model_vocab(tmt_model* m, uint32_t used_only, char* buf, uint64_t cap, uint64_t* need);
+/* vocabCf / vocabDf over all words (may be NULL). */
+tmt_status tmt_model_vocab_freq(tmt_model* m, uint64_t* cf, uint64_t* df);
+/* a document's word ids and topics in its original word order (py_LDA.cpp:613-619). */
+tmt_status tmt_model_doc(tmt_model* m, uint64_t doc, uint32_t* words, uint16_t* topics, uint32_t* len);
+/* _getTopicsByDoc (LDAModel.hpp:1145-1159) and the document's FP64 getLLDocs. */
+tmt_status tmt_model_doc_topic_dist(tmt_model* m, uint64_t doc, int normalize, float* out, double* ll);
+/* infer (together=False) of D string documents: words joined NUL-separated,
+ * doc_nwords[d] words each; unknown words are dropped (makeDoc). */
+tmt_status tmt_model_infer(tmt_model* m, const char* words, const uint64_t* doc_nwords, uint64_t D, uint32_t iters,
+                           uint64_t seed, float* theta, double* ll);
+/* infer with together=True (LDAModel.hpp:852-893): the D documents are
+ * sampled jointly against the model's counts plus their own; one ll. */
+tmt_status tmt_model_infer_together(tmt_model* m, const char* words, const uint64_t* doc_nwords, uint64_t D,
+                                    uint32_t iters, uint64_t seed, float* theta, double* ll);
+/* tomotopy's model layout (TopicModel.hpp:335-359): *out is malloc'ed; free
+ * it with tmt_model_free_buffer. */
+tmt_status tmt_model_save(tmt_model* m, const uint8_t* extra, uint64_t extra_len, int full, uint8_t** out,
+                          uint64_t* out_len);
+void tmt_model_free_buffer(uint8_t* buf);
+/* _loadModel (TopicModel.hpp:361-395) + prepare(false): *extra is malloc'ed.
+ * device < 0 parses only: queries and save work from the host copy, no GPU
+ * is touched, and training / inference are unavailable. */
+tmt_status tmt_model_load(const uint8_t* data, uint64_t len, int32_t device, uint32_t sweep_groups, tmt_model** out,
+                          uint8_t** extra, uint64_t* extra_len);
+const char* tmt_model_last_error(const tmt_model* m);
+void tmt_model_destroy(tmt_model* m);
 
 /* ---- synthetic corpus (workload generator; not a tomotopy interface) ---- */
 typedef enum tmt_len_kind { TMT_LEN_POISSON = 0, TMT_LEN_LOGNORMAL = 1 } tmt_len_kind;

@@ -43,6 +43,19 @@ class TmtServerStats(C.Structure):
                 ("mean_active", C.c_double), ("tokens_in_flight_max", C.c_uint64)]
 
 
+class TmtModelArgs(C.Structure):
+    _fields_ = [("K", C.c_uint32), ("alpha", C.POINTER(C.c_float)), ("n_alpha", C.c_uint32), ("eta", C.c_float),
+                ("seed", C.c_uint64), ("min_cf", C.c_uint64), ("min_df", C.c_uint64), ("rm_top", C.c_uint64),
+                ("device", C.c_int32), ("sweep_groups", C.c_uint32)]
+
+
+class TmtModelInfo(C.Structure):
+    _fields_ = [("K", C.c_uint32), ("V", C.c_uint32), ("n_vocab", C.c_uint32), ("n_docs", C.c_uint64),
+                ("N", C.c_uint64), ("global_step", C.c_uint64), ("prepared", C.c_int32), ("alpha", C.c_float),
+                ("eta", C.c_float), ("optim_interval", C.c_uint32), ("burn_in", C.c_uint32), ("seed", C.c_uint64),
+                ("min_cf", C.c_uint64), ("min_df", C.c_uint64), ("rm_top", C.c_uint64)]
+
+
 class TmtSynthSpec(C.Structure):
     _fields_ = [("V", C.c_uint32), ("T", C.c_uint32), ("D", C.c_uint64), ("len_kind", C.c_int32),
                 ("len_a", C.c_double), ("len_b", C.c_double), ("len_min", C.c_uint32), ("len_max", C.c_uint32),
@@ -57,6 +70,9 @@ SIGNATURES = {
     "tmt_upload_corpus": (C.c_int, [_H, _P, _P, C.c_uint64, _P]),
     "tmt_train": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P]),
     "tmt_ll": (C.c_int, [_H, _P, _P]),
+    "tmt_set_counts": (C.c_int, [_H, _P, _P]),
+    "tmt_set_alpha": (C.c_int, [_H, _P]),
+    "tmt_set_global_step": (C.c_int, [_H, C.c_uint64]),
     "tmt_infer_batch": (C.c_int, [_H, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P]),
     "tmt_download_state": (C.c_int, [_H, _P, _P, _P, _P]),
     "tmt_download_doc_topic": (C.c_int, [_H, _P]),
@@ -76,6 +92,28 @@ SIGNATURES = {
     "tmt_server_get_stats": (C.c_int, [_H, C.POINTER(TmtServerStats)]),
     "tmt_server_last_error": (C.c_char_p, [_H]),
     "tmt_server_stop": (C.c_int, [_H]),
+    "tmt_model_create": (C.c_int, [C.POINTER(TmtModelArgs), C.POINTER(_H)]),
+    "tmt_model_add_doc": (C.c_int, [_H, C.c_char_p, C.c_uint32, C.POINTER(C.c_int64)]),
+    "tmt_model_prepare": (C.c_int, [_H]),
+    "tmt_model_train": (C.c_int, [_H, C.c_uint32]),
+    "tmt_model_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
+    "tmt_model_get_info": (C.c_int, [_H, C.POINTER(TmtModelInfo)]),
+    "tmt_model_ll": (C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "tmt_model_alpha": (C.c_int, [_H, _P]),
+    "tmt_model_topic_word_dist": (C.c_int, [_H, C.c_uint32, C.c_int, _P]),
+    "tmt_model_count_by_topics": (C.c_int, [_H, _P]),
+    "tmt_model_vocab": (C.c_int, [_H, C.c_uint32, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "tmt_model_vocab_freq": (C.c_int, [_H, _P, _P]),
+    "tmt_model_doc": (C.c_int, [_H, C.c_uint64, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_model_doc_topic_dist": (C.c_int, [_H, C.c_uint64, C.c_int, _P, C.POINTER(C.c_double)]),
+    "tmt_model_infer": (C.c_int, [_H, C.c_char_p, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P]),
+    "tmt_model_infer_together": (C.c_int, [_H, C.c_char_p, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P]),
+    "tmt_model_save": (C.c_int, [_H, _P, C.c_uint64, C.c_int, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_uint64)]),
+    "tmt_model_free_buffer": (None, [C.POINTER(C.c_uint8)]),
+    "tmt_model_load": (C.c_int, [_P, C.c_uint64, C.c_int32, C.c_uint32, C.POINTER(_H), C.POINTER(C.POINTER(C.c_uint8)),
+                                 C.POINTER(C.c_uint64)]),
+    "tmt_model_last_error": (C.c_char_p, [_H]),
+    "tmt_model_destroy": (None, [_H]),
     "tmt_synth_corpus": (C.c_int, [C.POINTER(TmtSynthSpec), _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 

@@ -1099,6 +1099,39 @@ tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk)
     });
 }
 
+tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_counts before the corpus was uploaded");
+        if (!n_kw || !n_k) throw ArgError("n_kw / n_k is NULL");
+        const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
+        if (kv) CK(cudaMemcpyAsync(h->d_nkw[h->cur], n_kw, kv * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_nk[h->cur], n_k, h->cfg.K * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_set_alpha(tmt_handle* h, const float* alpha)
+{
+    if (!h || !alpha) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_alpha before the corpus was uploaded");
+        for (uint32_t k = 0; k < h->cfg.K; ++k)
+            if (!(alpha[k] > 0)) throw ArgError("wrong alpha value");
+        std::copy(alpha, alpha + h->cfg.K, h->alpha.begin());
+        CK(cudaMemcpyAsync(h->d_alpha, h->alpha.data(), h->cfg.K * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_set_global_step(tmt_handle* h, uint64_t step)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    h->global_step = step;
+    return TMT_OK;
+}
+
 tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
 {
     if (!h || !out) return TMT_ERR_INVALID_ARGUMENT;
