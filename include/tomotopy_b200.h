@@ -124,6 +124,12 @@ tmt_status tmt_set_alpha(tmt_handle* h, const float* alpha);
 /* Sets the sweep counter (TopicModel::globalStep), e.g. after a load; it keys
  * the draws and the alpha-optimisation schedule. */
 tmt_status tmt_set_global_step(tmt_handle* h, uint64_t step);
+/* Sets the seed that keys the sweep draws (the model's random generator, which
+ * tomotopy's copy() carries over: LDAModel.hpp copy constructor via TopicModel's rg). */
+tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed);
+/* Sets the alpha-optimisation schedule between train() calls
+ * (LDAModel::optimInterval / burnIn, python setters py_LDA.cpp). */
+tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_in);
 
 /* Downloads n_dk (D x K row-major int32; DocumentLDA::numByTopic). */
 tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
@@ -260,8 +266,10 @@ tmt_status tmt_model_add_doc(tmt_model* m, const char* words, uint32_t n_words, 
 tmt_status tmt_model_prepare(tmt_model* m);
 /* TopicModel::train (TopicModel.hpp:684-755) for `iters` sweeps. */
 tmt_status tmt_model_train(tmt_model* m, uint32_t iters);
-/* optim_interval / burn_in properties (LDAModel.hpp:1000-1010); before train. */
+/* optim_interval / burn_in properties (LDAModel.hpp:1000-1010); any time between train() calls. */
 tmt_status tmt_model_set_optim(tmt_model* m, uint32_t optim_interval, uint32_t burn_in);
+/* Sets the seed of the model's sweep draws (copy() keeps the original's). */
+tmt_status tmt_model_set_seed(tmt_model* m, uint64_t seed);
 tmt_status tmt_model_get_info(tmt_model* m, tmt_model_info* out);
 /* getLLDocs + getLLRest in FP64 (LDAModel.hpp:616-674). */
 tmt_status tmt_model_ll(tmt_model* m, double* ll_docs, double* ll_rest);

@@ -73,6 +73,8 @@ SIGNATURES = {
     "tmt_set_counts": (C.c_int, [_H, _P, _P]),
     "tmt_set_alpha": (C.c_int, [_H, _P]),
     "tmt_set_global_step": (C.c_int, [_H, C.c_uint64]),
+    "tmt_set_seed": (C.c_int, [_H, C.c_uint64]),
+    "tmt_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
     "tmt_infer_batch": (C.c_int, [_H, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P]),
     "tmt_download_state": (C.c_int, [_H, _P, _P, _P, _P]),
     "tmt_download_doc_topic": (C.c_int, [_H, _P]),
@@ -97,6 +99,7 @@ SIGNATURES = {
     "tmt_model_prepare": (C.c_int, [_H]),
     "tmt_model_train": (C.c_int, [_H, C.c_uint32]),
     "tmt_model_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
+    "tmt_model_set_seed": (C.c_int, [_H, C.c_uint64]),
     "tmt_model_get_info": (C.c_int, [_H, C.POINTER(TmtModelInfo)]),
     "tmt_model_ll": (C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "tmt_model_alpha": (C.c_int, [_H, _P]),

@@ -1132,6 +1132,21 @@ tmt_status tmt_set_global_step(tmt_handle* h, uint64_t step)
     return TMT_OK;
 }
 
+tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    h->cfg.seed = seed;
+    return TMT_OK;
+}
+
+tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_in)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    h->cfg.optim_interval = optim_interval;
+    h->cfg.burn_in = burn_in;
+    return TMT_OK;
+}
+
 tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
 {
     if (!h || !out) return TMT_ERR_INVALID_ARGUMENT;

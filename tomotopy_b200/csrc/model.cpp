@@ -682,9 +682,18 @@ tmt_status tmt_model_set_optim(tmt_model* m, uint32_t optim_interval, uint32_t b
 {
     if (!m) return TMT_ERR_INVALID_ARGUMENT;
     return guard(m, [&] {
-        if (m->eng) throw ArgErr("optim_interval / burn_in must be set before train()");
         m->optim_interval = optim_interval;
         m->burn_in = burn_in;
+        if (m->eng) m->check(tmt_set_optim(m->eng, optim_interval, burn_in));
+    });
+}
+
+tmt_status tmt_model_set_seed(tmt_model* m, uint64_t seed)
+{
+    if (!m) return TMT_ERR_INVALID_ARGUMENT;
+    return guard(m, [&] {
+        m->seed = seed;
+        if (m->eng) m->check(tmt_set_seed(m->eng, seed));
     });
 }
 

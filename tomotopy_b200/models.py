@@ -372,6 +372,9 @@ class LDAModel:
             inst.init_params = pickle.loads(extra) if extra else {}
         except Exception:
             inst.init_params = {}
+        seed = inst.init_params.get("seed") if isinstance(inst.init_params, dict) else None
+        if isinstance(seed, int):
+            _check(lib.tmt_model_set_seed(h, seed & 0xFFFFFFFFFFFFFFFF), h)
         return inst
 
     @classmethod
@@ -381,8 +384,9 @@ class LDAModel:
 
     def copy(self) -> "LDAModel":
         """A deep copy (through the binary layout)."""
-        c = type(self).loads(self.saves(full=True))
+        c = type(self).loads(self.saves(full=True), device=int(self.init_params.get("device", 0)))
         c.init_params = deepcopy(self.init_params)
+        _check(lib.tmt_model_set_seed(c._h, self._info().seed), c._h)
         return c
 
     # -- properties --------------------------------------------------------------
