@@ -49,6 +49,12 @@ def bytes_per_sweep(N, K, V):
     return N * (4 * K + 16) + 8 * K * V + 4 * (V + 1) + 8 * K
 
 
+# DRAM bytes of one sweep (k_sweep_doc + k_phi_copy over all document groups),
+# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of the same
+# workload (profiles/k_sweep_doc_c3_traffic.md); keyed by (config, D, groups).
+MEASURED_TRAFFIC = {("c3", 1000000, 8): 122.207e9}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -468,8 +474,12 @@ def main():
                        "tokens": int(N), "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups), "parallelism": f"dp{world} (independent chains)",
                        "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": MEASURED_TRAFFIC.get((args.config, int(len(off) - 1), int(info.sweep_groups))),
                          "kernel": "k_sweep_doc", "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg,
+                         "per": "one sweep = all k_sweep_doc + k_phi_copy launches of the document groups",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                           "profiles/k_sweep_doc_c3_traffic.md",
                          "peak_source": peak_kind},
             "e2e": e2e_obj,
             "gpu_launches": int(launches),
