@@ -172,6 +172,10 @@ typedef struct tmt_server_stats {
     uint64_t steps, completed, queued;
     double mean_active;          /* documents per step, averaged over steps */
     uint64_t tokens_in_flight_max;
+    uint64_t token_sweeps;       /* token-sweeps advanced (document length x sweeps) */
+    double alg_bytes;            /* token-sweeps x (4K + 8): the frozen n_kw column per draw + z */
+    double kernel_ms;            /* device time of the inference launches (CUDA events) */
+    double busy_ms;              /* wall time of the steps */
 } tmt_server_stats;
 
 tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out);
@@ -187,6 +191,16 @@ tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* w
  * completion. */
 tmt_status tmt_server_poll(tmt_server* s, uint32_t wait_ms, uint64_t* request_id, uint32_t* model_id,
                            float* theta, uint32_t theta_cap, double* ll, double* latency_ms);
+/* Queues n documents (document d = wid[doc_off[d] .. doc_off[d+1]), model
+ * model_ids[d], key keys[d] or 0) under one lock; request_ids[d] gets each id. */
+tmt_status tmt_server_submit_batch(tmt_server* s, const uint32_t* model_ids, const uint32_t* wid,
+                                   const uint64_t* doc_off, uint64_t n, uint32_t iters, uint64_t seed,
+                                   const uint64_t* keys, uint64_t* request_ids);
+/* Waits up to wait_ms for finished documents and returns up to max_n of them
+ * (*n_out); result i has theta at theta + i * theta_stride (theta_stride >= K). */
+tmt_status tmt_server_poll_batch(tmt_server* s, uint32_t wait_ms, uint64_t max_n, uint64_t* request_ids,
+                                 uint32_t* model_ids, float* theta, uint32_t theta_stride, double* ll,
+                                 double* latency_ms, uint64_t* n_out);
 tmt_status tmt_server_get_stats(tmt_server* s, tmt_server_stats* out);
 const char* tmt_server_last_error(const tmt_server* s);
 /* Stops the worker (queued and running documents are dropped) and frees the server. */

@@ -111,3 +111,44 @@ def test_admission_by_token_budget_and_bounded_waits():
     with pytest.raises(ValueError):
         srv.submit(mid, np.zeros(301, np.uint32), iters=10)
     srv.close()
+
+
+def test_batch_submit_and_poll():
+    e1, e2 = model(24, seed=2), model(130, V=800, seed=4)
+    d1, d2 = docs(e1.V, 40, seed=8), docs(e2.V, 40, seed=9)
+    k1 = np.arange(40, dtype=np.uint64) * 3
+    t1, l1 = batch_ref(e1, d1, 20, 3, k1)
+    t2, l2 = batch_ref(e2, d2, 20, 3, np.zeros(40))
+    srv = T.Server(max_slots=8, token_budget=3000, step_token_sweeps=300, max_doc_len=1000)
+    m1, m2 = srv.add_engine_model(e1), srv.add_engine_model(e2)
+    allds = d1 + d2
+    off = np.concatenate([[0], np.cumsum([len(d) for d in allds])]).astype(np.uint64)
+    w = np.concatenate(allds).astype(np.uint32)
+    mids = np.array([m1] * 40 + [m2] * 40, np.uint32)
+    keys = np.concatenate([k1, np.zeros(40, np.uint64)])
+    rids = srv.submit_batch(mids, off, w, iters=20, seed=3, keys=keys)
+    assert len(set(rids.tolist())) == 80
+    where = {int(r): i for i, r in enumerate(rids)}
+    got = 0
+    t0 = time.time()
+    while got < 80 and time.time() - t0 < 60:
+        r = srv.poll_batch(max_n=7, wait_ms=2000)
+        if r is None:
+            continue
+        rid, mid, th, ll, lat = r
+        assert len(rid) <= 7
+        for j in range(len(rid)):
+            i = where[int(rid[j])]
+            if i < 40:
+                assert mid[j] == m1
+                np.testing.assert_array_equal(th[j, :24], t1[i]); assert ll[j] == l1[i]
+            else:
+                assert mid[j] == m2
+                np.testing.assert_array_equal(th[j, :130], t2[i - 40]); assert ll[j] == l2[i - 40]
+            assert lat[j] > 0
+        got += len(rid)
+    assert got == 80
+    assert srv.poll_batch(max_n=4, wait_ms=20) is None
+    st = srv.stats()
+    assert st.kernel_ms > 0 and st.busy_ms >= st.kernel_ms * 0.5 and st.token_sweeps > 0
+    srv.close()

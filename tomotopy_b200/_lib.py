@@ -40,7 +40,9 @@ class TmtServerConfig(C.Structure):
 
 class TmtServerStats(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("completed", C.c_uint64), ("queued", C.c_uint64),
-                ("mean_active", C.c_double), ("tokens_in_flight_max", C.c_uint64)]
+                ("mean_active", C.c_double), ("tokens_in_flight_max", C.c_uint64),
+                ("token_sweeps", C.c_uint64), ("alg_bytes", C.c_double), ("kernel_ms", C.c_double),
+                ("busy_ms", C.c_double)]
 
 
 class TmtModelArgs(C.Structure):
@@ -91,6 +93,9 @@ SIGNATURES = {
                                     C.POINTER(C.c_uint64)]),
     "tmt_server_poll": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), _P, C.c_uint32,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "tmt_server_submit_batch": (C.c_int, [_H, _P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P]),
+    "tmt_server_poll_batch": (C.c_int, [_H, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, _P, _P,
+                                        C.POINTER(C.c_uint64)]),
     "tmt_server_get_stats": (C.c_int, [_H, C.POINTER(TmtServerStats)]),
     "tmt_server_last_error": (C.c_char_p, [_H]),
     "tmt_server_stop": (C.c_int, [_H]),

@@ -136,6 +136,29 @@ k_infer_slots(InferArgs a)
                 re += 32;
             }
         };
+        // the frozen n_kw column of word `v_have`, this lane's blocks of four,
+        // loaded once per run of a word.  (Loading the next token's column
+        // during the current draw measured slower on B200: the extra registers
+        // cost more occupancy than the hidden latency gained.)
+        int4 gv[CHR];
+        uint32_t v_have = 0xFFFFFFFFu;
+        auto load_col = [&](uint32_t v, int4 (&g)[CHR]) {
+            const int32_t* col = a.nkw + (uint64_t)v * K;
+#pragma unroll
+            for (int jj = 0; jj < CHR; ++jj) {
+                if (jj < nch) {
+                    const int k0 = 128 * jj + 4 * lane;
+                    if (vecg) {
+                        g[jj] = __ldg(reinterpret_cast<const int4*>(col + k0));
+                    } else {
+                        g[jj].x = __ldg(col + k0);
+                        g[jj].y = k0 + 1 < K ? __ldg(col + k0 + 1) : 0;
+                        g[jj].z = k0 + 2 < K ? __ldg(col + k0 + 2) : 0;
+                        g[jj].w = k0 + 3 < K ? __ldg(col + k0 + 3) : 0;
+                    }
+                }
+            }
+        };
         for (uint32_t it = it0; it < it1; ++it) {
             uint32_t run_b = 0, run_e = 0;      // the multi-token run whose histogram is in `own`
             for (uint32_t base = 0; base < L; base += 32) {
@@ -167,6 +190,7 @@ k_infer_slots(InferArgs a)
                     }
                     const bool multi = j < run_e;
                     const int32_t* gcol = a.nkw + (uint64_t)v * K;
+                    if (CH > 0 && v != v_have) { load_col(v, gv); v_have = v; }
                     if (lane == 0) {
                         if (multi) own[zo] -= 1;
                         const int n = rowi[zo] - 1;
@@ -184,16 +208,7 @@ k_infer_slots(InferArgs a)
                                 const int k0 = 128 * jj + 4 * lane;
                                 const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
                                 const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
-                                int g0, g1 = 0, g2 = 0, g3 = 0;
-                                if (vecg) {
-                                    const int4 G4 = __ldg(reinterpret_cast<const int4*>(gcol + k0));
-                                    g0 = G4.x; g1 = G4.y; g2 = G4.z; g3 = G4.w;
-                                } else {
-                                    g0 = __ldg(gcol + k0);
-                                    if (k0 + 1 < K) g1 = __ldg(gcol + k0 + 1);
-                                    if (k0 + 2 < K) g2 = __ldg(gcol + k0 + 2);
-                                    if (k0 + 3 < K) g3 = __ldg(gcol + k0 + 3);
-                                }
+                                int g0 = gv[jj].x, g1 = gv[jj].y, g2 = gv[jj].z, g3 = gv[jj].w;
                                 if (multi) {
                                     const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
                                     g0 += O4.x; g1 += O4.y; g2 += O4.z; g3 += O4.w;

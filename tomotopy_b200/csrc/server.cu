@@ -4,7 +4,8 @@
 // A worker thread runs steps.  Each step it admits queued requests into free
 // slots of their model's slot pool and into free space of the shared token
 // arena (the HBM budget for documents in flight), then launches the
-// resumable inference kernel (infer.cuh) once per model with active slots,
+// resumable inference kernel (infer.cuh) once per model with active slots
+// (each model on its own stream, so the models of one step run concurrently),
 // advancing every active document by ceil(step_token_sweeps / length) sweeps
 // (at least one), so long documents do not stall a step.  Documents that have
 // done all their sweeps leave with their theta and log-likelihood.  Requests
@@ -122,6 +123,8 @@ struct Arena {
 };
 
 struct Model {
+    cudaStream_t stream = nullptr;       // this model's launches; models of one step run concurrently
+    cudaEvent_t ev_done = nullptr;
     uint32_t K = 0, V = 0;
     float eta = 0;
     std::vector<float> alpha;
@@ -186,6 +189,10 @@ struct tmt_server {
     tmt_status worker_status = TMT_OK;
     // statistics
     uint64_t steps = 0, completed = 0, active_sum = 0, tokens_in_flight_max = 0;
+    uint64_t token_sweeps = 0;                   // token-sweeps advanced
+    double alg_bytes = 0;                        // token-sweeps x (4K + 8) per model
+    double kernel_ms = 0, busy_ms = 0;           // inference launches (events); whole steps (wall)
+    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
 
     template <class T>
     T* dalloc(size_t n)
@@ -213,6 +220,12 @@ struct tmt_server {
         if (stream) cudaStreamSynchronize(stream);
         for (void* p : allocs) cudaFree(p);
         for (void* p : pinned_allocs) cudaFreeHost(p);
+        for (auto& m : models) {
+            if (m->ev_done) cudaEventDestroy(m->ev_done);
+            if (m->stream) cudaStreamDestroy(m->stream);
+        }
+        if (ev_k0) cudaEventDestroy(ev_k0);
+        if (ev_k1) cudaEventDestroy(ev_k1);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -222,6 +235,7 @@ namespace {
 // One step of the worker; returns false when there was nothing to do.
 bool server_step(tmt_server* s)
 {
+    const auto t_step = Clock::now();
     std::vector<std::pair<Model*, uint32_t>> admitted;   // (model, slot)
     std::vector<Model*> models;                          // tmt_server_add_model may append meanwhile
     {
@@ -274,6 +288,7 @@ bool server_step(tmt_server* s)
     bool any = false;
     std::vector<std::pair<Model*, uint32_t>> finishing;
     std::vector<uint32_t> nfin(models.size(), 0);
+    std::vector<char> active_model(models.size(), 0);
     for (size_t mi = 0; mi < models.size(); ++mi) {
         Model* m = models[mi];
         std::vector<uint32_t> work;
@@ -283,6 +298,9 @@ bool server_step(tmt_server* s)
             const uint32_t adv = std::max(1u, (s->cfg.step_token_sweeps + len - 1) / len);
             m->h_it_begin[sl] = m->h_done[sl];
             m->h_it_end[sl] = std::min(m->h_it_total[sl], m->h_done[sl] + adv);
+            const uint64_t ts = (uint64_t)(m->h_it_end[sl] - m->h_it_begin[sl]) * m->h_tok_len[sl];
+            s->token_sweeps += ts;
+            s->alg_bytes += (double)ts * (4.0 * m->K + 8.0);
             work.push_back(sl);
             if (m->h_it_end[sl] == m->h_it_total[sl]) {
                 finishing.emplace_back(m, sl);
@@ -290,18 +308,22 @@ bool server_step(tmt_server* s)
             }
         }
         if (work.empty()) continue;
+        if (!any) CK(cudaEventRecord(s->ev_k0, s->stream));   // the fork: admitted documents are in place
         any = true;
+        cudaStream_t ms = m->stream;
+        active_model[mi] = 1;
+        CK(cudaStreamWaitEvent(ms, s->ev_k0, 0));
         s->active_sum += work.size();
         const size_t S = m->slots;
-        CK(cudaMemcpyAsync(m->d_tok_begin, m->h_tok_begin, S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_tok_len, m->h_tok_len, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_keys, m->h_keys, S * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_begin, m->h_it_begin, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_end, m->h_it_end, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemcpyAsync(m->d_it_total, m->h_it_total, S * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(m->d_tok_begin, m->h_tok_begin, S * sizeof(uint64_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemcpyAsync(m->d_tok_len, m->h_tok_len, S * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemcpyAsync(m->d_keys, m->h_keys, S * sizeof(uint64_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemcpyAsync(m->d_it_begin, m->h_it_begin, S * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemcpyAsync(m->d_it_end, m->h_it_end, S * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemcpyAsync(m->d_it_total, m->h_it_total, S * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
         std::copy(work.begin(), work.end(), m->h_work);
-        CK(cudaMemcpyAsync(m->d_work, m->h_work, work.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
+        CK(cudaMemcpyAsync(m->d_work, m->h_work, work.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
+        CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), ms));
         InferArgs a{};
         a.nkw = m->d_nkw;
         a.nk = m->d_nk;
@@ -337,18 +359,18 @@ bool server_step(tmt_server* s)
         for (uint32_t sl : work) by_seed[m->req[sl].seed].push_back(sl);
         if (by_seed.size() == 1) {
             a.key = by_seed.begin()->first ^ (uint64_t)tmt::kStreamInfer;
-            launch_infer(a, s->num_sms, s->stream);
+            launch_infer(a, s->num_sms, ms);
         } else {
             uint32_t at = 0;
             for (auto& [seed, sls] : by_seed) {
                 std::copy(sls.begin(), sls.end(), m->h_work + at);
-                CK(cudaMemcpyAsync(m->d_work + at, m->h_work + at, sls.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+                CK(cudaMemcpyAsync(m->d_work + at, m->h_work + at, sls.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ms));
                 a.work = m->d_work + at;
                 at += (uint32_t)sls.size();
-                CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), s->stream));
+                CK(cudaMemsetAsync(m->d_counter, 0, sizeof(uint32_t), ms));
                 a.n_work = (uint32_t)sls.size();
                 a.key = seed ^ (uint64_t)tmt::kStreamInfer;
-                launch_infer(a, s->num_sms, s->stream);
+                launch_infer(a, s->num_sms, ms);
             }
         }
     }
@@ -357,15 +379,27 @@ bool server_step(tmt_server* s)
     for (size_t mi = 0; mi < models.size(); ++mi) {
         Model* m = models[mi];
         const uint32_t n = nfin[mi];
-        if (!n) continue;
-        CK(cudaMemcpyAsync(m->d_fin, m->h_fin, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-        k_gather_results<<<std::min<uint32_t>(n, 4096), 128, 0, s->stream>>>(m->d_theta, m->d_ll, m->d_fin, n, m->K,
-                                                                             m->d_out_theta, m->d_out_ll);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(m->h_out_theta, m->d_out_theta, (uint64_t)n * m->K * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaMemcpyAsync(m->h_out_ll, m->d_out_ll, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        if (n) {
+            CK(cudaMemcpyAsync(m->d_fin, m->h_fin, n * sizeof(uint32_t), cudaMemcpyHostToDevice, m->stream));
+            k_gather_results<<<std::min<uint32_t>(n, 4096), 128, 0, m->stream>>>(m->d_theta, m->d_ll, m->d_fin, n,
+                                                                                 m->K, m->d_out_theta, m->d_out_ll);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(m->h_out_theta, m->d_out_theta, (uint64_t)n * m->K * sizeof(float),
+                               cudaMemcpyDeviceToHost, m->stream));
+            CK(cudaMemcpyAsync(m->h_out_ll, m->d_out_ll, n * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+        }
+        if (active_model[mi]) {     // the join
+            CK(cudaEventRecord(m->ev_done, m->stream));
+            CK(cudaStreamWaitEvent(s->stream, m->ev_done, 0));
+        }
     }
+    CK(cudaEventRecord(s->ev_k1, s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, s->ev_k0, s->ev_k1));
+        s->kernel_ms += ms;
+    }
     std::vector<Result> out(finishing.size());
     {
         std::vector<uint32_t> seen(models.size(), 0);
@@ -379,6 +413,7 @@ bool server_step(tmt_server* s)
     }
     const auto now = Clock::now();
     ++s->steps;
+    s->busy_ms += std::chrono::duration<double, std::milli>(now - t_step).count();
     {
         std::lock_guard<std::mutex> lk(s->mu);
         for (Model* m : models)
@@ -446,6 +481,8 @@ tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out)
         CK(cudaSetDevice(s->device));
         CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
         CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
+        CK(cudaEventCreate(&s->ev_k0));
+        CK(cudaEventCreate(&s->ev_k1));
         s->d_words = s->dalloc<uint32_t>(cfg->token_budget);
         s->d_z = s->dalloc<uint16_t>(cfg->token_budget);
         s->d_staging = s->dalloc<uint32_t>(cfg->token_budget);
@@ -501,6 +538,8 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
     std::lock_guard<std::mutex> lk(s->mu);      // the worker does not allocate meanwhile
     try {
         CK(cudaSetDevice(s->device));
+        CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&m->ev_done, cudaEventDisableTiming));
         m->h_tok_begin = s->palloc<uint64_t>(S);
         m->h_keys = s->palloc<uint64_t>(S);
         m->h_tok_len = s->palloc<uint32_t>(S);
@@ -585,17 +624,82 @@ tmt_status tmt_server_poll(tmt_server* s, uint32_t wait_ms, uint64_t* request_id
         if (s->worker_status != TMT_OK) return s->worker_status;
         return TMT_ERR_TIMEOUT;
     }
+    if (theta && theta_cap < s->results.front().theta.size()) return TMT_ERR_INVALID_ARGUMENT;   // kept queued
     Result r = std::move(s->results.front());
     s->results.pop_front();
     lk.unlock();
     *request_id = r.id;
     if (model_id) *model_id = r.model;
-    if (theta) {
-        if (theta_cap < r.theta.size()) return TMT_ERR_INVALID_ARGUMENT;
-        std::memcpy(theta, r.theta.data(), r.theta.size() * sizeof(float));
-    }
+    if (theta) std::memcpy(theta, r.theta.data(), r.theta.size() * sizeof(float));
     if (ll) *ll = r.ll;
     if (latency_ms) *latency_ms = r.latency_ms;
+    return TMT_OK;
+}
+
+tmt_status tmt_server_submit_batch(tmt_server* s, const uint32_t* model_ids, const uint32_t* wid,
+                                   const uint64_t* doc_off, uint64_t n, uint32_t iters, uint64_t seed,
+                                   const uint64_t* keys, uint64_t* request_ids)
+{
+    if (!s || (n && (!model_ids || !doc_off || !request_ids))) return TMT_ERR_INVALID_ARGUMENT;
+    std::vector<Request> rs(n);
+    for (uint64_t d = 0; d < n; ++d) {
+        if (doc_off[d + 1] < doc_off[d]) return TMT_ERR_INVALID_ARGUMENT;
+        const uint64_t len = doc_off[d + 1] - doc_off[d];
+        if (len > s->cfg.max_doc_len || (len && !wid)) return TMT_ERR_INVALID_ARGUMENT;
+        Request& r = rs[d];
+        r.words.assign(wid + doc_off[d], wid + doc_off[d + 1]);
+        std::stable_sort(r.words.begin(), r.words.end());
+        r.iters = iters;
+        r.seed = seed;
+        r.key = keys ? keys[d] : 0;
+    }
+    const auto now = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
+        for (uint64_t d = 0; d < n; ++d)
+            if (model_ids[d] >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
+        for (uint64_t d = 0; d < n; ++d) {
+            Request& r = rs[d];
+            r.model = model_ids[d];
+            r.id = s->next_id++;
+            r.t_submit = now;
+            request_ids[d] = r.id;
+            s->queue.push_back(std::move(r));
+        }
+    }
+    s->cv_work.notify_one();
+    return TMT_OK;
+}
+
+tmt_status tmt_server_poll_batch(tmt_server* s, uint32_t wait_ms, uint64_t max_n, uint64_t* request_ids,
+                                 uint32_t* model_ids, float* theta, uint32_t theta_stride, double* ll,
+                                 double* latency_ms, uint64_t* n_out)
+{
+    if (!s || !request_ids || !n_out || max_n == 0) return TMT_ERR_INVALID_ARGUMENT;
+    *n_out = 0;
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !s->results.empty() || s->stop; });
+    if (s->results.empty()) {
+        if (s->worker_status != TMT_OK) return s->worker_status;
+        return TMT_ERR_TIMEOUT;
+    }
+    uint64_t n = 0;
+    while (n < max_n && !s->results.empty()) {
+        const Result& r = s->results.front();
+        if (theta && theta_stride < r.theta.size()) {
+            if (n == 0) return TMT_ERR_INVALID_ARGUMENT;   // kept queued
+            break;
+        }
+        request_ids[n] = r.id;
+        if (model_ids) model_ids[n] = r.model;
+        if (theta) std::memcpy(theta + n * theta_stride, r.theta.data(), r.theta.size() * sizeof(float));
+        if (ll) ll[n] = r.ll;
+        if (latency_ms) latency_ms[n] = r.latency_ms;
+        s->results.pop_front();
+        ++n;
+    }
+    *n_out = n;
     return TMT_OK;
 }
 
@@ -608,6 +712,10 @@ tmt_status tmt_server_get_stats(tmt_server* s, tmt_server_stats* out)
     out->queued = s->queue.size();
     out->mean_active = s->steps ? (double)s->active_sum / (double)s->steps : 0.0;
     out->tokens_in_flight_max = s->tokens_in_flight_max;
+    out->token_sweeps = s->token_sweeps;
+    out->alg_bytes = s->alg_bytes;
+    out->kernel_ms = s->kernel_ms;
+    out->busy_ms = s->busy_ms;
     return TMT_OK;
 }
 

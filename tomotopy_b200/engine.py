@@ -186,6 +186,37 @@ class Server:
             raise TmtError(st, lib.tmt_server_last_error(self.h).decode())
         return rid.value, mid.value, theta[:self.K[mid.value]].copy(), ll.value, lat.value
 
+    def submit_batch(self, model_ids, doc_off, words, iters=100, seed=0, keys=None):
+        """Queues len(doc_off) - 1 documents at once; returns their request ids."""
+        off = np.ascontiguousarray(doc_off, dtype=np.uint64)
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        n = len(off) - 1
+        mids = np.ascontiguousarray(np.broadcast_to(np.asarray(model_ids, np.uint32), (n,)))
+        k = np.ascontiguousarray(keys, dtype=np.uint64) if keys is not None else None
+        rids = np.zeros(max(n, 1), dtype=np.uint64)
+        check(lib.tmt_server_submit_batch(self.h, _p(mids), _p(w), _p(off), n, int(iters), int(seed), _p(k),
+                                          _p(rids)), None, "tmt_server_submit_batch")
+        return rids[:n]
+
+    def poll_batch(self, max_n=4096, wait_ms=1000):
+        """Up to max_n finished documents as arrays (request_id, model_id,
+        theta [n x max K], ll, latency_ms), or None on timeout."""
+        cap = max(self.K.values()) if self.K else 1
+        rid = np.zeros(max_n, np.uint64)
+        mid = np.zeros(max_n, np.uint32)
+        theta = np.zeros((max_n, cap), np.float32)
+        ll = np.zeros(max_n, np.float64)
+        lat = np.zeros(max_n, np.float64)
+        n = C.c_uint64()
+        st = lib.tmt_server_poll_batch(self.h, int(wait_ms), int(max_n), _p(rid), _p(mid), _p(theta), cap, _p(ll),
+                                       _p(lat), C.byref(n))
+        if st == -7:
+            return None
+        if st != 0:
+            raise TmtError(st, lib.tmt_server_last_error(self.h).decode())
+        k = n.value
+        return rid[:k], mid[:k], theta[:k], ll[:k], lat[:k]
+
     def stats(self):
         s = TmtServerStats()
         check(lib.tmt_server_get_stats(self.h, C.byref(s)), None, "tmt_server_get_stats")
