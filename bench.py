@@ -123,6 +123,31 @@ def make_corpus(w, threads=0):
     return off, words, realV
 
 
+def make_shard(w, rank, world):
+    """Rank r's part of one corpus split across ranks: the documents
+    [r*D, (r+1)*D) of the seeded generator, prepared with the vocabulary order
+    of the whole corpus (the ranks' (cf, df) summed), and every rank's
+    document lengths."""
+    import torch
+    import torch.distributed as dist
+    import tomotopy_b200 as T
+    from tomotopy_b200 import shard as S
+    off, words = T.synth_corpus(w["V"], w["T"], w["D"], w["length"], seed=w["seed"], doc_offset=rank * w["D"])
+
+    def sum_counts(cf, df):
+        t = torch.from_numpy(np.concatenate([cf, df]).astype(np.int64)).cuda()
+        dist.all_reduce(t)
+        a = t.cpu().numpy().astype(np.uint64)
+        cf[:] = a[:len(cf)]
+        df[:] = a[len(cf):]
+
+    off, words, V, _ = S.prepare_ids(off, words, w["V"], sum_counts)
+    lens = torch.from_numpy(np.diff(off.astype(np.int64))).cuda()
+    allg = torch.empty(world * len(lens), dtype=torch.int64, device="cuda")
+    dist.all_gather_into_tensor(allg, lens)
+    return off, words, V, allg.cpu().numpy().astype(np.uint64)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -449,15 +474,41 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import tomotopy_b200 as T
 
-    off, words, V = make_corpus(w)
     K = w["K"]
-    # documents sharded across ranks (weak scaling: every rank holds a full-size corpus
-    # of its own documents; ranks are independent chains)
-    eng = T.Engine(K, V, alpha=ALPHA, eta=ETA, seed=1 + rank, optim_interval=0, device=local,
-                   sweep_groups=args.groups)
-    eng.upload(off, words)
+    if world > 1:
+        # one corpus split across the ranks (weak scaling: every rank holds a
+        # full-size share); one chain, n_kw deltas summed per group over NCCL
+        from tomotopy_b200 import shard as S
+        off, words, V, lens_global = make_shard(w, rank, world)
+
+        def new_engine():
+            return S.ShardedEngine(K, V, alpha=ALPHA, eta=ETA, seed=1, optim_interval=0, device=local,
+                                   sweep_groups=args.groups)
+
+        def upload(e, o, ws):
+            e.upload_shard(o, ws, lens_global, rank * w["D"], rank, world)
+    else:
+        off, words, V = make_corpus(w)
+
+        def new_engine():
+            return T.Engine(K, V, alpha=ALPHA, eta=ETA, seed=1, optim_interval=0, device=local,
+                            sweep_groups=args.groups)
+
+        def upload(e, o, ws):
+            e.upload(o, ws)
+
+    def total(x, op="sum"):
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX if op == "max"
+                                         else torch.distributed.ReduceOp.SUM)
+        return float(t.item())
+
+    eng = new_engine()
+    upload(eng, off, words)
     info0 = eng.info()
     N = info0.N
+    N_all_ranks = int(total(N))
     eng.train(args.warmup)
     if world > 1:
         torch.distributed.barrier()
@@ -472,13 +523,11 @@ def main():
     launches = info.kernel_launches - launches0
     clk = clocks.stop()
     kernel_ms = info.sweep_kernel_ms / max(info.sweeps_timed, 1)
-    # device time of the K sweeps: sum of per-sweep events (kernel + the n_kw copy)
-    step_ms = wall * 1000 / args.steps
-    t_dev = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t_dev, op=torch.distributed.ReduceOp.MAX)
-    step_ms = float(t_dev.item())
-    value = N * world * 1000.0 / step_ms
+    # device time of the K sweeps (CUDA events on the engine's stream around the
+    # whole train call), the max over ranks
+    step_ms = total(info.train_ms / args.steps, "max")
+    wall_ms = total(wall * 1000 / args.steps, "max")
+    value = N_all_ranks * 1000.0 / step_ms
 
     # e2e through the C ABI from host buffers: upload + steps + ll + download
     if args.no_e2e:
@@ -488,19 +537,20 @@ def main():
         eng.close()
         pin_words = torch.from_numpy(words).pin_memory().numpy()
         pin_off = torch.from_numpy(off).pin_memory().numpy()
-        e2e = T.Engine(K, V, alpha=ALPHA, eta=ETA, seed=1 + rank, optim_interval=0, device=local,
-                       sweep_groups=args.groups)
+        e2e = new_engine()
+        if world > 1:
+            torch.distributed.barrier()
         torch.cuda.synchronize()
         te0 = time.perf_counter()
-        e2e.upload(pin_off, pin_words)
+        upload(e2e, pin_off, pin_words)
         e2e.train(args.steps)
         ll = e2e.ll()
         z, nkw, nk, _ = e2e.state()
-        te = time.perf_counter() - te0
+        te = total(time.perf_counter() - te0, "max")
         h2d = pin_words.nbytes + pin_off.nbytes
         d2h = z.nbytes + nkw.nbytes + nk.nbytes + 16
-        e2e_obj = {"value": N * world * args.steps / te, "unit": "tokens/s", "h2d_bytes_per_step": h2d / args.steps,
-                   "d2h_bytes_per_step": d2h / args.steps,
+        e2e_obj = {"value": N_all_ranks * args.steps / te, "unit": "tokens/s",
+                   "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                    "includes": "corpus upload (pinned), z0 init + counts, the sweeps, ll, z/n_kw/n_k download"}
         e2e.close()
 
@@ -510,14 +560,18 @@ def main():
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "tokens/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": step_ms, "wall_ms_per_step": wall_ms,
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
-            "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1),
-                       "tokens": int(N), "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups), "parallelism": f"dp{world} (independent chains)",
+            "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1) * world,
+                       "tokens": N_all_ranks, "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups),
+                       "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
+                                       if world > 1 else "dp1"),
                        "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": MEASURED_TRAFFIC.get((args.config, int(len(off) - 1), int(info.sweep_groups))),
+                         "traffic": (MEASURED_TRAFFIC.get((args.config, int(len(off) - 1), int(info.sweep_groups)))
+                                     if world == 1 else None),
                          "kernel": "k_sweep_doc", "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg,
                          "per": "one sweep = all k_sweep_doc + k_phi_copy launches of the document groups",
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
@@ -526,9 +580,9 @@ def main():
             "e2e": e2e_obj,
             "gpu_launches": int(launches),
             "clocks": clk,
-            "ll_per_word": (ll[0] + ll[1]) / N if N else 0.0,
+            "ll_per_word": (ll[0] + ll[1]) / N_all_ranks if N_all_ranks else 0.0,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline_sample(w, off, words, V)
         print(json.dumps(line), flush=True)
     eng.close()

@@ -81,6 +81,8 @@ typedef struct tmt_info {
     double sweep_kernel_ms;  /* device time of the sweep kernels of the last tmt_train call */
     uint32_t sweeps_timed;   /* sweeps in that sum */
     uint32_t sweep_groups;   /* document groups per sweep in use */
+    double train_ms;         /* device time of the last tmt_train call, first sweep to last (CUDA events) */
+    uint32_t rank, world;    /* this handle's shard of a corpus split across ranks (0, 1: unsharded) */
 } tmt_info;
 
 /* Replaces ILDAModel::create (LDAModel.cpp:10-13) + the LDAModel ctor checks
@@ -95,6 +97,48 @@ tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out);
  * wid[doc_off[D]], doc_off[D+1]; z0 is doc-major or NULL. */
 tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off,
                              uint64_t D, const uint16_t* z0);
+
+/* Documents sharded across GPUs: tomotopy's COPY_MERGE scheme
+ * (LDAModel.hpp:555-570) with the workers on different devices.  Rank r holds
+ * the contiguous global documents [doc_begin, doc_begin + D) and a replica of
+ * n_kw / n_k.  The document groups are cut over the GLOBAL longest-first order,
+ * so every group's snapshot is the same on every rank; after each group the
+ * ranks' integer count deltas (n_kw then n_k, K*V + K int32) are summed by
+ * `allreduce`, and the next group starts from the summed state.  Draws use the
+ * global token index, so z and every count equal those of one GPU holding the
+ * whole corpus, bit for bit (with the alpha optimisation the digamma sums are
+ * reduced in another order: equal up to FP64 rounding).
+ *
+ * allreduce(user, buf, count, dtype, stream): an in-place SUM over all ranks of
+ * `count` elements (dtype TMT_I32 or TMT_F64) of DEVICE memory, ordered on the
+ * CUDA stream `stream` (a cudaStream_t); returns 0 on success.  Every rank makes
+ * the same calls in the same order. */
+enum { TMT_I32 = 0, TMT_F64 = 1 };
+typedef int32_t (*tmt_allreduce_fn)(void* user, void* buf, uint64_t count, int32_t dtype, void* stream);
+typedef struct tmt_shard {
+    uint32_t rank, world;
+    uint64_t D_global;                /* documents over all ranks */
+    uint64_t doc_begin;               /* global index of this rank's first document */
+    const uint64_t* doc_len_global;   /* D_global document lengths (all words), rank order */
+    tmt_allreduce_fn allreduce;
+    void* user;
+} tmt_shard;
+
+/* The plan behind tmt_upload_shard (host only): the global longest-first order
+ * cut into `groups` equal-token ranges, as tmt_upload_corpus cuts one corpus.
+ * local_order[D_local] = this rank's documents (local indices) in global order;
+ * local_bounds[groups + 1]: group g is local_order[local_bounds[g] ..
+ * local_bounds[g+1]); global_bounds[groups + 1] (nullable): the groups'
+ * document counts over all ranks, as prefix bounds; *token_offset (nullable) =
+ * the global index of this rank's first token. */
+tmt_status tmt_plan_shard(const uint64_t* doc_len_global, uint64_t D_global, uint32_t groups, uint64_t doc_begin,
+                          uint64_t D_local, uint32_t* local_order, uint64_t* local_bounds, uint64_t* global_bounds,
+                          uint64_t* token_offset);
+
+/* tmt_upload_corpus for one rank of a sharded corpus (see tmt_shard); the
+ * counts after z0 are summed over the ranks. */
+tmt_status tmt_upload_shard(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                            const uint16_t* z0, const tmt_shard* shard);
 
 /* Replaces TopicModel::train (TopicModel.hpp:684-755) -> LDAModel::trainOne
  * (LDAModel.hpp:505-539): `iters` sweeps, each = sampling (performSampling /
@@ -219,6 +263,18 @@ tmt_status tmt_prepare_corpus(uint64_t D, const uint64_t* doc_off, const uint32_
                               uint32_t n_vocab, uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
                               uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
                               uint64_t* vocab_cf, uint64_t* vocab_df, uint32_t* real_v);
+
+/* tmt_prepare_corpus in two halves, for a corpus split across processes:
+ * the (cf, df) of one shard's words (by old id), and the preparation of one
+ * shard from the counts summed over all shards, so that every shard gets the
+ * same vocabulary order. */
+tmt_status tmt_corpus_counts(uint64_t D, const uint64_t* doc_off, const uint32_t* words, uint32_t n_vocab,
+                             uint64_t* vocab_cf, uint64_t* vocab_df);
+tmt_status tmt_prepare_corpus_counted(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                                      uint32_t n_vocab, const uint64_t* cf, const uint64_t* df,
+                                      uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
+                                      uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
+                                      uint32_t* real_v);
 
 /* No counterpart in tomotopy.  The FP64 log-likelihood of tmt_ll computed
  * from caller-owned DEVICE arrays -- n_dk (D x K), doc_len (D valid-token

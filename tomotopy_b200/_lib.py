@@ -30,12 +30,22 @@ class TmtInfo(C.Structure):
     _fields_ = [("D", C.c_uint64), ("N_all", C.c_uint64), ("N", C.c_uint64), ("global_step", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("K", C.c_uint32), ("V", C.c_uint32), ("sampler", C.c_int32),
                 ("last_sweep_ms", C.c_float), ("kernel_launches", C.c_uint64),
-                ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32), ("sweep_groups", C.c_uint32)]
+                ("sweep_kernel_ms", C.c_double), ("sweeps_timed", C.c_uint32), ("sweep_groups", C.c_uint32),
+                ("train_ms", C.c_double), ("rank", C.c_uint32), ("world", C.c_uint32)]
 
 
 class TmtServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_slots", C.c_uint32), ("token_budget", C.c_uint64),
                 ("step_token_sweeps", C.c_uint32), ("max_doc_len", C.c_uint32)]
+
+
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p)
+TMT_I32, TMT_F64 = 0, 1
+
+
+class TmtShard(C.Structure):
+    _fields_ = [("rank", C.c_uint32), ("world", C.c_uint32), ("D_global", C.c_uint64), ("doc_begin", C.c_uint64),
+                ("doc_len_global", C.c_void_p), ("allreduce", ALLREDUCE_FN), ("user", C.c_void_p)]
 
 
 class TmtServerStats(C.Structure):
@@ -74,6 +84,11 @@ SIGNATURES = {
     "tmt_ll": (C.c_int, [_H, _P, _P]),
     "tmt_set_counts": (C.c_int, [_H, _P, _P]),
     "tmt_set_alpha": (C.c_int, [_H, _P]),
+    "tmt_corpus_counts": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P]),
+    "tmt_prepare_corpus_counted": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint64, C.c_uint64,
+                                             C.c_uint64, _P, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_plan_shard": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _P, _P, _P, _P]),
+    "tmt_upload_shard": (C.c_int, [_H, _P, _P, C.c_uint64, _P, C.POINTER(TmtShard)]),
     "tmt_set_global_step": (C.c_int, [_H, C.c_uint64]),
     "tmt_set_seed": (C.c_int, [_H, C.c_uint64]),
     "tmt_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),

@@ -46,12 +46,14 @@ constexpr int kSweepWarps = 8;           // warps per sweep block
 // initialisation: z0 ~ Discrete(alpha) (initializeDocState, LDAModel.hpp:781-813)
 // ---------------------------------------------------------------------------
 __global__ void k_init_z(const uint32_t* __restrict__ words, uint64_t n_all, uint32_t V, uint32_t K,
-                         const float* __restrict__ acum, uint64_t seed, uint16_t* __restrict__ z)
+                         const float* __restrict__ acum, uint64_t seed, uint64_t tok_offset,
+                         uint16_t* __restrict__ z)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_all;
          i += (uint64_t)gridDim.x * blockDim.x) {
         if (words[i] >= V) { z[i] = 0xFFFF; continue; }
-        float u = tmt::u01(tmt::philox_u32((uint32_t)i, (uint32_t)(i >> 32), tmt::kStreamInit, 0, seed));
+        const uint64_t gi = i + tok_offset;      // the token's index in the whole (unsharded) corpus
+        float u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamInit, 0, seed));
         float r = __fmul_rn(u, acum[K - 1]);
         uint32_t lo = 0, hi = K - 1;
         while (lo < hi) {
@@ -124,6 +126,50 @@ __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __res
     }
 }
 
+// Sharded corpus: fold the ranks' summed deltas of one group into the state.
+// n_k first (one block), then n_kw and, when phi != NULL, the word table of
+// the new state; the deltas are zeroed for the next group.
+__global__ void k_nk_apply(int32_t* __restrict__ nk, int32_t* __restrict__ dnk, uint32_t K)
+{
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+        nk[k] += dnk[k];
+        dnk[k] = 0;
+    }
+}
+
+__global__ void k_phi_apply(int32_t* __restrict__ nkw, int32_t* __restrict__ delta, const int32_t* __restrict__ nk,
+                            uint32_t V, uint32_t K, uint32_t KP, float eta, float veta, float* __restrict__ phi,
+                            uint32_t smem_k, int fold)
+{
+    extern __shared__ float s_R[];
+    const bool r_smem = phi && K <= smem_k;
+    if (r_smem)
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+    __syncthreads();
+    for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
+        int32_t* col = nkw + v * K;
+        int32_t* dcol = delta + v * K;
+        float* ph = phi ? phi + v * KP : nullptr;
+        for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
+            float val = 0.f;
+            if (k < K) {
+                int32_t n = col[k];
+                if (fold) {
+                    n += dcol[k];
+                    col[k] = n;
+                    dcol[k] = 0;
+                }
+                if (ph) {
+                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+                    val = __fmul_rn(__fadd_rn((float)n, eta), R);
+                }
+            }
+            if (ph) ph[k] = val;
+        }
+    }
+}
+
 struct SweepArgs {
     const uint64_t* doc_off;
     const uint32_t* words;
@@ -143,6 +189,7 @@ struct SweepArgs {
     uint64_t seed;
     uint32_t iter;
     uint64_t pos_begin, pos_end;  // this launch samples doc_order positions [pos_begin, pos_end)
+    uint64_t tok_offset;     // global index of token 0 (a shard of a corpus split across GPUs)
     uint32_t rowi_smem;      // 1: the int n_dk row lives in shared memory
     uint32_t dnk_smem;       // 1: n_k deltas aggregate in shared memory
 };
@@ -220,7 +267,8 @@ k_sweep_doc(SweepArgs a)
             if (my_i < e) {
                 my_w = a.words[my_i];
                 my_z = a.z[my_i];
-                my_u = tmt::u01(tmt::philox_u32((uint32_t)my_i, (uint32_t)(my_i >> 32), tmt::kStreamSweep,
+                const uint64_t gi = my_i + a.tok_offset;
+                my_u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamSweep,
                                                 a.iter, a.seed));
             }
             uint32_t my_new = my_z;
@@ -520,6 +568,22 @@ __global__ void k_alpha_update(const double* __restrict__ part_nom, const double
     }
 }
 
+// sums of the partial rows in the order k_alpha_update uses: out[k] (k < K) and out[K]
+__global__ void k_alpha_fold(const double* __restrict__ part_nom, const double* __restrict__ part_den,
+                             uint32_t nparts, uint32_t K, double* __restrict__ out)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) {
+        double nom = 0;
+        for (uint32_t i = 0; i < nparts; ++i) nom += part_nom[(uint64_t)i * K + k];
+        out[k] = nom;
+    } else if (k == K) {
+        double den = 0;
+        for (uint32_t i = 0; i < nparts; ++i) den += part_den[i];
+        out[K] = den;
+    }
+}
+
 __global__ void k_sum_alpha(const float* __restrict__ alpha, uint32_t K, float* __restrict__ out)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -541,6 +605,8 @@ struct tmt_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // around the sweep kernel only
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;   // around a whole tmt_train call
+    double train_ms = 0;
     double sweep_kernel_ms = 0;                   // summed over the last train() call
     uint32_t sweeps_timed = 0;
     int num_sms = 0;
@@ -562,6 +628,13 @@ struct tmt_handle {
     float* d_phi = nullptr;          // per-word topic weights of the current snapshot
     uint32_t groups = 1;             // document groups per sweep
     std::vector<uint64_t> group_bounds;   // doc_order positions: group g = [b[g], b[g+1])
+    // a corpus sharded across GPUs (tmt_upload_shard); world == 1: this GPU holds all of it
+    uint32_t rank = 0, world = 1;
+    uint64_t D_global = 0, tok_offset = 0;
+    std::vector<uint64_t> gbounds;   // the groups over all ranks (document-count prefix bounds)
+    tmt_allreduce_fn allreduce = nullptr;
+    void* ar_user = nullptr;
+    int32_t* d_delta = nullptr;      // sharded: one group's count deltas, n_kw (K*V) then n_k (K)
     // sweep-kernel autotuner: variants give bit-identical results, so the
     // first sweeps each time one variant and the fastest is kept
     int variant = 0;
@@ -596,6 +669,7 @@ struct tmt_handle {
     } inf;
     double* d_part_nom = nullptr;
     double* d_part_den = nullptr;
+    double* d_alpha_fold = nullptr;  // sharded: K + 1 sums exchanged across ranks
     uint32_t n_apart = 0;
 
     template <class T>
@@ -632,6 +706,8 @@ struct tmt_handle {
         if (ev1) cudaEventDestroy(ev1);
         if (kev0) cudaEventDestroy(kev0);
         if (kev1) cudaEventDestroy(kev1);
+        if (tev0) cudaEventDestroy(tev0);
+        if (tev1) cudaEventDestroy(tev1);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -738,11 +814,97 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a)
     else launch_sweep_t<0, 3, false>(h, b, sh);
 }
 
+// In-place SUM over the ranks of a sharded corpus, ordered on the engine's stream.
+void exchange(tmt_handle* h, void* buf, uint64_t count, int32_t dtype)
+{
+    if (h->world <= 1) return;
+    const int32_t rc = h->allreduce(h->ar_user, buf, count, dtype, (void*)h->stream);
+    if (rc != 0) throw CudaError("allreduce across ranks failed (" + std::to_string(rc) + ")");
+}
+
+SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32_t* nkw_next, int32_t* nk_next,
+                     uint64_t pos_begin, uint64_t pos_end)
+{
+    SweepArgs a{};
+    a.doc_off = h->d_doc_off;
+    a.words = h->d_words;
+    a.z = h->d_z;
+    a.ndk = h->d_ndk;
+    a.nkw = nkw;
+    a.nk = nk;
+    a.phi = h->d_phi;
+    a.nkw_next = nkw_next;
+    a.nk_next = nk_next;
+    a.alpha = h->d_alpha;
+    a.doc_order = h->d_doc_order;
+    a.doc_counter = h->d_counter;
+    a.D = h->D;
+    a.K = h->cfg.K;
+    a.V = h->cfg.V;
+    a.c = (h->cfg.K + 31) / 32;
+    a.eta = h->cfg.eta;
+    a.veta = h->cfg.eta * (float)h->cfg.V;
+    a.seed = h->cfg.seed;
+    a.iter = (uint32_t)h->global_step;
+    a.pos_begin = pos_begin;
+    a.pos_end = pos_end;
+    a.tok_offset = h->tok_offset;
+    return a;
+}
+
+// A sweep of one rank of a sharded corpus: per group, the word table of the
+// current (summed) state, this rank's documents of the group with their count
+// deltas into d_delta, the SUM of the deltas over the ranks, and the fold of
+// the summed deltas into the state (fused with the next group's table).  Every
+// rank runs every group that holds documents on any rank, so the collectives
+// match; n_kw is updated in place (h->cur stays 0).
+void do_sweep_sharded(tmt_handle* h)
+{
+    const uint32_t K = h->cfg.K, V = h->cfg.V;
+    const float veta = h->cfg.eta * (float)V;
+    const uint64_t KV = (uint64_t)K * V;
+    int32_t* dnkw = h->d_delta;
+    int32_t* dnk = h->d_delta + KV;
+    const uint32_t smem_k = K <= 12288 ? K : 0;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
+    bool pending = false, recorded = false;
+    const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
+    for (uint32_t g = 0; g < G; ++g) {
+        if (h->gbounds[g] == h->gbounds[g + 1]) continue;      // empty on every rank
+        if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
+        if (pending) {
+            k_nk_apply<<<1, 1024, 0, h->stream>>>(h->d_nk[0], dnk, K);
+            launch_check(h);
+        }
+        k_phi_apply<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta,
+                                                        veta, h->d_phi, smem_k, pending ? 1 : 0);
+        launch_check(h);
+        if (h->group_bounds[g] < h->group_bounds[g + 1]) {
+            CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+            launch_sweep(h, sweep_args(h, h->d_nkw[0], h->d_nk[0], dnkw, dnk, h->group_bounds[g],
+                                       h->group_bounds[g + 1]));
+        }
+        exchange(h, h->d_delta, KV + K, TMT_I32);
+        pending = true;
+    }
+    if (pending) {
+        k_nk_apply<<<1, 1024, 0, h->stream>>>(h->d_nk[0], dnk, K);
+        launch_check(h);
+        k_phi_apply<<<grid, 256, 0, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta, veta,
+                                                nullptr, 0, 1);
+        launch_check(h);
+    }
+    CK(cudaEventRecord(h->kev1, h->stream));
+    if (!recorded) CK(cudaEventRecord(h->kev0, h->stream));
+    h->sampler_used = TMT_SAMPLER_DENSE;
+}
+
 // One sweep = one launch per document group (contiguous ranges of the
 // longest-first order holding equal shares of the tokens); before each, the
 // word table and the next-state copy are rebuilt from the current state.
 void do_sweep(tmt_handle* h)
 {
+    if (h->world > 1) return do_sweep_sharded(h);
     const uint32_t K = h->cfg.K, V = h->cfg.V;
     const float veta = h->cfg.eta * (float)V;
     bool recorded = false;
@@ -756,29 +918,8 @@ void do_sweep(tmt_handle* h)
                                                         veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k);
         launch_check(h);
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
-        SweepArgs a{};
-        a.doc_off = h->d_doc_off;
-        a.words = h->d_words;
-        a.z = h->d_z;
-        a.ndk = h->d_ndk;
-        a.nkw = h->d_nkw[cur];
-        a.nk = h->d_nk[cur];
-        a.phi = h->d_phi;
-        a.nkw_next = h->d_nkw[nxt];
-        a.nk_next = h->d_nk[nxt];
-        a.alpha = h->d_alpha;
-        a.doc_order = h->d_doc_order;
-        a.doc_counter = h->d_counter;
-        a.D = h->D;
-        a.K = K;
-        a.V = V;
-        a.c = (K + 31) / 32;
-        a.eta = h->cfg.eta;
-        a.veta = veta;
-        a.seed = h->cfg.seed;
-        a.iter = (uint32_t)h->global_step;
-        a.pos_begin = h->group_bounds[g];
-        a.pos_end = h->group_bounds[g + 1];
+        const SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
+                                       h->group_bounds[g], h->group_bounds[g + 1]);
         if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
         launch_sweep(h, a);
         h->cur = nxt;
@@ -798,8 +939,21 @@ void do_optimize(tmt_handle* h)
         k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_alpha, h->d_doc_len, h->d_asum,
                                                   h->d_part_nom, h->d_part_den);
         launch_check(h);
-        k_alpha_update<<<1, 1024, 0, h->stream>>>(h->d_part_nom, h->d_part_den, h->n_apart, K, h->D,
-                                                  h->d_alpha, h->d_asum, h->d_dg_points);
+        uint32_t nparts = h->n_apart;
+        const double* nom = h->d_part_nom;
+        const double* den = h->d_part_den;
+        if (h->world > 1) {
+            // this rank's sums into one row (K digamma sums, then the length sum), summed over the ranks
+            k_alpha_fold<<<(K + 256) / 256, 256, 0, h->stream>>>(h->d_part_nom, h->d_part_den, h->n_apart, K,
+                                                                 h->d_alpha_fold);
+            launch_check(h);
+            exchange(h, h->d_alpha_fold, (uint64_t)K + 1, TMT_F64);
+            nparts = 1;
+            nom = h->d_alpha_fold;
+            den = h->d_alpha_fold + K;
+        }
+        k_alpha_update<<<1, 1024, 0, h->stream>>>(nom, den, nparts, K, h->D_global, h->d_alpha, h->d_asum,
+                                                  h->d_dg_points);
         launch_check(h);
     }
 }
@@ -820,6 +974,54 @@ void do_ll(tmt_handle* h, double* d_out)
     launch_check(h);
     k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out);
     launch_check(h);
+    exchange(h, d_out, 1, TMT_F64);     // LLDocs over every rank's documents; LLRest is replicated
+}
+
+// The document order and groups of a (possibly sharded) corpus: documents
+// longest first (stable), cut into G ranges holding equal shares of the
+// tokens -- position p is in group g when prefix(p) * G lies in
+// [g * total, (g+1) * total).  The rank's documents keep that order.
+struct ShardPlan {
+    std::vector<uint32_t> order;        // local document indices, global order
+    std::vector<uint64_t> bounds;       // group g = order[bounds[g] .. bounds[g+1])
+    std::vector<uint64_t> gbounds;      // group g holds global positions [gbounds[g], gbounds[g+1])
+    uint64_t tok_offset = 0;
+};
+
+ShardPlan plan_shard(const uint64_t* len, uint64_t D_global, uint32_t groups, uint64_t doc_begin, uint64_t D_local)
+{
+    if (doc_begin > D_global || D_local > D_global - doc_begin) throw ArgError("shard outside the corpus");
+    ShardPlan p;
+    std::vector<uint64_t> gorder(D_global);
+    std::iota(gorder.begin(), gorder.end(), (uint64_t)0);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](uint64_t a, uint64_t b) { return len[a] > len[b]; });
+    uint64_t total = 0;
+    for (uint64_t d = 0; d < D_global; ++d) {
+        total += len[d];
+        if (d < doc_begin) p.tok_offset += len[d];
+    }
+    const uint64_t G = std::max<uint32_t>(1, groups);
+    p.gbounds.assign(G + 1, 0);
+    p.gbounds[G] = D_global;
+    p.bounds.assign(G + 1, 0);
+    p.order.reserve(D_local);
+    uint64_t prefix = 0, g = 1;
+    for (uint64_t q = 0; q < D_global; ++q) {
+        while (g < G && prefix * G >= g * total) {
+            p.gbounds[g] = q;
+            p.bounds[g] = p.order.size();
+            ++g;
+        }
+        const uint64_t d = gorder[q];
+        if (d >= doc_begin && d - doc_begin < D_local) p.order.push_back((uint32_t)(d - doc_begin));
+        prefix += len[d];
+    }
+    for (; g < G; ++g) {
+        p.gbounds[g] = D_global;
+        p.bounds[g] = p.order.size();
+    }
+    p.bounds[G] = p.order.size();
+    return p;
 }
 
 void validate_config(const tmt_config& c)
@@ -840,50 +1042,10 @@ void validate_config(const tmt_config& c)
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-extern "C" {
+namespace {
 
-tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out)
-{
-    if (!cfg || !out) return TMT_ERR_INVALID_ARGUMENT;
-    *out = nullptr;
-    tmt_handle* h = nullptr;
-    try {
-        h = new tmt_handle();
-    } catch (...) {
-        return TMT_ERR_OUT_OF_MEMORY;
-    }
-    h->cfg = *cfg;
-    h->cfg.alpha = nullptr;
-    h->device = cfg->device;
-    try {
-        validate_config(*cfg);   // the ctor's argument checks, before any CUDA call
-    } catch (const std::exception& e) {
-        h->err = e.what();
-        *out = h;
-        return TMT_ERR_INVALID_ARGUMENT;
-    }
-    tmt_status s = guarded(h, [&] {
-        h->groups = cfg->sweep_groups ? cfg->sweep_groups : 8;
-        h->alpha.assign(cfg->K, cfg->alpha_scalar);
-        if (cfg->alpha) std::copy(cfg->alpha, cfg->alpha + cfg->K, h->alpha.begin());
-        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-        CK(cudaEventCreate(&h->ev0));
-        CK(cudaEventCreate(&h->ev1));
-        CK(cudaEventCreate(&h->kev0));
-        CK(cudaEventCreate(&h->kev1));
-        CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
-    });
-    if (s != TMT_OK) {
-        // keep the handle so the caller can read the message
-        *out = h;
-        return s;
-    }
-    *out = h;
-    return TMT_OK;
-}
-
-tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
-                             const uint16_t* z0)
+tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D, const uint16_t* z0,
+                       const tmt_shard* shard)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
@@ -914,34 +1076,55 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
             N += c;
         }
         h->N = N;
-        std::vector<uint32_t> order(D);
-        std::iota(order.begin(), order.end(), 0u);
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-            return doc_off[a + 1] - doc_off[a] > doc_off[b + 1] - doc_off[b];
-        });
-
-        // groups: contiguous ranges of the order with equal shares of the tokens;
-        // position p is in group g when prefix(p) * G lies in [g * total, (g+1) * total)
-        {
-            const uint64_t G = std::max<uint64_t>(1, h->groups);
-            h->group_bounds.assign(G + 1, 0);
-            h->group_bounds[G] = D;
-            uint64_t prefix = 0;
-            uint64_t g = 1;
-            for (uint64_t p = 0; p < D; ++p) {
-                while (g < G && prefix * G >= g * n_all) h->group_bounds[g++] = p;
-                prefix += doc_off[order[p] + 1] - doc_off[order[p]];
-            }
-            while (g < G) h->group_bounds[g++] = D;
+        ShardPlan plan;
+        if (shard) {
+            if (shard->world == 0 || shard->rank >= shard->world) throw ArgError("bad rank / world");
+            if (shard->world > 1 && !shard->allreduce) throw ArgError("a sharded corpus needs an allreduce");
+            if (!shard->doc_len_global && shard->D_global) throw ArgError("doc_len_global is NULL");
+            if (shard->doc_begin > shard->D_global || D > shard->D_global - shard->doc_begin)
+                throw ArgError("shard outside the corpus");
+            for (uint64_t d = 0; d < D; ++d)
+                if (shard->doc_len_global[shard->doc_begin + d] != doc_off[d + 1] - doc_off[d])
+                    throw ArgError("doc_len_global disagrees with doc_off at document " + std::to_string(d));
+            plan = plan_shard(shard->doc_len_global, shard->D_global, h->groups, shard->doc_begin, D);
+            h->rank = shard->rank;
+            h->world = shard->world;
+            h->D_global = shard->D_global;
+            h->allreduce = shard->allreduce;
+            h->ar_user = shard->user;
+        } else {
+            std::vector<uint64_t> lens(D);
+            for (uint64_t d = 0; d < D; ++d) lens[d] = doc_off[d + 1] - doc_off[d];
+            plan = plan_shard(lens.data(), D, h->groups, 0, D);
+            h->rank = 0;
+            h->world = 1;
+            h->D_global = D;
+            h->allreduce = nullptr;
+            h->ar_user = nullptr;
         }
+        h->tok_offset = plan.tok_offset;
+        h->group_bounds = plan.bounds;
+        h->gbounds = plan.gbounds;
+        const std::vector<uint32_t>& order = plan.order;
+
         h->d_doc_off = h->dalloc<uint64_t>(D + 1);
         h->d_words = h->dalloc<uint32_t>(n_all);
         h->d_z = h->dalloc<uint16_t>(n_all);
         h->d_ndk = h->dalloc<int32_t>(D * (uint64_t)K);
         h->d_nkw[0] = h->dalloc<int32_t>((uint64_t)K * V);
-        h->d_nkw[1] = h->dalloc<int32_t>((uint64_t)K * V);
         h->d_nk[0] = h->dalloc<int32_t>(K);
-        h->d_nk[1] = h->dalloc<int32_t>(K);
+        if (h->world > 1) {
+            // the next-state buffers become one exchanged delta buffer
+            h->d_delta = h->dalloc<int32_t>((uint64_t)K * V + K);
+            h->d_nkw[1] = h->d_delta;
+            h->d_nk[1] = h->d_delta + (uint64_t)K * V;
+            h->d_alpha_fold = h->dalloc<double>((uint64_t)K + 1);
+        } else {
+            h->d_delta = nullptr;
+            h->d_alpha_fold = nullptr;
+            h->d_nkw[1] = h->dalloc<int32_t>((uint64_t)K * V);
+            h->d_nk[1] = h->dalloc<int32_t>(K);
+        }
         h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
         {
             h->n_variants = round4(K) <= 4096 ? 2 : 1;
@@ -985,7 +1168,7 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
             float* d_acum = h->dalloc<float>(K);
             CK(cudaMemcpyAsync(d_acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (n_all + 255) / 256);
-            k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->d_z);
+            k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->tok_offset, h->d_z);
             launch_check(h);
         }
         if (D) {
@@ -994,9 +1177,94 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
                                            h->d_nk[0], h->d_doc_len);
             launch_check(h);
         }
+        if (h->world > 1) {
+            if (h->d_delta) CK(cudaMemsetAsync(h->d_delta, 0, ((uint64_t)K * V + K) * sizeof(int32_t), st));
+            // every rank counted its own documents: the model's counts are the sums
+            exchange(h, h->d_nkw[0], (uint64_t)K * V, TMT_I32);
+            exchange(h, h->d_nk[0], K, TMT_I32);
+        }
         CK(cudaStreamSynchronize(st));
         h->uploaded = true;
     });
+}
+
+} // namespace
+
+extern "C" {
+
+tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out)
+{
+    if (!cfg || !out) return TMT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    tmt_handle* h = nullptr;
+    try {
+        h = new tmt_handle();
+    } catch (...) {
+        return TMT_ERR_OUT_OF_MEMORY;
+    }
+    h->cfg = *cfg;
+    h->cfg.alpha = nullptr;
+    h->device = cfg->device;
+    try {
+        validate_config(*cfg);   // the ctor's argument checks, before any CUDA call
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        *out = h;
+        return TMT_ERR_INVALID_ARGUMENT;
+    }
+    tmt_status s = guarded(h, [&] {
+        h->groups = cfg->sweep_groups ? cfg->sweep_groups : 8;
+        h->alpha.assign(cfg->K, cfg->alpha_scalar);
+        if (cfg->alpha) std::copy(cfg->alpha, cfg->alpha + cfg->K, h->alpha.begin());
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&h->ev0));
+        CK(cudaEventCreate(&h->ev1));
+        CK(cudaEventCreate(&h->kev0));
+        CK(cudaEventCreate(&h->kev1));
+        CK(cudaEventCreate(&h->tev0));
+        CK(cudaEventCreate(&h->tev1));
+        CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    });
+    if (s != TMT_OK) {
+        // keep the handle so the caller can read the message
+        *out = h;
+        return s;
+    }
+    *out = h;
+    return TMT_OK;
+}
+
+
+tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                             const uint16_t* z0)
+{
+    return upload_impl(h, wid, doc_off, D, z0, nullptr);
+}
+
+tmt_status tmt_upload_shard(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                            const uint16_t* z0, const tmt_shard* shard)
+{
+    if (!shard) return TMT_ERR_INVALID_ARGUMENT;
+    return upload_impl(h, wid, doc_off, D, z0, shard);
+}
+
+tmt_status tmt_plan_shard(const uint64_t* doc_len_global, uint64_t D_global, uint32_t groups, uint64_t doc_begin,
+                          uint64_t D_local, uint32_t* local_order, uint64_t* local_bounds, uint64_t* global_bounds,
+                          uint64_t* token_offset)
+{
+    if ((D_global && !doc_len_global) || (D_local && !local_order) || !local_bounds) return TMT_ERR_INVALID_ARGUMENT;
+    try {
+        const ShardPlan p = plan_shard(doc_len_global, D_global, groups, doc_begin, D_local);
+        std::copy(p.order.begin(), p.order.end(), local_order);
+        std::copy(p.bounds.begin(), p.bounds.end(), local_bounds);
+        if (global_bounds) std::copy(p.gbounds.begin(), p.gbounds.end(), global_bounds);
+        if (token_offset) *token_offset = p.tok_offset;
+        return TMT_OK;
+    } catch (const ArgError&) {
+        return TMT_ERR_INVALID_ARGUMENT;
+    } catch (const std::bad_alloc&) {
+        return TMT_ERR_OUT_OF_MEMORY;
+    }
 }
 
 tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* ll_out)
@@ -1016,6 +1284,7 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
         uint32_t pt = 0;
         h->sweep_kernel_ms = 0;
         h->sweeps_timed = 0;
+        CK(cudaEventRecord(h->tev0, h->stream));
         for (uint32_t i = 0; i < iters; ++i) {
             CK(cudaEventRecord(h->ev0, h->stream));
             do_sweep(h);
@@ -1045,8 +1314,14 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
             ++h->global_step;
             if (npts && (i + 1) % ll_every == 0 && pt < npts) do_ll(h, h->d_ll + 2 * pt++);
         }
+        CK(cudaEventRecord(h->tev1, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+        {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->tev0, h->tev1));
+            h->train_ms = ms;
+        }
         if (npts) {
             std::vector<double> tmp(2 * (size_t)npts);
             CK(cudaMemcpy(tmp.data(), h->d_ll, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1163,6 +1438,9 @@ tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
     out->sweep_kernel_ms = h->sweep_kernel_ms;
     out->sweeps_timed = h->sweeps_timed;
     out->sweep_groups = h->groups;
+    out->train_ms = h->train_ms;
+    out->rank = h->rank;
+    out->world = h->world;
     return TMT_OK;
 }
 
