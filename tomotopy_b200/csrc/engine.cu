@@ -407,8 +407,8 @@ k_sweep_doc(SweepArgs a)
 // log-likelihood in FP64 (getLLDocs / getLLRest, LDAModel.hpp:616-668)
 // ---------------------------------------------------------------------------
 
-// Rows 0..D-1 are n_dk rows, rows D..D+V-1 are n_kw columns.  Static
-// warp-to-row assignment and fixed reduction trees: bit-reproducible.
+// n_dk rows and n_kw columns, each dealt to the warps in a fixed order, and
+// fixed reduction trees: bit-reproducible.
 // lg_alpha[k] = lgamma(alpha_k); asum[0] = sum(alpha), asum[1] = lgamma(sum(alpha))
 __global__ void k_ll_prep(const float* __restrict__ alpha, uint32_t K, double* __restrict__ lg_alpha,
                           double* __restrict__ asum)
@@ -434,20 +434,21 @@ __global__ void k_ll_partials(const int32_t* __restrict__ ndk, uint64_t D, uint3
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     double accd = 0, accr = 0;
-    for (uint64_t r = gw; r < D + V; r += nw) {
-        if (r < D) {
-            const int32_t* p = ndk + r * K;
-            for (uint32_t k = lane; k < K; k += 32) {
-                int32_t n = p[k];
-                if (n) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
-            }
-            if (lane == 0) accd -= lgamma((double)doc_len[r] + asum) - lg_asum;
-        } else {
-            const int32_t* p = nkw + (r - D) * K;
-            for (uint32_t k = lane; k < K; k += 32) {
-                int32_t n = p[k];
-                if (n) accr += lgamma((double)n + eta) - lg_eta;
-            }
+    for (uint64_t r = gw; r < D; r += nw) {
+        const int32_t* p = ndk + r * K;
+        for (uint32_t k = lane; k < K; k += 32) {
+            int32_t n = p[k];
+            if (n) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
+        }
+        if (lane == 0) accd -= lgamma((double)doc_len[r] + asum) - lg_asum;
+    }
+    // the word rows' assignment does not depend on D: LLRest is the same bits on
+    // every rank of a sharded corpus and on one GPU holding all of it
+    for (uint64_t v = gw; v < V; v += nw) {
+        const int32_t* p = nkw + v * K;
+        for (uint32_t k = lane; k < K; k += 32) {
+            int32_t n = p[k];
+            if (n) accr += lgamma((double)n + eta) - lg_eta;
         }
     }
     accd = warp_sum(accd);
