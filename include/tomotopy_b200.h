@@ -44,9 +44,11 @@ typedef struct tmt_handle tmt_handle;
 
 /* Sampler kernels for the training sweep. */
 typedef enum tmt_sampler {
-    TMT_SAMPLER_AUTO = 0,   /* dense for K <= 256, sparse above */
+    TMT_SAMPLER_AUTO = 0,   /* the engine's choice: the dense sampler */
     TMT_SAMPLER_DENSE = 1,  /* full K-vector conditional per token */
-    TMT_SAMPLER_SPARSE = 2  /* exact doc/word bucket decomposition */
+    TMT_SAMPLER_SPARSE = 2  /* accepted; runs the dense sampler (documents of the benchmark corpora
+                               keep ~160 nonzero topics at K = 1000, where the bucket decomposition
+                               would gather more per token than the dense pass loads) */
 } tmt_sampler;
 
 /* Model hyper-parameters.  Mirrors LDAArgs (LDA.h:170-176) plus the
@@ -91,12 +93,27 @@ tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out);
 
 /* Replaces LDAModel::prepare's device-relevant part (LDAModel.hpp:1073-1138):
  * uploads the doc-major corpus (words already vocab-reordered and sorted by
- * id inside each document, as prepareDoc does, LDAModel.hpp:716-722), builds
- * the word-major layout, draws z0 ~ Discrete(alpha) (initializeDocState,
- * LDAModel.hpp:781-813) unless z0 is given, and builds n_dk, n_kw and n_k.
+ * id inside each document, as prepareDoc does, LDAModel.hpp:716-722), draws
+ * z0 ~ Discrete(alpha) (initializeDocState, LDAModel.hpp:781-813) unless z0
+ * is given, and builds n_dk, n_kw and n_k.
  * wid[doc_off[D]], doc_off[D+1]; z0 is doc-major or NULL. */
 tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off,
                              uint64_t D, const uint16_t* z0);
+
+/* tmt_upload_corpus with weighted counts: the LDAModel<TermWeight::idf|pmi>
+ * instantiations (LDAModel.hpp:287-299 addWordTo with doc.wordWeights, the
+ * weights set in initializeDocState, :795-809).  weights[i] is token i's
+ * weight (the caller computes tomotopy's IDF / PMI weights; entries of
+ * words >= V are ignored), finite, in [0, 65536], all together below 2^38.
+ * n_dk, n_kw and n_k are then float sums of weights; a removal clamps at 0
+ * (updateCnt<true>, Utils.hpp:132-155); each document's length is its weight
+ * sum (SumWordWeight, LDA.h:104-117), used by the log-likelihood and the
+ * alpha optimiser.  n_dk rows change in float in token order; n_kw / n_k are
+ * float states that change between document groups by integer deltas in
+ * units of 2^-24, so results do not depend on the order of atomic adds.
+ * Single GPU only (a sharded corpus is rejected). */
+tmt_status tmt_upload_corpus_weighted(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off,
+                                      uint64_t D, const uint16_t* z0, const float* weights);
 
 /* Documents sharded across GPUs: tomotopy's COPY_MERGE scheme
  * (LDAModel.hpp:555-570) with the workers on different devices.  Rank r holds
@@ -163,6 +180,9 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
  * (TopicModel::_loadModel, TopicModel.hpp:361-395).  Later sweeps and
  * inference use it. */
 tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k);
+/* tmt_set_counts for weighted counts (tmt_upload_corpus_weighted): n_kw (V x K
+ * floats, column v = K values) and n_k (K); values finite and >= 0. */
+tmt_status tmt_set_counts_f32(tmt_handle* h, const float* n_kw, const float* n_k);
 /* Replaces alpha (K values > 0), e.g. the optimised alphas of a loaded model. */
 tmt_status tmt_set_alpha(tmt_handle* h, const float* alpha);
 /* Sets the sweep counter (TopicModel::globalStep), e.g. after a load; it keys
@@ -174,6 +194,18 @@ tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed);
 /* Sets the alpha-optimisation schedule between train() calls
  * (LDAModel::optimInterval / burnIn, python setters py_LDA.cpp). */
 tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_in);
+/* Single GPU: after the autotuner's first sweeps, each sweep is one launch of
+ * a CUDA graph holding the sweep's kernels (default on).  0 launches every
+ * kernel from the host instead; results are identical either way.  Replaces
+ * nothing in tomotopy: the loop it captures is TopicModel::train's
+ * (TopicModel.hpp:684-755) iteration over trainOne. */
+tmt_status tmt_set_graphs(tmt_handle* h, int32_t enable);
+
+/* Weighted counts (tmt_upload_corpus_weighted): n_dk (D x K row-major),
+ * n_kw (V x K, column v = K floats: numByTopicWord of ModelStateLDA<float>),
+ * n_k (K) and the document weight sums (D); any pointer may be NULL.
+ * Integer-count corpora return TMT_ERR_STATE (use tmt_download_state). */
+tmt_status tmt_download_counts_f32(tmt_handle* h, float* n_dk, float* n_kw, float* n_k, float* doc_wlen);
 
 /* Downloads n_dk (D x K row-major int32; DocumentLDA::numByTopic). */
 tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
@@ -193,6 +225,15 @@ tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk);
  * changed. */
 tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
                            uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll);
+/* tmt_infer_batch for a model with weighted counts (tmt_upload_corpus_weighted):
+ * weights[i] is token i's weight, computed by the caller as tomotopy does for
+ * new documents (IDF: the word's vocabWeights entry; PMI: from the word's
+ * count in the document, LDAModel.hpp:795-809); every token of one word in a
+ * document must carry the same weight.  n_dk is a float sum of weights, theta
+ * divides by the document's weight sum (_getTopicsByDoc, LDAModel.hpp:1145-1159). */
+tmt_status tmt_infer_batch_weighted(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                                    const float* weights, uint32_t iters, uint64_t seed, const uint64_t* doc_keys,
+                                    float* theta, double* ll);
 
 /* ---- served inference: continuous batching over resident frozen models ----
  * No single tomotopy counterpart: it serves tomotopy's infer() (models.py:354,
@@ -318,6 +359,7 @@ typedef struct tmt_model_args {
     uint64_t min_cf, min_df, rm_top;
     int32_t device;
     uint32_t sweep_groups;   /* 0: engine default */
+    int32_t tw;              /* TermWeight (tomotopy/__init__.py:10-33): 0 ONE, 1 IDF, 2 PMI */
 } tmt_model_args;
 typedef struct tmt_model_info {
     uint32_t K, V, n_vocab;  /* V = realV (used vocabulary); n_vocab = all words seen */
@@ -326,6 +368,8 @@ typedef struct tmt_model_info {
     float alpha, eta;
     uint32_t optim_interval, burn_in;
     uint64_t seed, min_cf, min_df, rm_top;
+    int32_t tw;              /* TermWeight: 0 ONE, 1 IDF, 2 PMI */
+    double weighted_n;       /* TopicModel::weightedN, ll_per_word's denominator */
 } tmt_model_info;
 
 /* LDAModel ctor checks (LDAModel.hpp:962-983). */

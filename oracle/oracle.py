@@ -71,6 +71,17 @@ def _load():
         "orc_optimize_alpha": (None, [C.c_uint64, C.c_uint32, V, V, V]),
         "orc_infer_doc": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, C.c_uint32,
                                        C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
+        "orc_wq": (C.c_int64, [C.c_float]),
+        "orc_fold": (C.c_float, [C.c_float, C.c_int64]),
+        "orc_fold_w": (None, [C.c_uint32, C.c_uint32, V, V, V, V]),
+        "orc_counts_from_z_w": (None, [C.c_uint64, V, V, V, V, C.c_uint32, C.c_uint32, V, V, V, V]),
+        "orc_sweep_doc_live_w_subset": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32]
+                                        + [V] * 10 + [C.c_uint64]),
+        "orc_ll_docs_w_f64": (C.c_double, [C.c_uint64, C.c_uint32, V, V, V]),
+        "orc_ll_rest_w_f64": (C.c_double, [C.c_uint32, C.c_uint32, V, V, C.c_float]),
+        "orc_optimize_alpha_w": (None, [C.c_uint64, C.c_uint32, V, V, V]),
+        "orc_infer_doc_w": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, C.c_uint32,
+                                         C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -263,6 +274,111 @@ class State:
         return (a + b) / max(self.c.N, 1)
 
 
+def weights_idf(corpus):
+    """TermWeight.IDF token weights: vocabWeights[v] = (float)log(D / (double)df[v])
+    (LDAModel.hpp:1093-1113, df over documents' distinct in-vocabulary words),
+    token weight = vocabWeights[word] (:801-803); 0 for out-of-vocabulary tokens."""
+    c = corpus
+    df = np.zeros(c.V, dtype=np.int64)
+    for d in range(c.D):
+        ws = c.words[c.doc_off[d]:c.doc_off[d + 1]]
+        df[np.unique(ws[ws < c.V])] += 1
+    with np.errstate(divide="ignore"):
+        vw = np.log(c.D / df.astype(np.float64)).astype(np.float32)
+    wt = np.zeros(len(c.words), dtype=np.float32)
+    m = c.words < c.V
+    wt[m] = vw[c.words[m]]
+    return wt, vw
+
+
+def weights_pmi(corpus):
+    """TermWeight.PMI token weights: vocabWeights[v] = (float)(cf[v] / (double)totCf)
+    (LDAModel.hpp:1114-1121; cf over every token of the corpus), token weight
+    max((float)log(tf / vocabWeights[v] / len), 0) with tf the word's count in
+    the document and len the document's token count, in float (:804-807)."""
+    c = corpus
+    nv = int(c.words.max()) + 1 if len(c.words) else 0
+    cf = np.bincount(c.words.astype(np.int64), minlength=max(nv, c.V)).astype(np.float64)
+    tot = float(len(c.words))
+    vw = (cf[:c.V] / tot).astype(np.float32)
+    wt = np.zeros(len(c.words), dtype=np.float32)
+    for d in range(c.D):
+        b, e = int(c.doc_off[d]), int(c.doc_off[d + 1])
+        ws = c.words[b:e]
+        m = ws < c.V
+        tf = np.bincount(ws[m].astype(np.int64), minlength=c.V)
+        q = (tf[ws[m]].astype(np.float32) / vw[ws[m]]) / np.float32(e - b)
+        wt[b:e][m] = np.maximum(np.log(q.astype(np.float64)).astype(np.float32), np.float32(0))
+    return wt, vw
+
+
+class StateW:
+    """Weighted counts (TermWeight IDF / PMI) for the device sweep's semantics:
+    float n_dk rows updated in token order, float n_kw / n_k folded between
+    document groups from integer deltas in units of 2^-24."""
+
+    def __init__(self, corpus, K, alpha, eta, seed, weights, z0=None):
+        self.c = corpus
+        self.K = int(K)
+        self.alpha = f32(np.broadcast_to(np.asarray(alpha, dtype=np.float32), (self.K,)).copy())
+        self.eta = float(np.float32(eta))
+        self.seed = int(seed)
+        self.wt = np.ascontiguousarray(weights, dtype=np.float32)
+        n_all = len(corpus.words)
+        if z0 is None:
+            self.z = np.zeros(max(n_all, 1), dtype=np.uint16)
+            lib.orc_init_z(n_all, _ptr(corpus.words), corpus.V, self.K, _ptr(self.alpha), self.seed,
+                           _ptr(self.z))
+            self.z = self.z[:n_all]
+        else:
+            self.z = np.ascontiguousarray(z0, dtype=np.uint16).copy()
+        self.recount()
+
+    def recount(self):
+        c = self.c
+        self.ndk = np.zeros((c.D, self.K), dtype=np.float32)
+        self.doc_wlen = np.zeros(max(c.D, 1), dtype=np.float32)
+        self.nkw = np.zeros((c.V, self.K), dtype=np.float32)
+        self.nk = np.zeros(self.K, dtype=np.float32)
+        lib.orc_counts_from_z_w(c.D, _ptr(c.doc_off), _ptr(c.words), _ptr(self.z), _ptr(self.wt), c.V, self.K,
+                                _ptr(self.ndk), _ptr(self.doc_wlen), _ptr(self.nkw), _ptr(self.nk))
+
+    group_bounds = State.group_bounds
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+        c = self.c
+        order, b = self.group_bounds(groups)
+        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
+        dkw = np.zeros((c.V, self.K), dtype=np.int64)
+        dk = np.zeros(self.K, dtype=np.int64)
+        for it in range(iters):
+            for part in parts:
+                if len(part) == 0:
+                    continue
+                lib.orc_fold_w(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), _ptr(dkw), _ptr(dk))
+                lib.orc_sweep_doc_live_w_subset(self.K, c.V, _ptr(self.alpha), self.eta, self.seed,
+                                                start_step + it, _ptr(c.doc_off), _ptr(c.words), _ptr(self.wt),
+                                                _ptr(self.ndk), _ptr(self.nkw), _ptr(self.nk), _ptr(dkw), _ptr(dk),
+                                                _ptr(self.z), _ptr(part), len(part))
+            lib.orc_fold_w(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), _ptr(dkw), _ptr(dk))
+
+    def optimize_alpha(self):
+        lib.orc_optimize_alpha_w(self.c.D, self.K, _ptr(self.ndk), _ptr(self.doc_wlen), _ptr(self.alpha))
+
+    def ll_f64(self):
+        c = self.c
+        a = lib.orc_ll_docs_w_f64(c.D, self.K, _ptr(self.ndk), _ptr(self.doc_wlen), _ptr(self.alpha))
+        b = lib.orc_ll_rest_w_f64(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), self.eta)
+        return a, b
+
+    def ll_per_word(self):
+        """ll / realN: tomotopy counts weightedN in prepare() before the
+        weights exist (TopicModel.hpp:507-523, 652-655), so a freshly trained
+        weighted model divides by the token count."""
+        a, b = self.ll_f64()
+        return (a + b) / self.c.N
+
+
 class Partition:
     """tomotopy's PARTITION scheme on host threads (the CPU baseline)."""
 
@@ -298,4 +414,19 @@ def infer_doc(K, V, alpha, eta, nkw, nk, words, iters, seed, doc_key):
     ll = lib.orc_infer_doc(K, V, _ptr(a), float(np.float32(eta)), _ptr(np.ascontiguousarray(nkw, np.int32)),
                            _ptr(np.ascontiguousarray(nk, np.int32)), _ptr(words), len(words), iters, seed,
                            doc_key, _ptr(z), _ptr(ndk), _ptr(theta))
+    return ll, z[:len(words)], ndk, theta
+
+
+def infer_doc_w(K, V, alpha, eta, nkw, nk, words, weights, iters, seed, doc_key):
+    """Infer one document (ids sorted ascending, one weight per word within
+    the document) against a frozen model with weighted counts."""
+    words = np.ascontiguousarray(words, dtype=np.uint32)
+    wt = np.ascontiguousarray(weights, dtype=np.float32)
+    z = np.zeros(max(len(words), 1), dtype=np.uint16)
+    ndk = np.zeros(K, dtype=np.float32)
+    theta = np.zeros(K, dtype=np.float32)
+    a = f32(np.broadcast_to(np.asarray(alpha, dtype=np.float32), (K,)).copy())
+    ll = lib.orc_infer_doc_w(K, V, _ptr(a), float(np.float32(eta)), _ptr(np.ascontiguousarray(nkw, np.float32)),
+                             _ptr(np.ascontiguousarray(nk, np.float32)), _ptr(words), _ptr(wt), len(words), iters,
+                             seed, doc_key, _ptr(z), _ptr(ndk), _ptr(theta))
     return ll, z[:len(words)], ndk, theta

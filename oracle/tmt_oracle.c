@@ -1090,3 +1090,444 @@ void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
     orc_sweep_doc_live_subset(K, V, alpha, eta, seed, iter, D, doc_off, words, ndk, nkw, nk,
                               nkw_next, nk_next, z, NULL, D);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Weighted counts: TermWeight IDF / PMI (LDAModel.hpp:287-299, 795-809,     */
+/* 1093-1122; Utils.hpp:132-155)                                            */
+/* ------------------------------------------------------------------------ */
+/* Every token carries a float weight (IDF: vocabWeights[v]; PMI: the
+ * per-document formula); n_dk, n_kw and n_k are float sums of weights and a
+ * decrement clamps at 0 (updateCnt<true>).  The device semantics restated
+ * here: a document's n_dk row is updated in float in token order by its
+ * warp; the model counts are float states that change only between document
+ * groups, by folding the group's deltas, which accumulate as integers in
+ * units of 2^-24 (each token weight rounded to that grid), so the fold is
+ * independent of the order of the atomic adds. */
+int64_t orc_wq(float w)
+{
+    return (int64_t)llrintf(w * 16777216.0f);
+}
+
+float orc_fold(float n, int64_t q)
+{
+    float d = (float)q * 5.9604644775390625e-8f;   /* 2^-24 */
+    float s = n + d;
+    return s > 0.f ? s : 0.f;
+}
+
+void orc_fold_w(uint32_t K, uint32_t V, float* nkw, float* nk, int64_t* dkw, int64_t* dk)
+{
+    for (uint32_t k = 0; k < K; ++k) { nk[k] = orc_fold(nk[k], dk[k]); dk[k] = 0; }
+    for (uint64_t i = 0; i < (uint64_t)V * K; ++i) { nkw[i] = orc_fold(nkw[i], dkw[i]); dkw[i] = 0; }
+}
+
+void orc_counts_from_z_w(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                         const uint16_t* z, const float* wt, uint32_t V, uint32_t K,
+                         float* ndk, float* doc_wlen, float* nkw, float* nk)
+{
+    int64_t* qkw = (int64_t*)calloc((size_t)V * K, sizeof(int64_t));
+    int64_t* qk = (int64_t*)calloc(K, sizeof(int64_t));
+    memset(ndk, 0, (size_t)D * K * sizeof(float));
+    for (uint64_t d = 0; d < D; ++d) {
+        float len = 0.f;
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            float w = wt[i];
+            ndk[d * K + z[i]] += w;
+            len += w;
+            int64_t q = orc_wq(w);
+            qkw[(size_t)v * K + z[i]] += q;
+            qk[z[i]] += q;
+        }
+        doc_wlen[d] = len;
+    }
+    for (uint32_t k = 0; k < K; ++k) nk[k] = orc_fold(0.f, qk[k]);
+    for (uint64_t i = 0; i < (uint64_t)V * K; ++i) nkw[i] = orc_fold(0.f, qkw[i]);
+    free(qkw);
+    free(qk);
+}
+
+void orc_sweep_doc_live_w_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, const float* wt, float* ndk,
+                                 const float* nkw, const float* nk, int64_t* dkw, int64_t* dk,
+                                 uint16_t* z, const uint64_t* docs, uint64_t n_docs)
+{
+    float veta = eta * (float)V;
+    float* R = (float*)malloc(K * sizeof(float));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* phi = (float*)malloc(K * sizeof(float));
+    for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / (nk[k] + veta);
+    for (uint64_t di = 0; di < n_docs; ++di) {
+        uint64_t d = docs ? docs[di] : di;
+        float* row = ndk + d * K;
+        for (uint32_t k = 0; k < K; ++k) A[k] = row[k] + alpha[k];
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            uint16_t zo = z[i];
+            float w = wt[i];
+            const float* col = nkw + (size_t)v * K;
+            float n = row[zo] - w;
+            row[zo] = n > 0.f ? n : 0.f;
+            A[zo] = row[zo] + alpha[zo];
+            for (uint32_t k = 0; k < K; ++k) phi[k] = (col[k] + eta) * R[k];
+            float co = col[zo] - w, no = nk[zo] - w;
+            co = co > 0.f ? co : 0.f;
+            no = no > 0.f ? no : 0.f;
+            float phi_own = (co + eta) * (1.0f / (no + veta));
+            float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, iter, seed));
+            uint16_t zn = (uint16_t)blocked_draw(A, phi, K, zo, phi_own, u);
+            row[zn] = row[zn] + w;
+            A[zn] = row[zn] + alpha[zn];
+            z[i] = zn;
+            if (zn != zo) {
+                int64_t q = orc_wq(w);
+                dkw[(size_t)v * K + zo] -= q; dkw[(size_t)v * K + zn] += q;
+                dk[zo] -= q; dk[zn] += q;
+            }
+        }
+    }
+    free(R); free(A); free(phi);
+}
+
+double orc_ll_docs_w_f64(uint64_t D, uint32_t K, const float* ndk, const float* doc_wlen,
+                         const float* alpha)
+{
+    double ll = 0, as = 0;
+    for (uint32_t k = 0; k < K; ++k) as += (double)alpha[k];
+    double lgas = lgamma(as);
+    for (uint64_t d = 0; d < D; ++d) {
+        double s = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            float c = ndk[d * K + k];
+            if (c == 0.f) continue;
+            s += lgamma((double)c + (double)alpha[k]) - lgamma((double)alpha[k]);
+        }
+        ll += s - (lgamma((double)doc_wlen[d] + as) - lgas);
+    }
+    return ll;
+}
+
+double orc_ll_rest_w_f64(uint32_t K, uint32_t V, const float* nkw, const float* nk, float eta)
+{
+    double ll = 0, e = (double)eta, veta = (double)V * (double)eta;
+    double lge = lgamma(e);
+    ll += lgamma(veta) * K;
+    for (uint32_t k = 0; k < K; ++k) ll -= lgamma((double)nk[k] + veta);
+    for (uint64_t i = 0; i < (uint64_t)V * K; ++i) {
+        if (nkw[i] == 0.f) continue;
+        ll += lgamma((double)nkw[i] + e) - lge;
+    }
+    return ll;
+}
+
+void orc_optimize_alpha_w(uint64_t D, uint32_t K, const float* ndk, const float* doc_wlen, float* alpha)
+{
+    for (int it = 0; it < 10; ++it) {
+        float as = alpha_sum_f(K, alpha);
+        float dsum = orc_digammaT(as);
+        double denom = 0;
+        for (uint64_t d = 0; d < D; ++d)
+            denom += (double)(orc_digammaApprox(doc_wlen[d] + as) - dsum);
+        for (uint32_t k = 0; k < K; ++k) {
+            float dk = orc_digammaT(alpha[k]);
+            double nom = 0;
+            for (uint64_t d = 0; d < D; ++d)
+                nom += (double)(orc_digammaApprox(ndk[d * K + k] + alpha[k]) - dk);
+            float a = (float)nom / (float)denom * alpha[k];
+            alpha[k] = a > 1e-5f ? a : 1e-5f;
+        }
+    }
+}
+
+/* Per-document infer with weighted counts: the device's k_infer_slots<WT>.
+ * n_dk starts from z0 in token order; within a run of one word (weight w),
+ * B_k = (n_kw[k,v] + own_k * w) + eta, R_k = 1 / ((n_k[k] + n_dk[k]) + V*eta);
+ * a removal clamps n_dk at 0; the document length is its weight sum. */
+double orc_infer_doc_w(uint32_t K, uint32_t V, const float* alpha, float eta,
+                       const float* nkw, const float* nk,
+                       const uint32_t* words, const float* wt, uint32_t len, uint32_t iters,
+                       uint64_t seed, uint64_t doc_key, uint16_t* z, float* ndk, float* theta)
+{
+    float veta = eta * (float)V;
+    uint64_t key = seed ^ (uint64_t)ORC_STREAM_INFER;
+    uint32_t klo = (uint32_t)doc_key, khi = (uint32_t)(doc_key >> 32);
+    int32_t* own = (int32_t*)calloc(K, sizeof(int32_t));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* BR = (float*)malloc(K * sizeof(float));
+    float* acum = (float*)malloc(K * sizeof(float));
+    float s = 0.f, wsum = 0.f;
+    for (uint32_t k = 0; k < K; ++k) { s = s + alpha[k]; acum[k] = s; }
+    memset(ndk, 0, K * sizeof(float));
+    for (uint32_t j = 0; j < len; ++j) {
+        if (words[j] >= V) { z[j] = 0xFFFF; continue; }
+        float u = orc_u01(philox_first(j, 0xFFFFFFFFu, klo, khi, key));
+        z[j] = (uint16_t)orc_sample_acc(acum, K, u);
+    }
+    for (uint32_t j = 0; j < len; ++j) {
+        if (words[j] >= V) continue;
+        ndk[z[j]] = ndk[z[j]] + wt[j];
+        wsum = wsum + wt[j];
+    }
+    for (uint32_t it = 0; it < iters; ++it) {
+        uint32_t rb = 0;
+        while (rb < len) {
+            uint32_t re = rb + 1;
+            while (re < len && words[re] == words[rb]) ++re;
+            uint32_t v = words[rb];
+            if (v < V) {
+                float w = wt[rb];
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+                const float* g = nkw + (size_t)v * K;
+                for (uint32_t j = rb; j < re; ++j) {
+                    uint16_t zo = z[j];
+                    own[zo]--;
+                    float n = ndk[zo] - w;
+                    ndk[zo] = n > 0.f ? n : 0.f;
+                    for (uint32_t k = 0; k < K; ++k) {
+                        A[k] = ndk[k] + alpha[k];
+                        float B = (g[k] + (float)own[k] * w) + eta;
+                        float R = 1.0f / ((nk[k] + ndk[k]) + veta);
+                        BR[k] = B * R;
+                    }
+                    float u = orc_u01(philox_first(j, it, klo, khi, key));
+                    uint16_t zn = (uint16_t)blocked_draw(A, BR, K, 0xFFFFFFFFu, 0.f, u);
+                    z[j] = zn;
+                    ndk[zn] = ndk[zn] + w;
+                    own[zn]++;
+                }
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]--;
+            }
+            rb = re;
+        }
+    }
+    double e = (double)eta, vd = (double)V * (double)eta, ll = 0, as = 0;
+    float asf = 0.f;
+    for (uint32_t k = 0; k < K; ++k) { as += (double)alpha[k]; asf = asf + alpha[k]; }
+    for (uint32_t k = 0; k < K; ++k) {
+        if (ndk[k] == 0.f) continue;
+        ll += lgamma((double)nk[k] + vd) - lgamma(((double)nk[k] + (double)ndk[k]) + vd);
+        ll += lgamma((double)ndk[k] + alpha[k]) - lgamma((double)alpha[k]);
+    }
+    ll -= lgamma((double)wsum + as) - lgamma(as);
+    uint32_t rb = 0;
+    while (rb < len) {
+        uint32_t re = rb + 1;
+        while (re < len && words[re] == words[rb]) ++re;
+        uint32_t v = words[rb];
+        if (v < V) {
+            const float* g = nkw + (size_t)v * K;
+            float w = wt[rb];
+            for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+            for (uint32_t j = rb; j < re; ++j) {
+                uint32_t k = z[j];
+                int32_t c = own[k];
+                if (!c) continue;
+                double after = lgamma(((double)g[k] + (double)((float)c * w)) + e);
+                double before = g[k] != 0.f ? lgamma((double)g[k] + e) : lgamma(e);
+                ll += after - before;
+                own[k] = 0;
+            }
+        }
+        rb = re;
+    }
+    if (theta)
+        for (uint32_t k = 0; k < K; ++k) theta[k] = (ndk[k] + alpha[k]) / (wsum + asf);
+    free(own); free(A); free(BR); free(acum);
+    return ll;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Word priors: set_word_prior (LDAModel.hpp:1031-1045, 724-737, 99-117)     */
+/* ------------------------------------------------------------------------ */
+/* etaByTopicWord is eta everywhere except the columns of prior words (pidx[v]
+ * >= 0 names row pidx[v] of `prior`, K floats); esum[k] = its row sums,
+ * rounded once to float from a double sum over v = 0..V-1.  z0 of every token
+ * ~ Discrete(its word's column) (updateStateWithDoc, :765-779), drawn like
+ * orc_init_z from the column's sequential float cumulative sum. */
+void orc_prior_esum(uint32_t K, uint32_t V, const int32_t* pidx, const float* prior, float eta, float* esum)
+{
+    for (uint32_t k = 0; k < K; ++k) {
+        double s = 0;
+        for (uint32_t v = 0; v < V; ++v) s += (double)(pidx[v] >= 0 ? prior[(size_t)pidx[v] * K + k] : eta);
+        esum[k] = (float)s;
+    }
+}
+
+static void column_cum(uint32_t K, const float* col, float eta, float* cum)
+{
+    float s = 0.f;
+    for (uint32_t k = 0; k < K; ++k) { s = s + (col ? col[k] : eta); cum[k] = s; }
+}
+
+void orc_init_z_p(uint64_t N, const uint32_t* words, uint32_t V, uint32_t K, const int32_t* pidx,
+                  const float* prior, float eta, uint64_t seed, uint16_t* z)
+{
+    float* cum = (float*)malloc(K * sizeof(float));
+    for (uint64_t i = 0; i < N; ++i) {
+        uint32_t v = words[i];
+        if (v >= V) { z[i] = 0xFFFF; continue; }
+        column_cum(K, pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL, eta, cum);
+        float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_INIT, 0, seed));
+        z[i] = (uint16_t)orc_sample_acc(cum, K, u);
+    }
+    free(cum);
+}
+
+/* one document group of the doc-major sweep with word priors:
+ *   R_k = 1 / ((float)n_k[k] + esum_k), phi_k = ((float)n_kw[k,v] + eta_kv) * R_k,
+ *   phi_own = ((float)(n_kw[zo,v] - 1) + eta_{zo,v}) * (1 / ((float)(n_k[zo] - 1) + esum_zo)) */
+void orc_sweep_doc_live_p_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
+                                 const int32_t* pidx, const float* prior, const float* esum,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, int32_t* ndk,
+                                 const int32_t* nkw, const int32_t* nk,
+                                 int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                                 const uint64_t* docs, uint64_t n_docs)
+{
+    float* R = (float*)malloc(K * sizeof(float));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* phi = (float*)malloc(K * sizeof(float));
+    for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / ((float)nk[k] + esum[k]);
+    for (uint64_t di = 0; di < n_docs; ++di) {
+        uint64_t d = docs ? docs[di] : di;
+        int32_t* row = ndk + d * K;
+        for (uint32_t k = 0; k < K; ++k) A[k] = (float)row[k] + alpha[k];
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            uint16_t zo = z[i];
+            const int32_t* col = nkw + (size_t)v * K;
+            const float* pe = pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL;
+            row[zo]--;
+            A[zo] = (float)row[zo] + alpha[zo];
+            for (uint32_t k = 0; k < K; ++k) phi[k] = ((float)col[k] + (pe ? pe[k] : eta)) * R[k];
+            float phi_own = ((float)(col[zo] - 1) + (pe ? pe[zo] : eta)) * (1.0f / ((float)(nk[zo] - 1) + esum[zo]));
+            float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, iter, seed));
+            uint16_t zn = (uint16_t)blocked_draw(A, phi, K, zo, phi_own, u);
+            row[zn]++;
+            A[zn] = (float)row[zn] + alpha[zn];
+            z[i] = zn;
+            if (zn != zo) {
+                nkw_next[(size_t)v * K + zo]--; nkw_next[(size_t)v * K + zn]++;
+                nk_next[zo]--; nk_next[zn]++;
+            }
+        }
+    }
+    free(R); free(A); free(phi);
+}
+
+/* getLLRest with etaByTopicWord (LDAModel.hpp:636-651), FP64 */
+double orc_ll_rest_p_f64(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta,
+                         const int32_t* pidx, const float* prior, const float* esum)
+{
+    double ll = 0, e = (double)eta, lge = lgamma(e);
+    for (uint32_t k = 0; k < K; ++k) ll += lgamma((double)esum[k]) - lgamma((double)nk[k] + (double)esum[k]);
+    for (uint32_t v = 0; v < V; ++v) {
+        const float* pe = pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL;
+        for (uint32_t k = 0; k < K; ++k) {
+            int32_t c = nkw[(size_t)v * K + k];
+            if (!c) continue;
+            if (pe) ll += lgamma((double)c + (double)pe[k]) - lgamma((double)pe[k]);
+            else ll += lgamma((double)c + e) - lge;
+        }
+    }
+    return ll;
+}
+
+/* per-document infer with word priors: z0 from the word's column, R_k =
+ * 1 / ((float)(n_k + n_dk) + esum_k), B_k = (float)(n_kw + own) + eta_kv */
+double orc_infer_doc_p(uint32_t K, uint32_t V, const float* alpha, float eta,
+                       const int32_t* pidx, const float* prior, const float* esum,
+                       const int32_t* nkw, const int32_t* nk,
+                       const uint32_t* words, uint32_t len, uint32_t iters,
+                       uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk, float* theta)
+{
+    uint64_t key = seed ^ (uint64_t)ORC_STREAM_INFER;
+    uint32_t klo = (uint32_t)doc_key, khi = (uint32_t)(doc_key >> 32);
+    int32_t* own = (int32_t*)calloc(K, sizeof(int32_t));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* BR = (float*)malloc(K * sizeof(float));
+    float* cum = (float*)malloc(K * sizeof(float));
+    memset(ndk, 0, K * sizeof(int32_t));
+    for (uint32_t j = 0; j < len; ++j) {
+        uint32_t v = words[j];
+        if (v >= V) { z[j] = 0xFFFF; continue; }
+        column_cum(K, pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL, eta, cum);
+        float u = orc_u01(philox_first(j, 0xFFFFFFFFu, klo, khi, key));
+        uint16_t k = (uint16_t)orc_sample_acc(cum, K, u);
+        z[j] = k;
+        ndk[k]++;
+    }
+    for (uint32_t it = 0; it < iters; ++it) {
+        uint32_t rb = 0;
+        while (rb < len) {
+            uint32_t re = rb + 1;
+            while (re < len && words[re] == words[rb]) ++re;
+            uint32_t v = words[rb];
+            if (v < V) {
+                const float* pe = pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL;
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+                const int32_t* g = nkw + (size_t)v * K;
+                for (uint32_t j = rb; j < re; ++j) {
+                    uint16_t zo = z[j];
+                    own[zo]--;
+                    ndk[zo]--;
+                    for (uint32_t k = 0; k < K; ++k) {
+                        A[k] = (float)ndk[k] + alpha[k];
+                        float B = (float)(g[k] + own[k]) + (pe ? pe[k] : eta);
+                        float R = 1.0f / ((float)(nk[k] + ndk[k]) + esum[k]);
+                        BR[k] = B * R;
+                    }
+                    float u = orc_u01(philox_first(j, it, klo, khi, key));
+                    uint16_t zn = (uint16_t)blocked_draw(A, BR, K, 0xFFFFFFFFu, 0.f, u);
+                    z[j] = zn;
+                    ndk[zn]++;
+                    own[zn]++;
+                }
+                for (uint32_t j = rb; j < re; ++j) own[z[j]]--;
+            }
+            rb = re;
+        }
+    }
+    double e = (double)eta, ll = 0, as = 0;
+    float asf = 0.f;
+    uint32_t n = 0;
+    for (uint32_t k = 0; k < K; ++k) { as += (double)alpha[k]; asf = asf + alpha[k]; }
+    for (uint32_t j = 0; j < len; ++j) n += words[j] < V;
+    for (uint32_t k = 0; k < K; ++k) {
+        if (!ndk[k]) continue;
+        double es = (double)esum[k];
+        ll += lgamma((double)nk[k] + es) - lgamma((double)(nk[k] + ndk[k]) + es);
+        ll += lgamma((double)ndk[k] + alpha[k]) - lgamma((double)alpha[k]);
+    }
+    ll -= lgamma((double)n + as) - lgamma(as);
+    uint32_t rb = 0;
+    while (rb < len) {
+        uint32_t re = rb + 1;
+        while (re < len && words[re] == words[rb]) ++re;
+        uint32_t v = words[rb];
+        if (v < V) {
+            const int32_t* g = nkw + (size_t)v * K;
+            const float* pe = pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL;
+            for (uint32_t j = rb; j < re; ++j) own[z[j]]++;
+            for (uint32_t j = rb; j < re; ++j) {
+                uint32_t k = z[j];
+                int32_t c = own[k];
+                if (!c) continue;
+                double ek = pe ? (double)pe[k] : e;
+                double after = lgamma((double)(g[k] + c) + ek);
+                double before = g[k] ? lgamma((double)g[k] + ek) : lgamma(ek);
+                ll += after - before;
+                own[k] = 0;
+            }
+        }
+        rb = re;
+    }
+    if (theta)
+        for (uint32_t k = 0; k < K; ++k) theta[k] = ((float)ndk[k] + alpha[k]) / ((float)n + asf);
+    free(own); free(A); free(BR); free(cum);
+    return ll;
+}

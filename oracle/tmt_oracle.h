@@ -170,6 +170,59 @@ double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
                      const uint32_t* words, uint32_t len, uint32_t iters,
                      uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk_out, float* theta);
 
+/* ---- weighted counts: TermWeight IDF / PMI ----------------------------- */
+/* Tokens carry float weights (LDAModel.hpp:795-809, 1093-1122); counts are
+ * float sums and decrements clamp at 0 (Utils.hpp:132-155).  Device
+ * semantics: n_dk rows change in float in token order; n_kw / n_k are float
+ * states folded between document groups from integer deltas in units of
+ * 2^-24 (orc_wq), so the fold does not depend on the order of the adds. */
+int64_t orc_wq(float w);                 /* llrintf(w * 2^24) */
+float   orc_fold(float n, int64_t q);    /* max(n + (float)q * 2^-24, 0) */
+void orc_fold_w(uint32_t K, uint32_t V, float* nkw, float* nk, int64_t* dkw, int64_t* dk);
+/* counts from z: n_dk and the document weight sums in token order (the
+ * reference's accumulation), n_kw / n_k folded from zero */
+void orc_counts_from_z_w(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                         const uint16_t* z, const float* wt, uint32_t V, uint32_t K,
+                         float* ndk, float* doc_wlen, float* nkw, float* nk);
+/* one document group of a weighted sweep: reads the folded state, writes
+ * deltas to dkw / dk */
+void orc_sweep_doc_live_w_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, const float* wt, float* ndk,
+                                 const float* nkw, const float* nk, int64_t* dkw, int64_t* dk,
+                                 uint16_t* z, const uint64_t* docs, uint64_t n_docs);
+double orc_ll_docs_w_f64(uint64_t D, uint32_t K, const float* ndk, const float* doc_wlen,
+                         const float* alpha);
+double orc_ll_rest_w_f64(uint32_t K, uint32_t V, const float* nkw, const float* nk, float eta);
+void orc_optimize_alpha_w(uint64_t D, uint32_t K, const float* ndk, const float* doc_wlen, float* alpha);
+/* per-document infer against a frozen weighted model; words sorted by id,
+ * every token of one word carrying the same weight */
+double orc_infer_doc_w(uint32_t K, uint32_t V, const float* alpha, float eta,
+                       const float* nkw, const float* nk,
+                       const uint32_t* words, const float* wt, uint32_t len, uint32_t iters,
+                       uint64_t seed, uint64_t doc_key, uint16_t* z, float* ndk, float* theta);
+
+/* ---- word priors (set_word_prior; LDAModel.hpp:99-117, 636-651, 724-737, 765-779) --- */
+/* pidx[v] >= 0: word v's eta column is row pidx[v] of prior (K floats), else
+ * eta everywhere; esum[k] = the rows' sums rounded once from double. */
+void orc_prior_esum(uint32_t K, uint32_t V, const int32_t* pidx, const float* prior, float eta, float* esum);
+void orc_init_z_p(uint64_t N, const uint32_t* words, uint32_t V, uint32_t K, const int32_t* pidx,
+                  const float* prior, float eta, uint64_t seed, uint16_t* z);
+void orc_sweep_doc_live_p_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
+                                 const int32_t* pidx, const float* prior, const float* esum,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, int32_t* ndk,
+                                 const int32_t* nkw, const int32_t* nk,
+                                 int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                                 const uint64_t* docs, uint64_t n_docs);
+double orc_ll_rest_p_f64(uint32_t K, uint32_t V, const int32_t* nkw, const int32_t* nk, float eta,
+                         const int32_t* pidx, const float* prior, const float* esum);
+double orc_infer_doc_p(uint32_t K, uint32_t V, const float* alpha, float eta,
+                       const int32_t* pidx, const float* prior, const float* esum,
+                       const int32_t* nkw, const int32_t* nk,
+                       const uint32_t* words, uint32_t len, uint32_t iters,
+                       uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk, float* theta);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,44 @@ def test_sweeps_bitexact(K, groups):
         assert_same_state(eng, st)
 
 
+@pytest.mark.parametrize("K,groups", [(24, 8), (300, 3)])
+def test_graph_sweeps_identical_to_launches(K, groups):
+    """Sweeps replayed as CUDA graphs (after the autotuner's eager sweeps) give
+    the same z, counts, alpha and ll history as kernel-by-kernel launches,
+    across train() calls, ll points, alpha optimisation and a seed change;
+    and the graph sweeps equal the oracle's."""
+    off, w, V = corpus(V=900, D=160, mean=60, seed=K, min_cf=2, lognormal=True)
+    out = []
+    for graphs in (True, False):
+        eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=13, optim_interval=5, sweep_groups=groups)
+        eng.set_graphs(graphs)
+        eng.upload(off, w)
+        lls = [eng.train(9, ll_every=3)]
+        eng.train(4)
+        lib_set_seed(eng, 99)
+        lls.append(eng.train(6, ll_every=2))
+        out.append((eng.state(), eng.doc_topic(), np.concatenate(lls), eng.info().kernel_launches))
+    (sa, ndk_a, ll_a, la), (sb, ndk_b, ll_b, lb) = out
+    for x, y in zip(sa, sb):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(ndk_a, ndk_b)
+    np.testing.assert_array_equal(ll_a, ll_b)
+    # a captured sweep counts its kernels, plus the sweep-counter kernels of the graph path
+    assert la >= lb
+
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=13, optim_interval=0, sweep_groups=groups)
+    eng.upload(off, w)
+    st = oracle_state(off, w, V, K, 0.1, 0.01, 13)
+    eng.train(6)
+    st.doc_live_sweeps(6, groups=groups)
+    assert_same_state(eng, st)
+
+
+def lib_set_seed(eng, seed):
+    from tomotopy_b200._lib import lib, check
+    check(lib.tmt_set_seed(eng.h, seed), eng.h)
+
+
 def test_counts_invariant_after_every_sweep():
     off, w, V = corpus(V=1500, D=300, mean=80, seed=3, lognormal=True)
     K = 50

@@ -58,14 +58,15 @@ class TmtServerStats(C.Structure):
 class TmtModelArgs(C.Structure):
     _fields_ = [("K", C.c_uint32), ("alpha", C.POINTER(C.c_float)), ("n_alpha", C.c_uint32), ("eta", C.c_float),
                 ("seed", C.c_uint64), ("min_cf", C.c_uint64), ("min_df", C.c_uint64), ("rm_top", C.c_uint64),
-                ("device", C.c_int32), ("sweep_groups", C.c_uint32)]
+                ("device", C.c_int32), ("sweep_groups", C.c_uint32), ("tw", C.c_int32)]
 
 
 class TmtModelInfo(C.Structure):
     _fields_ = [("K", C.c_uint32), ("V", C.c_uint32), ("n_vocab", C.c_uint32), ("n_docs", C.c_uint64),
                 ("N", C.c_uint64), ("global_step", C.c_uint64), ("prepared", C.c_int32), ("alpha", C.c_float),
                 ("eta", C.c_float), ("optim_interval", C.c_uint32), ("burn_in", C.c_uint32), ("seed", C.c_uint64),
-                ("min_cf", C.c_uint64), ("min_df", C.c_uint64), ("rm_top", C.c_uint64)]
+                ("min_cf", C.c_uint64), ("min_df", C.c_uint64), ("rm_top", C.c_uint64), ("tw", C.c_int32),
+                ("weighted_n", C.c_double)]
 
 
 class TmtSynthSpec(C.Structure):
@@ -80,9 +81,12 @@ _H = C.c_void_p
 SIGNATURES = {
     "tmt_create": (C.c_int, [C.POINTER(TmtConfig), C.POINTER(_H)]),
     "tmt_upload_corpus": (C.c_int, [_H, _P, _P, C.c_uint64, _P]),
+    "tmt_upload_corpus_weighted": (C.c_int, [_H, _P, _P, C.c_uint64, _P, _P]),
+    "tmt_download_counts_f32": (C.c_int, [_H, _P, _P, _P, _P]),
     "tmt_train": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P]),
     "tmt_ll": (C.c_int, [_H, _P, _P]),
     "tmt_set_counts": (C.c_int, [_H, _P, _P]),
+    "tmt_set_counts_f32": (C.c_int, [_H, _P, _P]),
     "tmt_set_alpha": (C.c_int, [_H, _P]),
     "tmt_corpus_counts": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P]),
     "tmt_prepare_corpus_counted": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint64, C.c_uint64,
@@ -91,8 +95,10 @@ SIGNATURES = {
     "tmt_upload_shard": (C.c_int, [_H, _P, _P, C.c_uint64, _P, C.POINTER(TmtShard)]),
     "tmt_set_global_step": (C.c_int, [_H, C.c_uint64]),
     "tmt_set_seed": (C.c_int, [_H, C.c_uint64]),
+    "tmt_set_graphs": (C.c_int, [_H, C.c_int32]),
     "tmt_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
     "tmt_infer_batch": (C.c_int, [_H, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P]),
+    "tmt_infer_batch_weighted": (C.c_int, [_H, _P, _P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P, _P, _P]),
     "tmt_download_state": (C.c_int, [_H, _P, _P, _P, _P]),
     "tmt_download_doc_topic": (C.c_int, [_H, _P]),
     "tmt_get_info": (C.c_int, [_H, C.POINTER(TmtInfo)]),

@@ -20,6 +20,19 @@ __device__ __forceinline__ float hs_scan32(float x, int lane)
     return x;
 }
 
+// the first `steps` steps of hs_scan32 (steps is warp-uniform, 0..5)
+__device__ __forceinline__ float hs_scan_n(float x, int lane, int steps)
+{
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        if (i < steps) {
+            const float y = __shfl_up_sync(FULL, x, 1 << i);
+            if (lane >= (1 << i)) x = __fadd_rn(x, y);
+        }
+    }
+    return x;
+}
+
 __host__ __device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
 
 __device__ __forceinline__ double warp_sum(double x)

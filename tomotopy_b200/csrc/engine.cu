@@ -170,6 +170,91 @@ __global__ void k_phi_apply(int32_t* __restrict__ nkw, int32_t* __restrict__ del
     }
 }
 
+// ---------------------------------------------------------------------------
+// weighted counts (TermWeight IDF / PMI)
+// ---------------------------------------------------------------------------
+// A token of weight w adds round(w * 2^24) to the integer deltas; a fold adds
+// the deltas to the float state, n' = max(n + (float)q * 2^-24, 0), and zeroes
+// them.  Integer deltas make the fold independent of the order of the adds.
+__device__ __forceinline__ long long wq_of(float w)
+{
+    return __float2ll_rn(__fmul_rn(w, 16777216.f));
+}
+
+__device__ __forceinline__ float fold_w(float n, long long q)
+{
+    const float s = __fadd_rn(n, __fmul_rn(__ll2float_rn(q), 5.9604644775390625e-8f));
+    return s > 0.f ? s : 0.f;
+}
+
+__global__ void k_nk_fold_w(float* __restrict__ nk, long long* __restrict__ dk, uint32_t K)
+{
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+        nk[k] = fold_w(nk[k], dk[k]);
+        dk[k] = 0;
+    }
+}
+
+// n_kw fold (fold != 0) and, when phi != NULL, the word table of the state
+__global__ void k_phi_fold_w(float* __restrict__ nkw, long long* __restrict__ dkw, const float* __restrict__ nk,
+                             uint32_t V, uint32_t K, uint32_t KP, float eta, float veta, float* __restrict__ phi,
+                             uint32_t smem_k, int fold)
+{
+    extern __shared__ float s_R[];
+    const bool r_smem = phi && K <= smem_k;
+    if (r_smem)
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) s_R[k] = __fdiv_rn(1.0f, __fadd_rn(nk[k], veta));
+    __syncthreads();
+    for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
+        float* col = nkw + v * K;
+        long long* dcol = dkw + v * K;
+        float* ph = phi ? phi + v * KP : nullptr;
+        for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
+            float val = 0.f;
+            if (k < K) {
+                float n = col[k];
+                if (fold) {
+                    n = fold_w(n, dcol[k]);
+                    col[k] = n;
+                    dcol[k] = 0;
+                }
+                if (ph) {
+                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn(nk[k], veta));
+                    val = __fmul_rn(__fadd_rn(n, eta), R);
+                }
+            }
+            if (ph) ph[k] = val;
+        }
+    }
+}
+
+// Weighted counts from z, thread per document: n_dk and the document's weight
+// sum accumulate in float in token order (addWordTo in initializeDocState and
+// updateSumWordWeight, LDAModel.hpp:795-809, LDA.h:113-116); n_kw and n_k go
+// to the integer deltas (folded afterwards).
+__global__ void k_counts_w(const uint64_t* __restrict__ doc_off, const uint32_t* __restrict__ words,
+                           const uint16_t* __restrict__ z, const float* __restrict__ wt, uint64_t D, uint32_t K,
+                           uint32_t V, float* __restrict__ ndk, long long* __restrict__ dkw,
+                           long long* __restrict__ dk, float* __restrict__ doc_wlen)
+{
+    for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < D; d += (uint64_t)gridDim.x * blockDim.x) {
+        float* row = ndk + d * K;
+        float len = 0.f;
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            const uint32_t v = words[i];
+            if (v >= V) continue;
+            const float w = wt[i];
+            const uint32_t k = z[i];
+            row[k] = __fadd_rn(row[k], w);
+            len = __fadd_rn(len, w);
+            const unsigned long long q = (unsigned long long)wq_of(w);
+            atomicAdd(reinterpret_cast<unsigned long long*>(dkw) + (uint64_t)v * K + k, q);
+            atomicAdd(reinterpret_cast<unsigned long long*>(dk) + k, q);
+        }
+        doc_wlen[d] = len;
+    }
+}
+
 struct SweepArgs {
     const uint64_t* doc_off;
     const uint32_t* words;
@@ -183,20 +268,28 @@ struct SweepArgs {
     const float* alpha;
     const uint32_t* doc_order;
     uint32_t* doc_counter;
+    // weighted counts (TermWeight IDF / PMI): ndk, nkw and nk hold floats,
+    // the deltas go to dkw / dk in units of 2^-24
+    const float* wt;          // token weights (doc-major)
+    long long* dkw;           // V x K
+    long long* dk;            // K
     uint64_t D;
     uint32_t K, V, c;
     float eta, veta;
     uint64_t seed;
     uint32_t iter;
+    const uint32_t* iter_ptr; // non-null (a captured sweep): the sweep counter lives on the device
     uint64_t pos_begin, pos_end;  // this launch samples doc_order positions [pos_begin, pos_end)
     uint64_t tok_offset;     // global index of token 0 (a shard of a corpus split across GPUs)
+    uint32_t scan_steps;     // Hillis-Steele steps over the lanes holding topics: ceil(log2(min(32, ceil(K/4))))
     uint32_t rowi_smem;      // 1: the int n_dk row lives in shared memory
     uint32_t dnk_smem;       // 1: n_k deltas aggregate in shared memory
 };
 
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
 // aligned regions): [n_k deltas: KP ints] [per warp: (float)n_dk + alpha, KP
-// floats, zero padded] [per warp: n_dk, KP ints].
+// floats, zero padded] [per warp: n_dk, KP ints (floats with weighted counts)].
+// With weighted counts the n_k deltas are KP long longs.
 
 
 
@@ -207,36 +300,45 @@ struct SweepArgs {
 //   CH == 0: any K, runtime loops.
 //   PF: the next token's word weights are loaded while the current token is
 //       sampled (the loads do not depend on the document row).
-template <int CH, int MINB, bool PF>
+//   WT: weighted counts (TermWeight IDF / PMI): n_dk, n_kw, n_k are floats,
+//       every token carries a weight w, a removal clamps at 0 (updateCnt<true>,
+//       Utils.hpp:132-155) and the count deltas are integers in units of 2^-24.
+template <int CH, int MINB, bool PF, bool WT>
 __global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
+    using CT = typename std::conditional<WT, float, int>::type;
     constexpr int CHR = CH > 0 ? CH : 1;
     extern __shared__ __align__(16) int smem[];
     const int K = (int)a.K;
     const int KP = (int)round4(a.K);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     int* s_dnk = smem;
-    float* s_rowf = reinterpret_cast<float*>(smem + (a.dnk_smem ? KP : 0));
+    long long* s_dnk64 = reinterpret_cast<long long*>(smem);
+    float* s_rowf = reinterpret_cast<float*>(smem + (a.dnk_smem ? (WT ? 2 * KP : KP) : 0));
     float* rowf = s_rowf + warp * KP;
     int* s_rowi = reinterpret_cast<int*>(s_rowf + nwarps * KP);
     if (a.dnk_smem) {
-        for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            if (WT) s_dnk64[k] = 0;
+            else s_dnk[k] = 0;
+        }
         __syncthreads();
     }
     // blocks of four owned by this lane
     const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
     const float eta = a.eta, veta = a.veta;
+    const uint32_t iter = a.iter_ptr ? *a.iter_ptr : a.iter;
 
-    auto load_word = [&](uint32_t v, int zo, float4 (&pv)[CHR], int& nkw_o, int& nk_o, float& phu) {
+    auto load_word = [&](uint32_t v, int zo, float4 (&pv)[CHR], CT& nkw_o, CT& nk_o, float& phu) {
         const float* ph = a.phi + (uint64_t)v * KP;
         if (CH > 0) {
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
-        nkw_o = __ldg(a.nkw + (uint64_t)v * K + zo);
-        nk_o = __ldg(a.nk + zo);
+        nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
+        nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
         phu = __ldg(ph + zo);
     };
 
@@ -247,12 +349,12 @@ k_sweep_doc(SweepArgs a)
         const uint64_t pos = a.pos_begin + q;
         if (pos >= a.pos_end) break;
         const uint64_t d = a.doc_order[pos];
-        int32_t* grow = a.ndk + d * (uint64_t)K;
-        int* rowi = a.rowi_smem ? (s_rowi + warp * KP) : grow;
+        CT* grow = reinterpret_cast<CT*>(a.ndk) + d * (uint64_t)K;
+        CT* rowi = a.rowi_smem ? reinterpret_cast<CT*>(s_rowi + warp * KP) : grow;
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f;
             if (k < K) {
-                const int n = grow[k];
+                const CT n = grow[k];
                 if (a.rowi_smem) rowi[k] = n;
                 f = __fadd_rn((float)n, __ldg(a.alpha + k));
             }
@@ -263,13 +365,14 @@ k_sweep_doc(SweepArgs a)
         for (uint64_t base = b; base < e; base += 32) {
             const uint64_t my_i = base + lane;
             uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
-            float my_u = 0.f;
+            float my_u = 0.f, my_wt = 0.f;
             if (my_i < e) {
                 my_w = a.words[my_i];
                 my_z = a.z[my_i];
+                if (WT) my_wt = a.wt[my_i];
                 const uint64_t gi = my_i + a.tok_offset;
                 my_u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamSweep,
-                                                a.iter, a.seed));
+                                                iter, a.seed));
             }
             uint32_t my_new = my_z;
             unsigned vm = __ballot_sync(FULL, my_i < e && my_w < a.V);
@@ -279,7 +382,7 @@ k_sweep_doc(SweepArgs a)
                 uint32_t v = __shfl_sync(FULL, my_w, j);
                 int zo = (int)__shfl_sync(FULL, my_z, j);
                 float4 pv[CHR];
-                int nkw_o, nk_o;
+                CT nkw_o, nk_o;
                 float phu;
                 load_word(v, zo, pv, nkw_o, nk_o, phu);
                 for (;;) {
@@ -287,7 +390,7 @@ k_sweep_doc(SweepArgs a)
                     uint32_t vn = 0;
                     int zon = 0;
                     float4 pvn[CHR];
-                    int nkw_on = 0, nk_on = 0;
+                    CT nkw_on = 0, nk_on = 0;
                     float phun = 0.f;
                     if (PF && jn >= 0) {
                         vn = __shfl_sync(FULL, my_w, jn);
@@ -295,15 +398,31 @@ k_sweep_doc(SweepArgs a)
                         load_word(vn, zon, pvn, nkw_on, nk_on, phun);
                     }
                     const float u = __shfl_sync(FULL, my_u, j);
+                    const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
                     const float* ph = a.phi + (uint64_t)v * KP;
                     if (lane == 0) {          // remove the token from its document
-                        const int n = rowi[zo] - 1;
-                        rowi[zo] = n;
-                        rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
+                        if constexpr (WT) {
+                            float n = __fsub_rn(rowi[zo], wt);
+                            n = n > 0.f ? n : 0.f;
+                            rowi[zo] = n;
+                            rowf[zo] = __fadd_rn(n, __ldg(a.alpha + zo));
+                        } else {
+                            const int n = rowi[zo] - 1;
+                            rowi[zo] = n;
+                            rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
+                        }
                     }
                     __syncwarp();
-                    const float phi_own = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eta),
-                                                    __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), veta)));
+                    float phi_own;
+                    if constexpr (WT) {
+                        float co = __fsub_rn(nkw_o, wt), no = __fsub_rn(nk_o, wt);
+                        co = co > 0.f ? co : 0.f;
+                        no = no > 0.f ? no : 0.f;
+                        phi_own = __fmul_rn(__fadd_rn(co, eta), __fdiv_rn(1.0f, __fadd_rn(no, veta)));
+                    } else {
+                        phi_own = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eta),
+                                            __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), veta)));
+                    }
                     // pass 1: fma chain over this lane's topics
                     float s = 0.f;
                     if (CH > 0) {
@@ -331,42 +450,101 @@ k_sweep_doc(SweepArgs a)
                         const float Ao = rowf[zo];
                         s = fmaxf(__fadd_rn(__fsub_rn(s, __fmul_rn(Ao, phu)), __fmul_rn(Ao, phi_own)), 0.f);
                     }
-                    const float x = hs_scan32(s, lane);
+                    // lanes at or above min(32, ceil(K/4)) hold no topics: a Hillis-Steele
+                    // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
+                    // the values of the full scan, and the total sits in lane
+                    // 2^scan_steps - 1
+                    const float x = hs_scan_n(s, lane, a.scan_steps);
                     float E = __shfl_up_sync(FULL, x, 1);
                     if (lane == 0) E = 0.f;
-                    const float total = __shfl_sync(FULL, x, 31);
+                    const float total = __shfl_sync(FULL, x, (1 << a.scan_steps) - 1);
                     const float r = __fmul_rn(u, total);
                     const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
                     int znew = K - 1;
                     if (m) {
-                        // pass 2: position among lane h's topics, 32 at a time
+                        // pass 2: position among lane h's topics
                         const int h = __ffs(m) - 1;
                         const float Eh = __shfl_sync(FULL, E, h);
                         const int mh = K - 4 * h;
                         const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
-                        float carry = 0.f;
                         int found = nh - 1;
-                        for (int mm = 0; mm < nh; mm += 32) {
-                            const int t = mm + lane;
-                            const int k = 128 * (t >> 2) + 4 * h + (t & 3);
-                            float x2 = 0.f;
-                            if (t < nh) x2 = __fmul_rn(rowf[k], k == zo ? phi_own : __ldg(ph + k));
-                            x2 = hs_scan32(x2, lane);
-                            const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
-                            if (mb) { found = mm + __ffs(mb) - 1; break; }
-                            carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                        if (CH > 0 && CH <= 2) {
+                            // at most 8 topics: lane h forms their Hillis-Steele prefix sums
+                            // (the warp-wide scan's order) from the weights in its registers
+                            if (lane == h) {
+                                float c[4 * CHR];
+#pragma unroll
+                                for (int jj = 0; jj < CHR; ++jj) {
+                                    const float4 A4 = jj < nch ? *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * h)
+                                                               : make_float4(0.f, 0.f, 0.f, 0.f);
+                                    const float av[4] = { A4.x, A4.y, A4.z, A4.w };
+                                    const float pw[4] = { pv[jj].x, pv[jj].y, pv[jj].z, pv[jj].w };
+#pragma unroll
+                                    for (int i = 0; i < 4; ++i) {
+                                        const int t = 4 * jj + i;
+                                        const int k = 128 * jj + 4 * h + i;
+                                        c[t] = t < nh ? __fmul_rn(av[i], k == zo ? phi_own : pw[i]) : 0.f;
+                                    }
+                                }
+#pragma unroll
+                                for (int off = 1; off < 4 * CHR; off <<= 1) {
+#pragma unroll
+                                    for (int t = 4 * CHR - 1; t >= off; --t) c[t] = __fadd_rn(c[t], c[t - off]);
+                                }
+                                bool hit = false;
+#pragma unroll
+                                for (int t = 0; t < 4 * CHR; ++t) {
+                                    if (!hit && t < nh && r < __fadd_rn(Eh, c[t])) {
+                                        found = t;
+                                        hit = true;
+                                    }
+                                }
+                            }
+                            found = __shfl_sync(FULL, found, h);
+                        } else {
+                            // 32 at a time; up to 16 topics (CH == 4) a 4-step scan gives the
+                            // same prefix values
+                            constexpr int kSteps2 = CH == 4 ? 4 : 5;
+                            float carry = 0.f;
+                            for (int mm = 0; mm < nh; mm += 32) {
+                                const int t = mm + lane;
+                                const int k = 128 * (t >> 2) + 4 * h + (t & 3);
+                                float x2 = 0.f;
+                                if (t < nh) x2 = __fmul_rn(rowf[k], k == zo ? phi_own : __ldg(ph + k));
+                                x2 = hs_scan_n(x2, lane, kSteps2);
+                                const unsigned mb =
+                                    __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
+                                if (mb) { found = mm + __ffs(mb) - 1; break; }
+                                carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                            }
                         }
                         znew = 128 * (found >> 2) + 4 * h + (found & 3);
                     }
                     if (lane == 0) {
-                        const int n = rowi[znew] + 1;
-                        rowi[znew] = n;
-                        rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
-                        if (znew != zo) {
-                            atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
-                            atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
-                            if (a.dnk_smem) { atomicSub(&s_dnk[zo], 1); atomicAdd(&s_dnk[znew], 1); }
-                            else { atomicSub(&a.nk_next[zo], 1); atomicAdd(&a.nk_next[znew], 1); }
+                        if constexpr (WT) {
+                            const float n = __fadd_rn(rowi[znew], wt);
+                            rowi[znew] = n;
+                            rowf[znew] = __fadd_rn(n, __ldg(a.alpha + znew));
+                            if (znew != zo) {
+                                const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(wt, 16777216.f));
+                                unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
+                                atomicAdd(dw + zo, 0ull - q);
+                                atomicAdd(dw + znew, q);
+                                unsigned long long* dn = a.dnk_smem ? reinterpret_cast<unsigned long long*>(s_dnk64)
+                                                                    : reinterpret_cast<unsigned long long*>(a.dk);
+                                atomicAdd(dn + zo, 0ull - q);
+                                atomicAdd(dn + znew, q);
+                            }
+                        } else {
+                            const int n = rowi[znew] + 1;
+                            rowi[znew] = n;
+                            rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
+                            if (znew != zo) {
+                                atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
+                                atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
+                                if (a.dnk_smem) { atomicSub(&s_dnk[zo], 1); atomicAdd(&s_dnk[znew], 1); }
+                                else { atomicSub(&a.nk_next[zo], 1); atomicAdd(&a.nk_next[znew], 1); }
+                            }
                         }
                     }
                     __syncwarp();
@@ -398,8 +576,14 @@ k_sweep_doc(SweepArgs a)
     }
     if (a.dnk_smem) {
         __syncthreads();
-        for (int k = threadIdx.x; k < K; k += blockDim.x)
-            if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            if constexpr (WT) {
+                if (s_dnk64[k])
+                    atomicAdd(reinterpret_cast<unsigned long long*>(a.dk) + k, (unsigned long long)s_dnk64[k]);
+            } else {
+                if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
+            }
+        }
     }
 }
 
@@ -422,10 +606,13 @@ __global__ void k_ll_prep(const float* __restrict__ alpha, uint32_t K, double* _
     }
 }
 
-__global__ void k_ll_partials(const int32_t* __restrict__ ndk, uint64_t D, uint32_t K,
+// CT: the count type (int32 for TermWeight ONE, float for weighted counts);
+// LT: the document length type (token count or weight sum).
+template <typename CT, typename LT>
+__global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K,
                               const double* __restrict__ lg_alpha, const float* __restrict__ alpha,
-                              const int32_t* __restrict__ doc_len, const double* __restrict__ asum_p,
-                              const int32_t* __restrict__ nkw, uint32_t V, double eta, double lg_eta,
+                              const LT* __restrict__ doc_len, const double* __restrict__ asum_p,
+                              const CT* __restrict__ nkw, uint32_t V, double eta, double lg_eta,
                               double* __restrict__ partials)
 {
     __shared__ double s_d[32], s_r[32];
@@ -435,20 +622,20 @@ __global__ void k_ll_partials(const int32_t* __restrict__ ndk, uint64_t D, uint3
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     double accd = 0, accr = 0;
     for (uint64_t r = gw; r < D; r += nw) {
-        const int32_t* p = ndk + r * K;
+        const CT* p = ndk + r * K;
         for (uint32_t k = lane; k < K; k += 32) {
-            int32_t n = p[k];
-            if (n) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
+            const CT n = p[k];
+            if (n != CT(0)) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
         }
         if (lane == 0) accd -= lgamma((double)doc_len[r] + asum) - lg_asum;
     }
     // the word rows' assignment does not depend on D: LLRest is the same bits on
     // every rank of a sharded corpus and on one GPU holding all of it
     for (uint64_t v = gw; v < V; v += nw) {
-        const int32_t* p = nkw + v * K;
+        const CT* p = nkw + v * K;
         for (uint32_t k = lane; k < K; k += 32) {
-            int32_t n = p[k];
-            if (n) accr += lgamma((double)n + eta) - lg_eta;
+            const CT n = p[k];
+            if (n != CT(0)) accr += lgamma((double)n + eta) - lg_eta;
         }
     }
     accd = warp_sum(accd);
@@ -464,8 +651,9 @@ __global__ void k_ll_partials(const int32_t* __restrict__ ndk, uint64_t D, uint3
     }
 }
 
+template <typename CT>
 __global__ void k_ll_final(const double* __restrict__ partials, uint32_t nparts,
-                           const int32_t* __restrict__ nk, uint32_t K, double veta, double* __restrict__ out)
+                           const CT* __restrict__ nk, uint32_t K, double veta, double* __restrict__ out)
 {
     __shared__ double s_d[32], s_r[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -501,8 +689,9 @@ static __device__ __align__(256) double g_ll_scratch[2 * kNoAllocMaxBlocks + kNo
 // ---------------------------------------------------------------------------
 // part_nom[bx*K + k] = sum over this block's docs of digammaApprox(n_dk + alpha_k)
 // part_den[bx]       = sum over this block's docs of digammaApprox(N_d + sum(alpha))
-__global__ void k_alpha_sums(const int32_t* __restrict__ ndk, uint64_t D, uint32_t K,
-                             const float* __restrict__ alpha, const int32_t* __restrict__ doc_len,
+template <typename CT, typename LT>
+__global__ void k_alpha_sums(const CT* __restrict__ ndk, uint64_t D, uint32_t K,
+                             const float* __restrict__ alpha, const LT* __restrict__ doc_len,
                              const float* __restrict__ asum_p,
                              double* __restrict__ part_nom, double* __restrict__ part_den)
 {
@@ -515,8 +704,8 @@ __global__ void k_alpha_sums(const int32_t* __restrict__ ndk, uint64_t D, uint32
         double acc = 0;
         uint64_t zeros = 0;
         for (uint64_t d = d0; d < d1; ++d) {
-            int32_t n = ndk[d * K + k];
-            if (n) acc += (double)tmt::digamma_approx_f(__fadd_rn((float)n, ak));
+            const CT n = ndk[d * K + k];
+            if (n != CT(0)) acc += (double)tmt::digamma_approx_f(__fadd_rn((float)n, ak));
             else ++zeros;
         }
         acc += (double)zeros * (double)tmt::digamma_approx_f(ak);
@@ -585,6 +774,18 @@ __global__ void k_alpha_fold(const double* __restrict__ part_nom, const double* 
     }
 }
 
+// the sweep counter of captured sweeps: set before a run of graph launches,
+// advanced by the last node of each
+__global__ void k_set_step(uint32_t* __restrict__ step, uint32_t v)
+{
+    *step = v;
+}
+
+__global__ void k_next_step(uint32_t* __restrict__ step)
+{
+    *step += 1;
+}
+
 __global__ void k_sum_alpha(const float* __restrict__ alpha, uint32_t K, float* __restrict__ out)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -636,12 +837,29 @@ struct tmt_handle {
     tmt_allreduce_fn allreduce = nullptr;
     void* ar_user = nullptr;
     int32_t* d_delta = nullptr;      // sharded: one group's count deltas, n_kw (K*V) then n_k (K)
+    // weighted counts (TermWeight IDF / PMI, tmt_upload_corpus_weighted): d_ndk,
+    // d_nkw[0], d_nk[0] hold floats; deltas of a document group in units of 2^-24
+    bool weighted = false;
+    float* d_wt = nullptr;           // token weights, doc-major
+    long long* d_dkw = nullptr;      // V x K
+    long long* d_dk = nullptr;       // K
+    float* d_doc_wlen = nullptr;     // per document: the sum of its token weights
     // sweep-kernel autotuner: variants give bit-identical results, so the
     // first sweeps each time one variant and the fastest is kept
-    int variant = 0;
+    int variant = 0;                 // the variant of the sweep being tuned
     int n_variants = 1;
-    int tuned = -1;                  // chosen variant, -1 while tuning
-    std::vector<float> variant_ms;
+    int tuned = -1;                  // 0 once every group has its variant, -1 while tuning
+    std::vector<int> group_variant;  // per document group, the fastest variant
+    std::vector<std::vector<float>> group_ms;   // tuning: per group, per variant
+    std::vector<cudaEvent_t> gev;    // tuning: start/end of each group's sweep kernel
+    std::vector<std::pair<const void*, int>> occ;   // blocks per SM of each sweep kernel launched
+    // captured sweeps (single GPU, after tuning): one graph per starting buffer parity
+    bool graphs = true;
+    uint32_t* d_step = nullptr;
+    cudaGraphExec_t graph_exec[2] = { nullptr, nullptr };
+    uint64_t graph_kernels = 0;      // kernels in one captured sweep
+    int graph_flip = 0;              // buffer parity change of one sweep
+    std::vector<cudaEvent_t> run_ev; // graph sweeps: start/end of each run between ll / optimiser steps
     int cur = 0;
     int32_t* d_doc_len = nullptr;
     uint32_t* d_doc_order = nullptr;
@@ -667,6 +885,8 @@ struct tmt_handle {
         double* ll = nullptr;
         float* acum = nullptr;
         uint32_t* counter = nullptr;
+        float* wt = nullptr;
+        uint64_t cap_wt = 0;
     } inf;
     double* d_part_nom = nullptr;
     double* d_part_den = nullptr;
@@ -692,9 +912,16 @@ struct tmt_handle {
         return static_cast<T*>(p);
     }
 
+    void drop_graphs()
+    {
+        for (auto& g : graph_exec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
     void release()
     {
         if (device >= 0) cudaSetDevice(device);
+        drop_graphs();
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         bytes = 0;
@@ -709,6 +936,8 @@ struct tmt_handle {
         if (kev1) cudaEventDestroy(kev1);
         if (tev0) cudaEventDestroy(tev0);
         if (tev1) cudaEventDestroy(tev1);
+        for (cudaEvent_t e : gev) cudaEventDestroy(e);
+        for (cudaEvent_t e : run_ev) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -758,29 +987,36 @@ struct SweepShape {
     uint32_t rowi_smem, dnk_smem;
 };
 
-SweepShape sweep_shape(uint32_t K)
+SweepShape sweep_shape(uint32_t K, bool weighted)
 {
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
     SweepShape s{};
-    s.dnk_smem = K <= 16384;
+    s.dnk_smem = K <= (weighted ? 8192u : 16384u);
     s.rowi_smem = K <= 8192;
     const uint32_t per_warp = 4 * KP + (s.rowi_smem ? 4 * KP : 0);
-    const uint32_t fixed = s.dnk_smem ? 4 * KP : 0;
+    const uint32_t fixed = s.dnk_smem ? (weighted ? 8 : 4) * KP : 0;
     uint32_t w = (budget - fixed) / per_warp;
     s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
     s.smem = fixed + s.warps * per_warp;
     return s;
 }
 
-template <int CH, int MINB, bool PF>
+template <int CH, int MINB, bool PF, bool WT>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF>;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    auto kern = k_sweep_doc<CH, MINB, PF, WT>;
+    // attribute and occupancy once per kernel (the shape depends on K only),
+    // so a captured sweep makes no such call
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.warps * 32, sh.smem));
-    if (per_sm < 1) throw CudaError("sweep kernel does not fit on an SM");
+    for (const auto& e : h->occ)
+        if (e.first == (const void*)kern) per_sm = e.second;
+    if (per_sm == 0) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.warps * 32, sh.smem));
+        if (per_sm < 1) throw CudaError("sweep kernel does not fit on an SM");
+        h->occ.emplace_back((const void*)kern, per_sm);
+    }
     const uint64_t docs = a.pos_end - a.pos_begin;
     uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms, (docs + sh.warps - 1) / sh.warps);
     if (grid == 0) grid = 1;
@@ -790,29 +1026,49 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
 // topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM.
-template <int CH>
-void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
+template <int CH, bool WT>
+void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, int variant)
 {
     constexpr bool kPrefetch = CH <= 8;   // above, the prefetch registers spill
-    if (h->variant == 1) launch_sweep_t<CH, 3, false>(h, a, sh);
-    else launch_sweep_t<CH, 2, kPrefetch>(h, a, sh);
+    if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
+    else launch_sweep_t<CH, 2, kPrefetch, WT>(h, a, sh);
 }
 
-void launch_sweep(tmt_handle* h, const SweepArgs& a)
+template <bool WT>
+void launch_sweep_w(tmt_handle* h, const SweepArgs& b, const SweepShape& sh, uint32_t ch, int variant)
+{
+    if (ch <= 1) launch_sweep_ch<1, WT>(h, b, sh, variant);
+    else if (ch <= 2) launch_sweep_ch<2, WT>(h, b, sh, variant);
+    else if (ch <= 4) launch_sweep_ch<4, WT>(h, b, sh, variant);
+    else if (ch <= 8) launch_sweep_ch<8, WT>(h, b, sh, variant);
+    else if (ch <= 16) launch_sweep_ch<16, WT>(h, b, sh, variant);
+    else if (ch <= 32) launch_sweep_ch<32, WT>(h, b, sh, variant);
+    else launch_sweep_t<0, 3, false, WT>(h, b, sh);
+}
+
+void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
 {
     const uint32_t KP = round4(a.K);
     const uint32_t ch = (KP + 127) / 128;
-    const SweepShape sh = sweep_shape(a.K);
+    const bool wt = a.wt != nullptr;
+    const SweepShape sh = sweep_shape(a.K, wt);
     SweepArgs b = a;
     b.rowi_smem = sh.rowi_smem;
     b.dnk_smem = sh.dnk_smem;
-    if (ch <= 1) launch_sweep_ch<1>(h, b, sh);
-    else if (ch <= 2) launch_sweep_ch<2>(h, b, sh);
-    else if (ch <= 4) launch_sweep_ch<4>(h, b, sh);
-    else if (ch <= 8) launch_sweep_ch<8>(h, b, sh);
-    else if (ch <= 16) launch_sweep_ch<16>(h, b, sh);
-    else if (ch <= 32) launch_sweep_ch<32>(h, b, sh);
-    else launch_sweep_t<0, 3, false>(h, b, sh);
+    if (wt) launch_sweep_w<true>(h, b, sh, ch, variant);
+    else launch_sweep_w<false>(h, b, sh, ch, variant);
+}
+
+// The variant of group g: the one being tuned, else the group's fastest.
+int variant_of(const tmt_handle* h, uint32_t g)
+{
+    return h->tuned < 0 ? h->variant : h->group_variant[g];
+}
+
+// Tuning sweeps time each group's sweep kernel with its own event pair.
+void tune_mark(tmt_handle* h, uint32_t g, int end)
+{
+    if (h->tuned < 0) CK(cudaEventRecord(h->gev[2 * g + end], h->stream));
 }
 
 // In-place SUM over the ranks of a sharded corpus, ordered on the engine's stream.
@@ -843,6 +1099,12 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.K = h->cfg.K;
     a.V = h->cfg.V;
     a.c = (h->cfg.K + 31) / 32;
+    {
+        const uint32_t lanes = std::min<uint32_t>(32, (h->cfg.K + 3) / 4);
+        uint32_t st = 0;
+        while ((1u << st) < lanes) ++st;
+        a.scan_steps = st;
+    }
     a.eta = h->cfg.eta;
     a.veta = h->cfg.eta * (float)h->cfg.V;
     a.seed = h->cfg.seed;
@@ -882,8 +1144,10 @@ void do_sweep_sharded(tmt_handle* h)
         launch_check(h);
         if (h->group_bounds[g] < h->group_bounds[g + 1]) {
             CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+            tune_mark(h, g, 0);
             launch_sweep(h, sweep_args(h, h->d_nkw[0], h->d_nk[0], dnkw, dnk, h->group_bounds[g],
-                                       h->group_bounds[g + 1]));
+                                       h->group_bounds[g + 1]), variant_of(h, g));
+            tune_mark(h, g, 1);
         }
         exchange(h, h->d_delta, KV + K, TMT_I32);
         pending = true;
@@ -900,12 +1164,67 @@ void do_sweep_sharded(tmt_handle* h)
     h->sampler_used = TMT_SAMPLER_DENSE;
 }
 
+// A sweep with weighted counts: per group, fold the previous group's deltas
+// into the float state (n_k first, then n_kw fused with the word table of the
+// new state), then the group's documents with their deltas going to
+// d_dkw / d_dk; after the last group, a final fold.  The state is updated in
+// place (h->cur stays 0).
+void do_sweep_w(tmt_handle* h, bool capture)
+{
+    const uint32_t K = h->cfg.K, V = h->cfg.V;
+    const float veta = h->cfg.eta * (float)V;
+    float* nkw = reinterpret_cast<float*>(h->d_nkw[0]);
+    float* nk = reinterpret_cast<float*>(h->d_nk[0]);
+    const uint32_t smem_k = K <= 12288 ? K : 0;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
+    bool pending = false, recorded = false;
+    const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
+    for (uint32_t g = 0; g < G; ++g) {
+        if (h->group_bounds[g] == h->group_bounds[g + 1]) continue;
+        if (pending) {
+            k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
+            launch_check(h);
+        }
+        k_phi_fold_w<<<grid, 256, smem_k * 4, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta,
+                                                         h->d_phi, smem_k, pending ? 1 : 0);
+        launch_check(h);
+        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+        SweepArgs a = sweep_args(h, h->d_nkw[0], h->d_nk[0], nullptr, nullptr, h->group_bounds[g],
+                                 h->group_bounds[g + 1]);
+        a.wt = h->d_wt;
+        a.dkw = h->d_dkw;
+        a.dk = h->d_dk;
+        if (capture) a.iter_ptr = h->d_step;
+        if (!capture) {
+            if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
+            tune_mark(h, g, 0);
+        }
+        launch_sweep(h, a, variant_of(h, g));
+        if (!capture) tune_mark(h, g, 1);
+        pending = true;
+    }
+    if (pending) {
+        k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
+        launch_check(h);
+        k_phi_fold_w<<<grid, 256, 0, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta, nullptr, 0, 1);
+        launch_check(h);
+    }
+    if (!capture) {
+        CK(cudaEventRecord(h->kev1, h->stream));
+        if (!recorded) CK(cudaEventRecord(h->kev0, h->stream));
+    }
+    h->sampler_used = TMT_SAMPLER_DENSE;
+}
+
 // One sweep = one launch per document group (contiguous ranges of the
 // longest-first order holding equal shares of the tokens); before each, the
 // word table and the next-state copy are rebuilt from the current state.
-void do_sweep(tmt_handle* h)
+// capture: the launches are being recorded into a graph (no timing events;
+// the draws read the sweep counter from d_step).
+void do_sweep(tmt_handle* h, bool capture = false)
 {
     if (h->world > 1) return do_sweep_sharded(h);
+    if (h->weighted) return do_sweep_w(h, capture);
     const uint32_t K = h->cfg.K, V = h->cfg.V;
     const float veta = h->cfg.eta * (float)V;
     bool recorded = false;
@@ -919,14 +1238,62 @@ void do_sweep(tmt_handle* h)
                                                         veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k);
         launch_check(h);
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
-        const SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
-                                       h->group_bounds[g], h->group_bounds[g + 1]);
-        if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
-        launch_sweep(h, a);
+        SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
+                                 h->group_bounds[g], h->group_bounds[g + 1]);
+        if (capture) a.iter_ptr = h->d_step;
+        if (!capture) {
+            if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
+            tune_mark(h, g, 0);
+        }
+        launch_sweep(h, a, variant_of(h, g));
+        if (!capture) tune_mark(h, g, 1);
         h->cur = nxt;
     }
-    CK(cudaEventRecord(h->kev1, h->stream));
-    if (!recorded) CK(cudaEventRecord(h->kev0, h->stream));
+    if (!capture) {
+        CK(cudaEventRecord(h->kev1, h->stream));
+        if (!recorded) CK(cudaEventRecord(h->kev0, h->stream));
+    }
+    h->sampler_used = TMT_SAMPLER_DENSE;
+}
+
+// One sweep as a graph launch: the sweep's launches are captured once per
+// starting buffer parity (after the autotuner has fixed every group's
+// variant) and replayed; the last node advances the device sweep counter.
+void graph_sweep(tmt_handle* h)
+{
+    const int p = h->cur;
+    if (!h->graph_exec[p]) {
+        const int cur0 = h->cur;
+        const uint64_t l0 = h->launches;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            do_sweep(h, true);
+            k_next_step<<<1, 1, 0, h->stream>>>(h->d_step);
+            launch_check(h);
+        } catch (...) {
+            cudaStreamEndCapture(h->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            h->cur = cur0;
+            h->launches = l0;
+            throw;
+        }
+        CK(cudaStreamEndCapture(h->stream, &g));
+        h->graph_kernels = h->launches - l0;
+        h->launches = l0;
+        h->graph_flip = h->cur ^ cur0;
+        h->cur = cur0;
+        const cudaError_t e = cudaGraphInstantiate(&h->graph_exec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->graph_exec[p] = nullptr;
+            throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        }
+    }
+    CK(cudaGraphLaunch(h->graph_exec[p], h->stream));
+    h->launches += h->graph_kernels;
+    h->cur ^= h->graph_flip;
     h->sampler_used = TMT_SAMPLER_DENSE;
 }
 
@@ -937,8 +1304,13 @@ void do_optimize(tmt_handle* h)
     k_sum_alpha<<<1, 32, 0, h->stream>>>(h->d_alpha, K, h->d_asum);
     launch_check(h);
     for (int it = 0; it < 10; ++it) {
-        k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_alpha, h->d_doc_len, h->d_asum,
-                                                  h->d_part_nom, h->d_part_den);
+        if (h->weighted)
+            k_alpha_sums<<<grid, 256, 0, h->stream>>>(reinterpret_cast<const float*>(h->d_ndk), h->D, K, h->d_alpha,
+                                                      (const float*)h->d_doc_wlen, h->d_asum, h->d_part_nom,
+                                                      h->d_part_den);
+        else
+            k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_alpha, h->d_doc_len, h->d_asum,
+                                                      h->d_part_nom, h->d_part_den);
         launch_check(h);
         uint32_t nparts = h->n_apart;
         const double* nom = h->d_part_nom;
@@ -968,12 +1340,21 @@ void do_ll(tmt_handle* h, double* d_out)
     const double veta = (double)h->cfg.V * eta;
     k_ll_prep<<<1, 256, 0, h->stream>>>(h->d_alpha, K, h->d_lg_alpha, h->d_asum_ll);
     launch_check(h);
-    k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
-                                                        h->d_doc_len, h->d_asum_ll,
-                                                        h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
-                                                        h->d_partials);
-    launch_check(h);
-    k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out);
+    if (h->weighted) {
+        k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(
+            reinterpret_cast<const float*>(h->d_ndk), h->D, K, h->d_lg_alpha, h->d_alpha, (const float*)h->d_doc_wlen,
+            h->d_asum_ll, reinterpret_cast<const float*>(h->d_nkw[0]), h->cfg.V, eta, std::lgamma(eta), h->d_partials);
+        launch_check(h);
+        k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, reinterpret_cast<const float*>(h->d_nk[0]),
+                                             K, veta, d_out);
+    } else {
+        k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
+                                                            h->d_doc_len, h->d_asum_ll,
+                                                            h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
+                                                            h->d_partials);
+        launch_check(h);
+        k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out);
+    }
     launch_check(h);
     exchange(h, d_out, 1, TMT_F64);     // LLDocs over every rank's documents; LLRest is replicated
 }
@@ -1046,7 +1427,7 @@ void validate_config(const tmt_config& c)
 namespace {
 
 tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D, const uint16_t* z0,
-                       const tmt_shard* shard)
+                       const tmt_shard* shard, const float* weights = nullptr)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
@@ -1060,6 +1441,20 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         if (z0) {
             for (uint64_t i = 0; i < n_all; ++i)
                 if (wid[i] < V && z0[i] >= K) throw ArgError("z0 holds a topic id >= K");
+        }
+        if (weights) {
+            // the deltas are int64 in units of 2^-24: the weights of all tokens
+            // together stay below 2^38 so no sum can overflow
+            if (shard && shard->world > 1) throw ArgError("weighted counts on a corpus sharded across GPUs are not supported");
+            double total = 0;
+            for (uint64_t i = 0; i < n_all; ++i) {
+                if (wid[i] >= V) continue;
+                const float w = weights[i];
+                if (!(w >= 0.f) || !(w <= 65536.f))
+                    throw ArgError("token weight " + std::to_string(i) + " is negative, too large or not finite");
+                total += (double)w;
+            }
+            if (total >= 274877906944.0) throw ArgError("the token weights sum to 2^38 or more");
         }
         h->release();
         h->uploaded = false;
@@ -1103,6 +1498,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             h->allreduce = nullptr;
             h->ar_user = nullptr;
         }
+        h->weighted = weights != nullptr;
         h->tok_offset = plan.tok_offset;
         h->group_bounds = plan.bounds;
         h->gbounds = plan.gbounds;
@@ -1120,6 +1516,16 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             h->d_nkw[1] = h->d_delta;
             h->d_nk[1] = h->d_delta + (uint64_t)K * V;
             h->d_alpha_fold = h->dalloc<double>((uint64_t)K + 1);
+        } else if (h->weighted) {
+            // the float state is updated in place; the deltas are int64
+            h->d_delta = nullptr;
+            h->d_alpha_fold = nullptr;
+            h->d_nkw[1] = nullptr;
+            h->d_nk[1] = nullptr;
+            h->d_wt = h->dalloc<float>(n_all);
+            h->d_dkw = h->dalloc<long long>((uint64_t)K * V);
+            h->d_dk = h->dalloc<long long>(K);
+            h->d_doc_wlen = h->dalloc<float>(D);
         } else {
             h->d_delta = nullptr;
             h->d_alpha_fold = nullptr;
@@ -1128,10 +1534,20 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         }
         h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
         {
+            // the first n_variants sweeps run eagerly, one variant each, and
+            // every group keeps its fastest
+            const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
             h->n_variants = round4(K) <= 4096 ? 2 : 1;
             h->variant = 0;
-            h->tuned = h->n_variants > 1 ? -1 : 0;
-            h->variant_ms.clear();
+            h->tuned = -1;
+            h->group_variant.assign(G, 0);
+            h->group_ms.assign(G, {});
+            while (h->gev.size() < 2 * (size_t)G) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                h->gev.push_back(e);
+            }
+            h->d_step = h->dalloc<uint32_t>(1);
         }
         h->d_doc_len = h->dalloc<int32_t>(D);
         h->d_doc_order = h->dalloc<uint32_t>(D);
@@ -1172,7 +1588,24 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->tok_offset, h->d_z);
             launch_check(h);
         }
-        if (D) {
+        if (D && h->weighted) {
+            if (n_all) CK(cudaMemcpyAsync(h->d_wt, weights, n_all * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(h->d_dkw, 0, (uint64_t)K * V * sizeof(long long), st));
+            CK(cudaMemsetAsync(h->d_dk, 0, K * sizeof(long long), st));
+            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D + 127) / 128);
+            k_counts_w<<<grid, 128, 0, st>>>(h->d_doc_off, h->d_words, h->d_z, h->d_wt, D, K, V,
+                                             reinterpret_cast<float*>(h->d_ndk), h->d_dkw, h->d_dk, h->d_doc_wlen);
+            launch_check(h);
+            k_nk_fold_w<<<1, 1024, 0, st>>>(reinterpret_cast<float*>(h->d_nk[0]), h->d_dk, K);
+            launch_check(h);
+            const uint32_t g2 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
+            k_phi_fold_w<<<g2, 256, 0, st>>>(reinterpret_cast<float*>(h->d_nkw[0]), h->d_dkw,
+                                             reinterpret_cast<const float*>(h->d_nk[0]), V, K, round4(K), h->cfg.eta,
+                                             h->cfg.eta * (float)V, nullptr, 0, 1);
+            launch_check(h);
+            // the token counts per document as well (the shard planner's facts)
+            CK(cudaMemcpyAsync(h->d_doc_len, len.data(), D * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        } else if (D) {
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D * 32 + 255) / 256);
             k_counts<<<grid, 256, 0, st>>>(h->d_doc_off, h->d_words, h->d_z, D, K, V, h->d_ndk, h->d_nkw[0],
                                            h->d_nk[0], h->d_doc_len);
@@ -1242,6 +1675,17 @@ tmt_status tmt_upload_corpus(tmt_handle* h, const uint32_t* wid, const uint64_t*
     return upload_impl(h, wid, doc_off, D, z0, nullptr);
 }
 
+tmt_status tmt_upload_corpus_weighted(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                                      const uint16_t* z0, const float* weights)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    if (!weights) {
+        h->err = "weights is NULL";
+        return TMT_ERR_INVALID_ARGUMENT;
+    }
+    return upload_impl(h, wid, doc_off, D, z0, nullptr, weights);
+}
+
 tmt_status tmt_upload_shard(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
                             const uint16_t* z0, const tmt_shard* shard)
 {
@@ -1285,39 +1729,85 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
         uint32_t pt = 0;
         h->sweep_kernel_ms = 0;
         h->sweeps_timed = 0;
+        const bool use_graphs = h->graphs && h->world == 1;
+        uint32_t runs = 0;              // runs of graph sweeps between ll / optimiser steps
+        bool in_run = false;
+        auto run_event = [&](uint32_t idx) {
+            while (h->run_ev.size() <= idx) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                h->run_ev.push_back(e);
+            }
+            return h->run_ev[idx];
+        };
+        auto end_run = [&] {
+            if (!in_run) return;
+            CK(cudaEventRecord(run_event(2 * runs + 1), h->stream));
+            ++runs;
+            in_run = false;
+        };
         CK(cudaEventRecord(h->tev0, h->stream));
         for (uint32_t i = 0; i < iters; ++i) {
-            CK(cudaEventRecord(h->ev0, h->stream));
-            do_sweep(h);
-            CK(cudaEventRecord(h->ev1, h->stream));
-            // the events of this sweep's kernel are complete before the next
-            // sweep records them again: read them now
-            {
+            if (use_graphs && h->tuned >= 0) {
+                if (!in_run) {
+                    k_set_step<<<1, 1, 0, h->stream>>>(h->d_step, (uint32_t)h->global_step);
+                    launch_check(h);
+                    CK(cudaEventRecord(run_event(2 * runs), h->stream));
+                    in_run = true;
+                }
+                CK(cudaEventRecord(h->ev0, h->stream));
+                graph_sweep(h);
+                CK(cudaEventRecord(h->ev1, h->stream));
+                ++h->sweeps_timed;
+            } else {
+                end_run();
+                CK(cudaEventRecord(h->ev0, h->stream));
+                do_sweep(h);
+                CK(cudaEventRecord(h->ev1, h->stream));
+                // the events of this sweep are complete before the next
+                // sweep records them again: read them now
                 CK(cudaEventSynchronize(h->kev1));
                 float ms = 0.f;
                 CK(cudaEventElapsedTime(&ms, h->kev0, h->kev1));
                 h->sweep_kernel_ms += ms;
                 ++h->sweeps_timed;
                 if (h->tuned < 0) {
-                    h->variant_ms.push_back(ms);
-                    if ((int)h->variant_ms.size() >= h->n_variants) {
-                        h->tuned = (int)(std::min_element(h->variant_ms.begin(), h->variant_ms.end()) -
-                                         h->variant_ms.begin());
-                        h->variant = h->tuned;
-                    } else {
-                        h->variant = (int)h->variant_ms.size();
+                    const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
+                    for (uint32_t g = 0; g < G; ++g) {
+                        if (h->group_bounds[g] == h->group_bounds[g + 1]) continue;
+                        float gm = 0.f;
+                        CK(cudaEventElapsedTime(&gm, h->gev[2 * g], h->gev[2 * g + 1]));
+                        h->group_ms[g].push_back(gm);
+                    }
+                    if (++h->variant >= h->n_variants) {
+                        for (uint32_t g = 0; g < G; ++g) {
+                            const auto& v = h->group_ms[g];
+                            h->group_variant[g] =
+                                v.empty() ? 0 : (int)(std::min_element(v.begin(), v.end()) - v.begin());
+                        }
+                        h->variant = 0;
+                        h->tuned = 0;
+                        h->drop_graphs();
                     }
                 }
             }
             const uint64_t gs = h->global_step;
-            if (gs >= h->cfg.burn_in && h->cfg.optim_interval && (gs + 1) % h->cfg.optim_interval == 0)
-                do_optimize(h);
+            const bool opt = gs >= h->cfg.burn_in && h->cfg.optim_interval && (gs + 1) % h->cfg.optim_interval == 0;
+            const bool llp = npts && (i + 1) % ll_every == 0 && pt < npts;
+            if (opt || llp) end_run();
+            if (opt) do_optimize(h);
             ++h->global_step;
-            if (npts && (i + 1) % ll_every == 0 && pt < npts) do_ll(h, h->d_ll + 2 * pt++);
+            if (llp) do_ll(h, h->d_ll + 2 * pt++);
         }
+        end_run();
         CK(cudaEventRecord(h->tev1, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+        for (uint32_t r = 0; r < runs; ++r) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->run_ev[2 * r], h->run_ev[2 * r + 1]));
+            h->sweep_kernel_ms += ms;
+        }
         {
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, h->tev0, h->tev1));
@@ -1352,6 +1842,8 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("no corpus uploaded");
+        if (h->weighted && (n_kw || n_k))
+            throw StateError("the counts are weighted (float): read them with tmt_download_counts_f32");
         const uint32_t K = h->cfg.K, V = h->cfg.V;
         if (z && h->N_all) CK(cudaMemcpyAsync(z, h->d_z, h->N_all * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream));
         if (n_kw) CK(cudaMemcpyAsync(n_kw, h->d_nkw[h->cur], (uint64_t)K * V * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
@@ -1362,12 +1854,29 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
     });
 }
 
+tmt_status tmt_download_counts_f32(tmt_handle* h, float* n_dk, float* n_kw, float* n_k, float* doc_wlen)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("no corpus uploaded");
+        if (!h->weighted) throw StateError("the counts are integers: read them with tmt_download_state");
+        const uint64_t K = h->cfg.K, V = h->cfg.V;
+        if (n_dk && h->D) CK(cudaMemcpyAsync(n_dk, h->d_ndk, h->D * K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        if (n_kw) CK(cudaMemcpyAsync(n_kw, h->d_nkw[0], K * V * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        if (n_k) CK(cudaMemcpyAsync(n_k, h->d_nk[0], K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        if (doc_wlen && h->D)
+            CK(cudaMemcpyAsync(doc_wlen, h->d_doc_wlen, h->D * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
 tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("no corpus uploaded");
         if (!n_dk) throw ArgError("n_dk is NULL");
+        if (h->weighted) throw StateError("the counts are weighted (float): read them with tmt_download_counts_f32");
         if (h->D)
             CK(cudaMemcpyAsync(n_dk, h->d_ndk, h->D * (uint64_t)h->cfg.K * sizeof(int32_t),
                                cudaMemcpyDeviceToHost, h->stream));
@@ -1381,9 +1890,28 @@ tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("set_counts before the corpus was uploaded");
         if (!n_kw || !n_k) throw ArgError("n_kw / n_k is NULL");
+        if (h->weighted) throw StateError("set_counts takes integer counts; this corpus has weighted counts");
         const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
         if (kv) CK(cudaMemcpyAsync(h->d_nkw[h->cur], n_kw, kv * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_nk[h->cur], n_k, h->cfg.K * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_set_counts_f32(tmt_handle* h, const float* n_kw, const float* n_k)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_counts before the corpus was uploaded");
+        if (!n_kw || !n_k) throw ArgError("n_kw / n_k is NULL");
+        if (!h->weighted) throw StateError("set_counts_f32 takes weighted counts; this corpus has integer counts");
+        const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
+        for (uint64_t i = 0; i < kv; ++i)
+            if (!(n_kw[i] >= 0.f) || !std::isfinite(n_kw[i])) throw ArgError("n_kw holds a negative or non-finite value");
+        for (uint32_t k = 0; k < h->cfg.K; ++k)
+            if (!(n_k[k] >= 0.f) || !std::isfinite(n_k[k])) throw ArgError("n_k holds a negative or non-finite value");
+        if (kv) CK(cudaMemcpyAsync(h->d_nkw[0], n_kw, kv * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_nk[0], n_k, h->cfg.K * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     });
 }
@@ -1412,6 +1940,13 @@ tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     h->cfg.seed = seed;
+    return guarded(h, [&] { h->drop_graphs(); });   // the seed is an argument of the captured launches
+}
+
+tmt_status tmt_set_graphs(tmt_handle* h, int32_t enable)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    h->graphs = enable != 0;
     return TMT_OK;
 }
 
@@ -1445,13 +1980,22 @@ tmt_status tmt_get_info(const tmt_handle* h, tmt_info* out)
     return TMT_OK;
 }
 
-tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
-                           uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll)
+} // extern "C"
+
+namespace {
+
+// tmt_infer_batch / tmt_infer_batch_weighted (weights == NULL: integer counts)
+tmt_status infer_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D, const float* weights,
+                      uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("infer() before the model has a state");
         if (!doc_off) throw ArgError("doc_off is NULL");
+        if (h->weighted && !weights)
+            throw StateError("the model has weighted counts: infer with tmt_infer_batch_weighted");
+        if (!h->weighted && weights)
+            throw StateError("the model has integer counts: infer with tmt_infer_batch");
         const uint64_t n_all = doc_off[D];
         if (n_all && !wid) throw ArgError("wid is NULL");
         for (uint64_t d = 0; d < D; ++d)
@@ -1460,10 +2004,33 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         if (D >= 0xFFFFFFFFull) throw ArgError("too many documents");
         if (D == 0) return;
         const uint32_t K = h->cfg.K;
-        // documents sorted by word id, as prepareDoc does (LDAModel.hpp:716-722)
+        // documents sorted by word id, as prepareDoc does (LDAModel.hpp:716-722),
+        // the weights following their tokens
         std::vector<uint32_t> sorted(wid, wid + n_all);
-        for (uint64_t d = 0; d < D; ++d)
-            std::stable_sort(sorted.begin() + doc_off[d], sorted.begin() + doc_off[d + 1]);
+        std::vector<float> wsorted;
+        if (weights) {
+            std::vector<std::pair<uint32_t, float>> pw(n_all);
+            for (uint64_t i = 0; i < n_all; ++i) pw[i] = { wid[i], weights[i] };
+            for (uint64_t d = 0; d < D; ++d)
+                std::stable_sort(pw.begin() + doc_off[d], pw.begin() + doc_off[d + 1],
+                                 [](const auto& x, const auto& y) { return x.first < y.first; });
+            wsorted.resize(n_all);
+            for (uint64_t i = 0; i < n_all; ++i) {
+                sorted[i] = pw[i].first;
+                wsorted[i] = pw[i].second;
+                if (sorted[i] >= h->cfg.V) continue;
+                if (!(wsorted[i] >= 0.f) || !(wsorted[i] <= 65536.f))
+                    throw ArgError("token weight " + std::to_string(i) + " is negative, too large or not finite");
+            }
+            for (uint64_t d = 0; d < D; ++d)
+                for (uint64_t i = doc_off[d] + 1; i < doc_off[d + 1]; ++i)
+                    if (sorted[i] == sorted[i - 1] && sorted[i] < h->cfg.V && wsorted[i] != wsorted[i - 1])
+                        throw ArgError("the tokens of one word in document " + std::to_string(d) +
+                                       " carry different weights");
+        } else {
+            for (uint64_t d = 0; d < D; ++d)
+                std::stable_sort(sorted.begin() + doc_off[d], sorted.begin() + doc_off[d + 1]);
+        }
         auto& B = h->inf;
         if (D > B.cap_docs) {
             B.doc_off = h->dalloc<uint64_t>(D + 1);
@@ -1480,6 +2047,10 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
             B.z = h->dalloc<uint16_t>(n_all);
             B.cap_tokens = n_all;
         }
+        if (weights && n_all > B.cap_wt) {
+            B.wt = h->dalloc<float>(n_all);
+            B.cap_wt = n_all;
+        }
         if (!B.acum) {
             B.acum = h->dalloc<float>(K);
             B.counter = h->dalloc<uint32_t>(1);
@@ -1494,6 +2065,8 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         cudaStream_t st = h->stream;
         CK(cudaMemcpyAsync(B.doc_off, doc_off, (D + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         if (n_all) CK(cudaMemcpyAsync(B.words, sorted.data(), n_all * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        if (weights && n_all)
+            CK(cudaMemcpyAsync(B.wt, wsorted.data(), n_all * sizeof(float), cudaMemcpyHostToDevice, st));
         if (doc_keys) CK(cudaMemcpyAsync(B.keys, doc_keys, D * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(B.acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(B.counter, 0, sizeof(uint32_t), st));
@@ -1527,12 +2100,34 @@ tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* d
         a.work = nullptr;
         a.n_work = (uint32_t)D;
         a.counter = B.counter;
+        a.wt = weights ? B.wt : nullptr;
         launch_infer(a, h->num_sms, h->stream);
         ++h->launches;
         if (theta) CK(cudaMemcpyAsync(theta, B.theta, D * (uint64_t)K * sizeof(float), cudaMemcpyDeviceToHost, st));
         if (ll) CK(cudaMemcpyAsync(ll, B.ll, D * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
     });
+}
+
+} // namespace
+
+extern "C" {
+
+tmt_status tmt_infer_batch(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                           uint32_t iters, uint64_t seed, const uint64_t* doc_keys, float* theta, double* ll)
+{
+    return infer_impl(h, wid, doc_off, D, nullptr, iters, seed, doc_keys, theta, ll);
+}
+
+tmt_status tmt_infer_batch_weighted(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_off, uint64_t D,
+                                    const float* weights, uint32_t iters, uint64_t seed, const uint64_t* doc_keys,
+                                    float* theta, double* ll)
+{
+    if (h && !weights) {
+        h->err = "weights is NULL";
+        return TMT_ERR_INVALID_ARGUMENT;
+    }
+    return infer_impl(h, wid, doc_off, D, weights, iters, seed, doc_keys, theta, ll);
 }
 
 /* Allocation-free FP64 log-likelihood over caller-owned device counts.

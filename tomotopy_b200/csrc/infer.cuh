@@ -19,6 +19,7 @@
 #pragma once
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include "common.cuh"
 #include "philox.cuh"
 
@@ -51,18 +52,33 @@ struct InferArgs {
     const uint32_t* work;        // slots advanced by this launch; NULL: 0 .. n_work-1
     uint32_t n_work;
     uint32_t* counter;           // zeroed before the launch
+    // weighted counts (TermWeight IDF / PMI): nkw, nk and ndk hold floats;
+    // wt[token] is the token's weight, the same for every token of one word
+    // within a document (IDF: the word's weight; PMI: a function of the word's
+    // count in the document)
+    const float* wt;
 };
 
-template <int CH>
+// WT: weighted counts.  The document's counts n_dk are float sums of weights
+// (a removal clamps at 0, updateCnt<true>); B_k = (n_kw[k,v] + own[k] * w) + eta
+// with w the weight of the current word's tokens; R_k = 1 / ((n_k[k] + n_dk[k])
+// + V*eta); the document's length is its weight sum.  n_dk starts from z0 in
+// token order (initializeDocState's addWordTo sequence).
+template <int CH, bool WT>
 __global__ void __launch_bounds__(256)
 k_infer_slots(InferArgs a)
 {
+    using CT = typename std::conditional<WT, float, int>::type;
+    using G4 = typename std::conditional<WT, float4, int4>::type;
     constexpr int CHR = CH > 0 ? CH : 1;
     extern __shared__ __align__(16) int smem[];
     const int K = (int)a.K;
     const int KP = (int)round4(a.K);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int* rowi = smem + warp * 4 * KP;
+    CT* rowi = reinterpret_cast<CT*>(smem + warp * 4 * KP);
+    const CT* nkw = reinterpret_cast<const CT*>(a.nkw);
+    const CT* nkv = reinterpret_cast<const CT*>(a.nk);
+    CT* ndk_s = reinterpret_cast<CT*>(a.ndk);
     float* rowf = reinterpret_cast<float*>(rowi + KP);
     float* rr = rowf + KP;
     int* own = reinterpret_cast<int*>(rr + KP);
@@ -85,6 +101,7 @@ k_infer_slots(InferArgs a)
         const uint32_t itT = a.it_total ? a.it_total[sl] : a.u_total;
         for (int k = lane; k < KP; k += 32) own[k] = 0;
         int nvalid = 0;
+        float wsum = 0.f;                    // WT: the document's weight sum, in token order
         if (it0 == 0) {
             // z0 ~ Discrete(alpha), added to the document's counts
             for (int k = lane; k < KP; k += 32) rowi[k] = 0;
@@ -101,24 +118,43 @@ k_infer_slots(InferArgs a)
                         if (r < a.acum[mid]) hi = mid; else lo = mid + 1;
                     }
                     zz = (uint16_t)lo;
-                    atomicAdd(&rowi[lo], 1);
+                    if (!WT) atomicAdd(reinterpret_cast<int*>(rowi) + lo, 1);
                     ++nvalid;
                 }
                 a.z[b + j] = zz;
             }
+            if (WT) {
+                __syncwarp();
+                if (lane == 0)
+                    for (uint32_t j = 0; j < L; ++j)
+                        if (a.words[b + j] < a.V) {
+                            const float wj = a.wt[b + j];
+                            rowi[a.z[b + j]] = __fadd_rn(rowi[a.z[b + j]], wj);
+                            wsum = __fadd_rn(wsum, wj);
+                        }
+            }
         } else {
-            for (int k = lane; k < KP; k += 32) rowi[k] = k < K ? a.ndk[(uint64_t)sl * K + k] : 0;
+            for (int k = lane; k < KP; k += 32) rowi[k] = k < K ? ndk_s[(uint64_t)sl * K + k] : CT(0);
             for (uint32_t j = lane; j < L; j += 32) nvalid += a.words[b + j] < a.V;
+            if (WT && lane == 0)
+                for (uint32_t j = 0; j < L; ++j)
+                    if (a.words[b + j] < a.V) wsum = __fadd_rn(wsum, a.wt[b + j]);
         }
 #pragma unroll
         for (int o = 16; o; o >>= 1) nvalid += __shfl_xor_sync(FULL, nvalid, o);
+        if (WT) wsum = __shfl_sync(FULL, wsum, 0);
         __syncwarp();
+        // R_k's denominator: (float)(n_k + n_dk) for integer counts, (n_k + n_dk) in float for weights
+        auto rden = [&](int k, CT n) -> float {
+            if constexpr (WT) return __fadd_rn(__fadd_rn(__ldg(nkv + k), n), veta);
+            else return __fadd_rn((float)(__ldg(nkv + k) + n), veta);
+        };
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f, g = 0.f;
             if (k < K) {
-                const int n = rowi[k];
+                const CT n = rowi[k];
                 f = __fadd_rn((float)n, __ldg(a.alpha + k));
-                g = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + k) + n), veta));
+                g = __frcp_rn(rden(k, n));
             }
             rowf[k] = f;
             rr[k] = g;
@@ -140,16 +176,16 @@ k_infer_slots(InferArgs a)
         // loaded once per run of a word.  (Loading the next token's column
         // during the current draw measured slower on B200: the extra registers
         // cost more occupancy than the hidden latency gained.)
-        int4 gv[CHR];
+        G4 gv[CHR];
         uint32_t v_have = 0xFFFFFFFFu;
-        auto load_col = [&](uint32_t v, int4 (&g)[CHR]) {
-            const int32_t* col = a.nkw + (uint64_t)v * K;
+        auto load_col = [&](uint32_t v, G4 (&g)[CHR]) {
+            const CT* col = nkw + (uint64_t)v * K;
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj) {
                 if (jj < nch) {
                     const int k0 = 128 * jj + 4 * lane;
                     if (vecg) {
-                        g[jj] = __ldg(reinterpret_cast<const int4*>(col + k0));
+                        g[jj] = __ldg(reinterpret_cast<const G4*>(col + k0));
                     } else {
                         g[jj].x = __ldg(col + k0);
                         g[jj].y = k0 + 1 < K ? __ldg(col + k0 + 1) : 0;
@@ -165,10 +201,11 @@ k_infer_slots(InferArgs a)
                 const uint32_t jl = base + lane;
                 uint32_t my_w = 0xFFFFFFFFu, my_z = 0;
                 bool my_same = false;            // my token's word equals the next token's
-                float my_u = 0.f;
+                float my_u = 0.f, my_wt = 1.f;
                 if (jl < L) {
                     my_w = a.words[b + jl];
                     my_z = a.z[b + jl];
+                    if (WT) my_wt = a.wt[b + jl];
                     my_same = jl + 1 < L && a.words[b + jl + 1] == my_w;
                     my_u = tmt::u01(tmt::philox_u32(jl, it, klo, khi, a.key));
                 }
@@ -179,6 +216,7 @@ k_infer_slots(InferArgs a)
                     const uint32_t v = __shfl_sync(FULL, my_w, q2);
                     const int zo = (int)__shfl_sync(FULL, my_z, q2);
                     const float u = __shfl_sync(FULL, my_u, q2);
+                    const float wt = WT ? __shfl_sync(FULL, my_wt, q2) : 1.f;
                     if (v >= a.V) continue;
                     const bool in_run = j < run_e;
                     if (!in_run && ((same_m >> q2) & 1u)) {
@@ -189,14 +227,25 @@ k_infer_slots(InferArgs a)
                         __syncwarp();
                     }
                     const bool multi = j < run_e;
-                    const int32_t* gcol = a.nkw + (uint64_t)v * K;
+                    const CT* gcol = nkw + (uint64_t)v * K;
                     if (CH > 0 && v != v_have) { load_col(v, gv); v_have = v; }
+                    // B_k before the multiplication by R_k
+                    auto bk = [&](CT g, int o) -> float {
+                        if constexpr (WT) return __fadd_rn(__fadd_rn(g, __fmul_rn((float)o, wt)), eta);
+                        else return __fadd_rn((float)(g + o), eta);
+                    };
                     if (lane == 0) {
                         if (multi) own[zo] -= 1;
-                        const int n = rowi[zo] - 1;
+                        CT n;
+                        if constexpr (WT) {
+                            n = __fsub_rn(rowi[zo], wt);
+                            n = n > 0.f ? n : 0.f;
+                        } else {
+                            n = rowi[zo] - 1;
+                        }
                         rowi[zo] = n;
                         rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
-                        rr[zo] = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + zo) + n), veta));
+                        rr[zo] = __frcp_rn(rden(zo, n));
                     }
                     __syncwarp();
                     // pass 1: fma chain over this lane's topics
@@ -208,23 +257,19 @@ k_infer_slots(InferArgs a)
                                 const int k0 = 128 * jj + 4 * lane;
                                 const float4 A4 = *reinterpret_cast<const float4*>(rowf + k0);
                                 const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
-                                int g0 = gv[jj].x, g1 = gv[jj].y, g2 = gv[jj].z, g3 = gv[jj].w;
-                                if (multi) {
-                                    const int4 O4 = *reinterpret_cast<const int4*>(own + k0);
-                                    g0 += O4.x; g1 += O4.y; g2 += O4.z; g3 += O4.w;
-                                }
-                                s = __fmaf_rn(A4.x, __fmul_rn(__fadd_rn((float)g0, eta), R4.x), s);
-                                s = __fmaf_rn(A4.y, __fmul_rn(__fadd_rn((float)g1, eta), R4.y), s);
-                                s = __fmaf_rn(A4.z, __fmul_rn(__fadd_rn((float)g2, eta), R4.z), s);
-                                s = __fmaf_rn(A4.w, __fmul_rn(__fadd_rn((float)g3, eta), R4.w), s);
+                                int4 O4 = make_int4(0, 0, 0, 0);
+                                if (multi) O4 = *reinterpret_cast<const int4*>(own + k0);
+                                s = __fmaf_rn(A4.x, __fmul_rn(bk(gv[jj].x, O4.x), R4.x), s);
+                                s = __fmaf_rn(A4.y, __fmul_rn(bk(gv[jj].y, O4.y), R4.y), s);
+                                s = __fmaf_rn(A4.z, __fmul_rn(bk(gv[jj].z, O4.z), R4.z), s);
+                                s = __fmaf_rn(A4.w, __fmul_rn(bk(gv[jj].w, O4.w), R4.w), s);
                             }
                         }
                     } else {
                         for (int jj = 0; jj < nch; ++jj)
                             for (int i = 0; i < 4; ++i) {
                                 const int k = 128 * jj + 4 * lane + i;
-                                if (k < K)
-                                    s = __fmaf_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + own[k]), eta), rr[k]), s);
+                                if (k < K) s = __fmaf_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), own[k]), rr[k]), s);
                             }
                     }
                     const float x = hs_scan32(s, lane);
@@ -247,7 +292,7 @@ k_infer_slots(InferArgs a)
                             const int k = 128 * (t >> 2) + 4 * h + (t & 3);
                             float x2 = 0.f;
                             if (t < nh)
-                                x2 = __fmul_rn(rowf[k], __fmul_rn(__fadd_rn((float)(__ldg(gcol + k) + (multi ? own[k] : 0)), eta), rr[k]));
+                                x2 = __fmul_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), multi ? own[k] : 0), rr[k]));
                             x2 = hs_scan32(x2, lane);
                             const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
                             if (mb) { found = mm + __ffs(mb) - 1; break; }
@@ -258,10 +303,12 @@ k_infer_slots(InferArgs a)
                     __syncwarp();
                     if (lane == 0) {
                         if (multi) own[znew] += 1;
-                        const int n = rowi[znew] + 1;
+                        CT n;
+                        if constexpr (WT) n = __fadd_rn(rowi[znew], wt);
+                        else n = rowi[znew] + 1;
                         rowi[znew] = n;
                         rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
-                        rr[znew] = __frcp_rn(__fadd_rn((float)(__ldg(a.nk + znew) + n), veta));
+                        rr[znew] = __frcp_rn(rden(znew, n));
                         a.z[b + j] = (uint16_t)znew;
                     }
                     __syncwarp();
@@ -274,18 +321,19 @@ k_infer_slots(InferArgs a)
             }
         }
         if (it1 < itT) {            // keep the document's counts for the next launch
-            for (int k = lane; k < K; k += 32) a.ndk[(uint64_t)sl * K + k] = rowi[k];
+            for (int k = lane; k < K; k += 32) ndk_s[(uint64_t)sl * K + k] = rowi[k];
             __syncwarp();
             continue;
         }
         // finished: theta, FP64 ll over the touched cells
         double acc = 0;
-        const float denom = __fadd_rn((float)nvalid, a.asum_f);
+        const float dlen = WT ? wsum : (float)nvalid;
+        const float denom = __fadd_rn(dlen, a.asum_f);
         for (int k = lane; k < K; k += 32) {
-            const int n = rowi[k];
+            const CT n = rowi[k];
             if (a.theta) a.theta[(uint64_t)sl * K + k] = __fdiv_rn(__fadd_rn((float)n, __ldg(a.alpha + k)), denom);
-            if (n) {
-                const double gk = (double)__ldg(a.nk + k);
+            if (n != CT(0)) {
+                const double gk = (double)__ldg(nkv + k);
                 acc += lgamma(gk + a.veta_d) - lgamma(gk + (double)n + a.veta_d);
                 const double al = (double)__ldg(a.alpha + k);
                 acc += lgamma((double)n + al) - lgamma(al);
@@ -305,12 +353,16 @@ k_infer_slots(InferArgs a)
             if (v < a.V) {
                 for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
                 __syncwarp();
+                const float wr = WT ? a.wt[b + rb] : 1.f;    // the run's weight
                 for (uint32_t j = rb + lane; j < re; j += 32) {
                     const int k = a.z[b + j];
                     const int c = atomicExch(&own[k], 0);
                     if (c) {
-                        const int gk = __ldg(a.nkw + (uint64_t)v * K + k);
-                        acc += lgamma((double)(gk + c) + (double)a.eta) - (gk ? lgamma((double)gk + (double)a.eta) : a.lg_eta);
+                        const CT gk = __ldg(nkw + (uint64_t)v * K + k);
+                        double after;
+                        if constexpr (WT) after = lgamma(((double)gk + (double)__fmul_rn((float)c, wr)) + (double)a.eta);
+                        else after = lgamma((double)(gk + c) + (double)a.eta);
+                        acc += after - (gk != CT(0) ? lgamma((double)gk + (double)a.eta) : a.lg_eta);
                     }
                 }
                 __syncwarp();
@@ -318,7 +370,7 @@ k_infer_slots(InferArgs a)
             rb = re;
         }
         acc = warp_sum(acc);
-        if (lane == 0 && a.ll) a.ll[sl] = acc - (lgamma((double)nvalid + a.asum_d) - a.lg_asum);
+        if (lane == 0 && a.ll) a.ll[sl] = acc - (lgamma((double)dlen + a.asum_d) - a.lg_asum);
         __syncwarp();
     }
 }
@@ -330,10 +382,10 @@ inline uint32_t infer_warps(uint32_t K)
     return std::min(8u, (200u * 1024u) / per_warp);
 }
 
-template <int CH>
+template <int CH, bool WT>
 inline void launch_infer_t(const InferArgs& a, uint32_t warps, int num_sms, cudaStream_t st)
 {
-    auto kern = k_infer_slots<CH>;
+    auto kern = k_infer_slots<CH, WT>;
     const uint32_t smem = warps * 16 * round4(a.K);
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -345,19 +397,27 @@ inline void launch_infer_t(const InferArgs& a, uint32_t warps, int num_sms, cuda
     CK(cudaGetLastError());
 }
 
-// One launch of the slot kernel for this K (the counter must be zeroed first).
+template <bool WT>
+inline void launch_infer_w(const InferArgs& a, uint32_t warps, uint32_t ch, int num_sms, cudaStream_t st)
+{
+    if (ch <= 1) launch_infer_t<1, WT>(a, warps, num_sms, st);
+    else if (ch <= 2) launch_infer_t<2, WT>(a, warps, num_sms, st);
+    else if (ch <= 4) launch_infer_t<4, WT>(a, warps, num_sms, st);
+    else if (ch <= 8) launch_infer_t<8, WT>(a, warps, num_sms, st);
+    else if (ch <= 16) launch_infer_t<16, WT>(a, warps, num_sms, st);
+    else if (ch <= 32) launch_infer_t<32, WT>(a, warps, num_sms, st);
+    else launch_infer_t<0, WT>(a, warps, num_sms, st);
+}
+
+// One launch of the slot kernel for this K (the counter must be zeroed first);
+// a.wt != NULL: weighted counts.
 inline void launch_infer(const InferArgs& a, int num_sms, cudaStream_t st)
 {
     const uint32_t warps = infer_warps(a.K);
     if (warps == 0) throw ArgError("K too large for on-chip inference state");
     const uint32_t ch = (round4(a.K) + 127) / 128;
-    if (ch <= 1) launch_infer_t<1>(a, warps, num_sms, st);
-    else if (ch <= 2) launch_infer_t<2>(a, warps, num_sms, st);
-    else if (ch <= 4) launch_infer_t<4>(a, warps, num_sms, st);
-    else if (ch <= 8) launch_infer_t<8>(a, warps, num_sms, st);
-    else if (ch <= 16) launch_infer_t<16>(a, warps, num_sms, st);
-    else if (ch <= 32) launch_infer_t<32>(a, warps, num_sms, st);
-    else launch_infer_t<0>(a, warps, num_sms, st);
+    if (a.wt) launch_infer_w<true>(a, warps, ch, num_sms, st);
+    else launch_infer_w<false>(a, warps, ch, num_sms, st);
 }
 
 } // namespace tmtk

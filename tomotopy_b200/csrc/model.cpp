@@ -151,6 +151,7 @@ struct Doc {
     std::vector<uint32_t> words;     // dictionary ids; after prepare: sorted by id
     std::vector<uint32_t> wOrder;    // wOrder[original position] = sorted position (after prepare)
     std::vector<uint16_t> Zs;        // sorted order
+    std::vector<float> wordWeights;  // TermWeight IDF / PMI: per token, sorted order (empty for ONE)
     float weight = 1.f;
     std::string rawStr, docUid;
     std::vector<uint32_t> origWordPos;
@@ -169,6 +170,8 @@ struct tmt_model {
     uint32_t optim_interval = 10, burn_in = 0;
     int32_t device = 0;
     uint32_t sweep_groups = 0;
+    int32_t tw = 0;                  // TermWeight: 0 ONE, 1 IDF, 2 PMI
+    double weightedN = 0;            // the ll_per_word denominator (TopicModel::weightedN)
     // vocabulary
     std::unordered_map<std::string, uint32_t> dict;
     std::vector<std::string> id2word;
@@ -182,6 +185,7 @@ struct tmt_model {
     // host copies, refreshed on demand
     bool host_fresh = false;
     std::vector<int32_t> nkw, nk, ndk;
+    std::vector<float> nkw_f, nk_f, ndk_f;   // the same for weighted counts
     std::string err;
 
     ~tmt_model()
@@ -208,17 +212,73 @@ struct tmt_model {
     {
         if (host_fresh || !eng) return;
         std::vector<uint16_t> z(realN_all());
-        nkw.assign((uint64_t)K * realV, 0);
-        nk.assign(K, 0);
-        check(tmt_download_state(eng, z.data(), nkw.data(), nk.data(), alphas.data()));
+        if (tw) {
+            nkw_f.assign((uint64_t)K * realV, 0.f);
+            nk_f.assign(K, 0.f);
+            ndk_f.assign((uint64_t)docs.size() * K, 0.f);
+            check(tmt_download_state(eng, z.data(), nullptr, nullptr, alphas.data()));
+            check(tmt_download_counts_f32(eng, docs.empty() ? nullptr : ndk_f.data(), nkw_f.data(), nk_f.data(),
+                                          nullptr));
+        } else {
+            nkw.assign((uint64_t)K * realV, 0);
+            nk.assign(K, 0);
+            check(tmt_download_state(eng, z.data(), nkw.data(), nk.data(), alphas.data()));
+            ndk.assign((uint64_t)docs.size() * K, 0);
+            if (!docs.empty()) check(tmt_download_doc_topic(eng, ndk.data()));
+        }
         uint64_t at = 0;
         for (auto& d : docs) {
             std::copy(z.begin() + at, z.begin() + at + d.words.size(), d.Zs.begin());
             at += d.words.size();
         }
-        ndk.assign((uint64_t)docs.size() * K, 0);
-        if (!docs.empty()) check(tmt_download_doc_topic(eng, ndk.data()));
         host_fresh = true;
+    }
+
+    static const char* tw_key(int32_t t) { return t == 1 ? "idf\0\0" : t == 2 ? "pmi\0\0" : "one\0\0"; }
+
+    // TermWeight IDF / PMI weights (LDAModel.hpp:1093-1122 vocabWeights,
+    // :795-809 per token), in each document's sorted order
+    void compute_weights()
+    {
+        const size_t V = id2word.size();
+        vocabWeights.assign(V, 0.f);
+        if (tw == 1) {
+            std::vector<uint64_t> df(V, 0);
+            for (auto& d : docs) {
+                std::unordered_set<uint32_t> u(d.words.begin(), d.words.end());
+                for (auto w : u)
+                    if (w < realV) ++df[w];
+            }
+            for (size_t i = 0; i < V; ++i) vocabWeights[i] = (float)std::log(docs.size() / (double)df[i]);
+        } else {
+            uint64_t tot = 0;
+            for (auto c : vocabCf) tot += c;
+            for (size_t i = 0; i < V; ++i) vocabWeights[i] = (float)(vocabCf[i] / (double)tot);
+        }
+        std::vector<uint32_t> tf(realV, 0);
+        for (auto& d : docs) doc_weights(d.words, d.wordWeights, tf);
+    }
+
+    // one document's token weights; tf: realV zeros on entry and exit
+    void doc_weights(const std::vector<uint32_t>& words, std::vector<float>& out, std::vector<uint32_t>& tf) const
+    {
+        out.assign(words.size(), 0.f);
+        if (tw == 2)
+            for (auto w : words)
+                if (w < realV) ++tf[w];
+        for (size_t i = 0; i < words.size(); ++i) {
+            const uint32_t w = words[i];
+            if (w >= realV) continue;
+            if (tw == 1) {
+                out[i] = vocabWeights[w];
+            } else {
+                const float q = (float)tf[w] / vocabWeights[w] / (float)words.size();
+                out[i] = std::max((float)std::log((double)q), 0.f);
+            }
+        }
+        if (tw == 2)
+            for (auto w : words)
+                if (w < realV) tf[w] = 0;
     }
 
     uint64_t realN_all() const
@@ -319,10 +379,30 @@ struct tmt_model {
             std::copy(docs[d].words.begin(), docs[d].words.end(), w.begin() + off[d]);
             if (with_z) std::copy(docs[d].Zs.begin(), docs[d].Zs.end(), z.begin() + off[d]);
         }
-        check(tmt_upload_corpus(eng, w.data(), off.data(), docs.size(), with_z ? z.data() : nullptr));
+        if (tw) {
+            std::vector<float> wt(off.back());
+            for (size_t d = 0; d < docs.size(); ++d)
+                std::copy(docs[d].wordWeights.begin(), docs[d].wordWeights.end(), wt.begin() + off[d]);
+            const float none = 0.f;    // a corpus without tokens still passes a weights array
+            check(tmt_upload_corpus_weighted(eng, w.data(), off.data(), docs.size(), with_z ? z.data() : nullptr,
+                                             wt.empty() ? &none : wt.data()));
+        } else {
+            check(tmt_upload_corpus(eng, w.data(), off.data(), docs.size(), with_z ? z.data() : nullptr));
+        }
         realN = 0;
         for (auto x : w) realN += x < realV;
         host_fresh = false;
+    }
+
+    // countRealN's weighted sum (TopicModel.hpp:507-523): the tokens' weights in
+    // document and token order, 1 per token without weights
+    double weighted_sum() const
+    {
+        double s = 0;
+        for (auto& d : docs)
+            for (size_t i = 0; i < d.words.size(); ++i)
+                if (d.words[i] < realV) s += d.wordWeights.empty() ? 1.0 : (double)d.wordWeights[i];
+        return s;
     }
 
     void prepare()
@@ -333,6 +413,13 @@ struct tmt_model {
             sort_doc(d);
             d.Zs.assign(d.words.size(), 0xFFFF);
         }
+        // tomotopy counts weightedN before the weights exist (prepare calls
+        // countRealN first, TopicModel.hpp:652-655): a fresh model's
+        // ll_per_word divides by the token count
+        weightedN = 0;
+        for (auto& d : docs)
+            for (auto w : d.words) weightedN += w < realV;
+        if (tw) compute_weights();
         make_engine();
         upload(false);
         prepared = true;
@@ -343,7 +430,7 @@ struct tmt_model {
     {
         refresh();
         w.key("LDA\0\0", 5);
-        w.key("one\0\0", 5);
+        w.key(tw_key(tw), 5);
         {   // TopicModel header fields
             Writer dic;
             dic.key("Dict", 4);
@@ -383,13 +470,16 @@ struct tmt_model {
             w.tagged("burnIn", bi, 1);
             w.tagged("optimInterval", oi, 0);
         }
-        // globalState: numByTopic (K x 1), numByTopicWord (K x V column-major)
+        // globalState: numByTopic (K x 1), numByTopicWord (K x V column-major);
+        // int32 for TermWeight ONE, float for IDF / PMI (ModelStateLDA<_tw>)
         w.pod<uint32_t>(K);
         w.pod<uint32_t>(1);
-        w.raw(nk.data(), K * sizeof(int32_t));
+        if (tw) w.raw(nk_f.data(), K * sizeof(float));
+        else w.raw(nk.data(), K * sizeof(int32_t));
         w.pod<uint32_t>(K);
         w.pod<uint32_t>((uint32_t)realV);
-        w.raw(nkw.data(), (uint64_t)K * realV * sizeof(int32_t));
+        if (tw) w.raw(nkw_f.data(), (uint64_t)K * realV * sizeof(float));
+        else w.raw(nkw.data(), (uint64_t)K * realV * sizeof(int32_t));
         if (!full) {
             w.pod<uint32_t>(0);
             return;
@@ -405,7 +495,7 @@ struct tmt_model {
             ol.vec(d.origWordLen);
             du.str(d.docUid);
             zs.vec(d.Zs);
-            ww.vec(std::vector<float>{});
+            ww.vec(d.wordWeights);
             w.tagged("weight", wt, 6);
             w.tagged("words", ws, 5);
             w.tagged("wOrder", wo, 4);
@@ -429,7 +519,10 @@ struct tmt_model {
     void load(Reader& r, std::vector<uint8_t>& extra)
     {
         if (!r.expect("LDA\0\0", 5)) throw FormatErr("not an LDA model");
-        if (!r.expect("one\0\0", 5)) throw FormatErr("only TermWeight.ONE models are supported");
+        tw = -1;
+        for (int32_t t = 0; t < 3 && tw < 0; ++t)
+            if (r.expect(tw_key(t), 5)) tw = t;
+        if (tw < 0) throw FormatErr("unknown term weighting");
         auto hdr = r.tagged_chain();
         auto sub = [&](const std::string& k) -> Reader {
             auto it = hdr.find(k);
@@ -496,12 +589,22 @@ struct tmt_model {
         {
             const uint32_t rows = r.pod<uint32_t>(), cols = r.pod<uint32_t>();
             if (rows != K || cols != 1) throw FormatErr("numByTopic shape");
-            nk.resize(K);
-            r.raw(nk.data(), K * sizeof(int32_t));
+            if (tw) {
+                nk_f.resize(K);
+                r.raw(nk_f.data(), K * sizeof(float));
+            } else {
+                nk.resize(K);
+                r.raw(nk.data(), K * sizeof(int32_t));
+            }
             const uint32_t r2 = r.pod<uint32_t>(), c2 = r.pod<uint32_t>();
             if (r2 != K || c2 != realV) throw FormatErr("numByTopicWord shape");
-            nkw.resize((uint64_t)K * realV);
-            r.raw(nkw.data(), nkw.size() * sizeof(int32_t));
+            if (tw) {
+                nkw_f.resize((uint64_t)K * realV);
+                r.raw(nkw_f.data(), nkw_f.size() * sizeof(float));
+            } else {
+                nkw.resize((uint64_t)K * realV);
+                r.raw(nkw.data(), nkw.size() * sizeof(int32_t));
+            }
         }
         // documents
         const uint32_t nd = r.pod<uint32_t>();
@@ -529,15 +632,23 @@ struct tmt_model {
                 Reader q(r.p, it->second.second);
                 q.i = it->second.first;
                 d.Zs = q.vec<uint16_t>();
+                auto iw = f2.find("wordWeights");
+                if (iw != f2.end()) {
+                    Reader q2(r.p, iw->second.second);
+                    q2.i = iw->second.first;
+                    d.wordWeights = q2.vec<float>();
+                }
             } else {
                 if (!r.expect("Docu", 4)) throw FormatErr("bad document");
                 d.weight = r.pod<float>();
                 d.words = r.vec<uint32_t>();
                 d.wOrder = r.vec<uint32_t>();
                 d.Zs = r.vec<uint16_t>();
-                r.vec<float>();
+                d.wordWeights = r.vec<float>();
             }
             if (d.Zs.size() != d.words.size()) throw FormatErr("Zs and words differ in length");
+            if (tw && d.wordWeights.size() != d.words.size()) throw FormatErr("wordWeights and words differ in length");
+            if (!tw) d.wordWeights.clear();
             for (size_t i = 0; i < d.words.size(); ++i)
                 if (d.words[i] < realV && d.Zs[i] >= K) throw FormatErr("topic id out of range");
         }
@@ -545,18 +656,29 @@ struct tmt_model {
         realN = 0;
         for (auto& d : docs)
             for (auto w : d.words) realN += w < realV;
+        // countRealN after a load sees the stored weights (TopicModel.hpp:392-394)
+        weightedN = weighted_sum();
         if (device < 0) {
             // parse only: the host arrays are the state; n_dk recounted from Zs
-            ndk.assign(docs.size() * (uint64_t)K, 0);
-            for (size_t di = 0; di < docs.size(); ++di)
-                for (size_t i = 0; i < docs[di].words.size(); ++i)
-                    if (docs[di].words[i] < realV) ++ndk[di * K + docs[di].Zs[i]];
+            if (tw) {
+                ndk_f.assign(docs.size() * (uint64_t)K, 0.f);
+                for (size_t di = 0; di < docs.size(); ++di)
+                    for (size_t i = 0; i < docs[di].words.size(); ++i)
+                        if (docs[di].words[i] < realV)
+                            ndk_f[di * K + docs[di].Zs[i]] += docs[di].wordWeights[i];
+            } else {
+                ndk.assign(docs.size() * (uint64_t)K, 0);
+                for (size_t di = 0; di < docs.size(); ++di)
+                    for (size_t i = 0; i < docs[di].words.size(); ++i)
+                        if (docs[di].words[i] < realV) ++ndk[di * K + docs[di].Zs[i]];
+            }
             host_fresh = true;
             return;
         }
         make_engine();
         upload(true);
-        check(tmt_set_counts(eng, nkw.data(), nk.data()));
+        if (tw) check(tmt_set_counts_f32(eng, nkw_f.data(), nk_f.data()));
+        else check(tmt_set_counts(eng, nkw.data(), nk.data()));
         check(tmt_set_alpha(eng, alphas.data()));
         check(tmt_set_global_step(eng, globalStep));
         host_fresh = false;
@@ -636,6 +758,8 @@ tmt_status tmt_model_create(const tmt_model_args* a, tmt_model** out)
         m->rm_top = a->rm_top;
         m->device = a->device;
         m->sweep_groups = a->sweep_groups;
+        if (a->tw < 0 || a->tw > 2) throw ArgErr("unknown term weight");
+        m->tw = a->tw;
     });
     *out = m;
     return st;
@@ -716,6 +840,8 @@ tmt_status tmt_model_get_info(tmt_model* m, tmt_model_info* out)
         out->min_cf = m->min_cf;
         out->min_df = m->min_df;
         out->rm_top = m->rm_top;
+        out->tw = m->tw;
+        out->weighted_n = m->weightedN;
     });
 }
 
@@ -745,9 +871,12 @@ tmt_status tmt_model_topic_word_dist(tmt_model* m, uint32_t topic, int normalize
         if (topic >= m->K) throw ArgErr("must topic_id < K");
         m->refresh();
         // _getWidsByTopic (LDAModel.hpp:828-841)
-        const float sum = normalize ? (float)m->nk[topic] + (float)m->realV * m->eta : 1.f;
-        for (uint64_t v = 0; v < m->realV; ++v)
-            out[v] = ((float)m->nkw[v * m->K + topic] + m->eta) / sum;
+        const float nt = m->tw ? m->nk_f[topic] : (float)m->nk[topic];
+        const float sum = normalize ? nt + (float)m->realV * m->eta : 1.f;
+        for (uint64_t v = 0; v < m->realV; ++v) {
+            const float c = m->tw ? m->nkw_f[v * m->K + topic] : (float)m->nkw[v * m->K + topic];
+            out[v] = (c + m->eta) / sum;
+        }
     });
 }
 
@@ -757,7 +886,15 @@ tmt_status tmt_model_count_by_topics(tmt_model* m, uint64_t* out)
     return guard(m, [&] {
         if (!m->eng && !m->host_fresh) throw ArgErr("the model is not trained");
         m->refresh();
-        for (uint32_t k = 0; k < m->K; ++k) out[k] = (uint64_t)m->nk[k];
+        if (m->tw) {
+            // _getTopicsCount (LDAModel.hpp:815-826) counts tokens, not weights
+            std::fill(out, out + m->K, 0);
+            for (auto& d : m->docs)
+                for (size_t i = 0; i < d.Zs.size(); ++i)
+                    if (d.words[i] < m->realV) ++out[d.Zs[i]];
+        } else {
+            for (uint32_t k = 0; k < m->K; ++k) out[k] = (uint64_t)m->nk[k];
+        }
     });
 }
 
@@ -814,19 +951,29 @@ tmt_status tmt_model_doc_topic_dist(tmt_model* m, uint64_t doc, int normalize, f
         if (!m->eng && !m->host_fresh) throw ArgErr("the model is not trained");
         if (doc >= m->docs.size()) throw ArgErr("document index out of range");
         m->refresh();
-        const int32_t* row = m->ndk.data() + doc * m->K;
-        int32_t n = 0;
-        for (uint32_t k = 0; k < m->K; ++k) n += row[k];
+        std::vector<float> row(m->K);
+        float n = 0.f;    // getSumWordWeight (LDA.h:104-133): the token count, or the weights' float sum
+        if (m->tw) {
+            std::copy(m->ndk_f.begin() + doc * m->K, m->ndk_f.begin() + (doc + 1) * m->K, row.begin());
+            for (float x : m->docs[doc].wordWeights) n += x;
+        } else {
+            int32_t c = 0;
+            for (uint32_t k = 0; k < m->K; ++k) {
+                row[k] = (float)m->ndk[doc * m->K + k];
+                c += m->ndk[doc * m->K + k];
+            }
+            n = (float)c;
+        }
         float as = 0.f;
         double asd = 0;
         for (float a : m->alphas) { as += a; asd += a; }
         // _getTopicsByDoc (LDAModel.hpp:1145-1159)
         for (uint32_t k = 0; k < m->K; ++k)
-            out[k] = normalize ? ((float)row[k] + m->alphas[k]) / ((float)n + as) : (float)row[k] + m->alphas[k];
+            out[k] = normalize ? (row[k] + m->alphas[k]) / (n + as) : row[k] + m->alphas[k];
         if (ll) {   // getLLDocs for this document (LDAModel.hpp:616-631), FP64
             double s = 0;
             for (uint32_t k = 0; k < m->K; ++k)
-                if (row[k]) s += std::lgamma((double)row[k] + m->alphas[k]) - std::lgamma((double)m->alphas[k]);
+                if (row[k] != 0.f) s += std::lgamma((double)row[k] + m->alphas[k]) - std::lgamma((double)m->alphas[k]);
             *ll = s - (std::lgamma((double)n + asd) - std::lgamma(asd));
         }
     });
@@ -851,7 +998,21 @@ tmt_status tmt_model_infer(tmt_model* m, const char* words, const uint64_t* doc_
             }
             off[d + 1] = ids.size();
         }
-        m->check(tmt_infer_batch(m->eng, ids.data(), off.data(), D, iters, seed, nullptr, theta, ll));
+        if (m->tw) {
+            // the new documents' weights (initializeDocState, LDAModel.hpp:795-809)
+            std::vector<float> wt(ids.size()), one;
+            std::vector<uint32_t> tf(m->realV, 0);
+            for (uint64_t d = 0; d < D; ++d) {
+                std::vector<uint32_t> ws(ids.begin() + off[d], ids.begin() + off[d + 1]);
+                m->doc_weights(ws, one, tf);
+                std::copy(one.begin(), one.end(), wt.begin() + off[d]);
+            }
+            const float none = 0.f;
+            m->check(tmt_infer_batch_weighted(m->eng, ids.data(), off.data(), D, wt.empty() ? &none : wt.data(),
+                                              iters, seed, nullptr, theta, ll));
+        } else {
+            m->check(tmt_infer_batch(m->eng, ids.data(), off.data(), D, iters, seed, nullptr, theta, ll));
+        }
     });
 }
 
@@ -893,18 +1054,45 @@ tmt_status tmt_model_infer_together(tmt_model* m, const char* words, const uint6
             if (s2 != TMT_OK) throw EngineErr(s2, tmp ? tmt_last_error(tmp) : "tmt_create failed");
         }
         auto ck = [&](tmt_status s2) { if (s2 != TMT_OK) throw EngineErr(s2, tmt_last_error(tmp)); };
-        ck(tmt_upload_corpus(tmp, ids.data(), off.data(), D, nullptr));
-        std::vector<int32_t> nkw((uint64_t)m->K * m->realV), nk(m->K);
-        ck(tmt_download_state(tmp, nullptr, nkw.data(), nk.data(), nullptr));
-        for (size_t i = 0; i < nkw.size(); ++i) nkw[i] += m->nkw[i];
-        for (uint32_t k = 0; k < m->K; ++k) nk[k] += m->nk[k];
-        ck(tmt_set_counts(tmp, nkw.data(), nk.data()));
+        if (m->tw) {
+            // weighted: the new documents' weights; the private state adds the
+            // model's float counts to the documents' (float adds)
+            std::vector<float> wt(ids.size()), one;
+            std::vector<uint32_t> tf(m->realV, 0);
+            for (uint64_t d = 0; d < D; ++d) {
+                std::vector<uint32_t> ws(ids.begin() + off[d], ids.begin() + off[d + 1]);
+                m->doc_weights(ws, one, tf);
+                std::copy(one.begin(), one.end(), wt.begin() + off[d]);
+            }
+            const float none = 0.f;
+            ck(tmt_upload_corpus_weighted(tmp, ids.data(), off.data(), D, nullptr, wt.empty() ? &none : wt.data()));
+            std::vector<float> nkw((uint64_t)m->K * m->realV), nk(m->K);
+            ck(tmt_download_counts_f32(tmp, nullptr, nkw.data(), nk.data(), nullptr));
+            for (size_t i = 0; i < nkw.size(); ++i) nkw[i] += m->nkw_f[i];
+            for (uint32_t k = 0; k < m->K; ++k) nk[k] += m->nk_f[k];
+            ck(tmt_set_counts_f32(tmp, nkw.data(), nk.data()));
+        } else {
+            ck(tmt_upload_corpus(tmp, ids.data(), off.data(), D, nullptr));
+            std::vector<int32_t> nkw((uint64_t)m->K * m->realV), nk(m->K);
+            ck(tmt_download_state(tmp, nullptr, nkw.data(), nk.data(), nullptr));
+            for (size_t i = 0; i < nkw.size(); ++i) nkw[i] += m->nkw[i];
+            for (uint32_t k = 0; k < m->K; ++k) nk[k] += m->nk[k];
+            ck(tmt_set_counts(tmp, nkw.data(), nk.data()));
+        }
         ck(tmt_train(tmp, iters, 0, nullptr));
         double d_docs = 0, d_rest = 0, m_docs = 0, m_rest = 0;
         ck(tmt_ll(tmp, &d_docs, &d_rest));
         m->check(tmt_ll(m->eng, &m_docs, &m_rest));
         if (ll) *ll = d_docs + d_rest - m_rest;
-        if (theta && D) {
+        if (theta && D && m->tw) {
+            std::vector<float> ndk(D * m->K), wl(D);
+            ck(tmt_download_counts_f32(tmp, ndk.data(), nullptr, nullptr, wl.data()));
+            float as = 0.f;
+            for (float a : m->alphas) as += a;
+            for (uint64_t d = 0; d < D; ++d)
+                for (uint32_t k = 0; k < m->K; ++k)
+                    theta[d * m->K + k] = (ndk[d * m->K + k] + m->alphas[k]) / (wl[d] + as);
+        } else if (theta && D) {
             std::vector<int32_t> ndk(D * m->K);
             ck(tmt_download_doc_topic(tmp, ndk.data()));
             float as = 0.f;

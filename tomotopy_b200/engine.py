@@ -46,13 +46,24 @@ class Engine:
     def __del__(self):
         self.close()
 
-    def upload(self, doc_off, words, z0=None):
+    def upload(self, doc_off, words, z0=None, weights=None):
+        """tmt_upload_corpus, or tmt_upload_corpus_weighted when per-token
+        weights (TermWeight IDF / PMI) are given."""
         self._doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
         self._words = np.ascontiguousarray(words, dtype=np.uint32)
         zz = np.ascontiguousarray(z0, dtype=np.uint16) if z0 is not None else None
         self.D = len(self._doc_off) - 1
         self.n_all = int(self._doc_off[-1]) if self.D >= 0 else 0
-        check(lib.tmt_upload_corpus(self.h, _p(self._words), _p(self._doc_off), self.D, _p(zz)), self.h)
+        if weights is None:
+            self.weighted = False
+            check(lib.tmt_upload_corpus(self.h, _p(self._words), _p(self._doc_off), self.D, _p(zz)), self.h)
+        else:
+            self._wt = np.ascontiguousarray(weights, dtype=np.float32)
+            if len(self._wt) != self.n_all:
+                raise ValueError("weights must hold one value per token")
+            self.weighted = True
+            check(lib.tmt_upload_corpus_weighted(self.h, _p(self._words), _p(self._doc_off), self.D, _p(zz),
+                                                 _p(self._wt)), self.h)
 
     def train(self, iters, ll_every=0):
         n = iters // ll_every if ll_every else 0
@@ -60,16 +71,27 @@ class Engine:
         check(lib.tmt_train(self.h, int(iters), int(ll_every), _p(out) if n else None), self.h)
         return out[:n]
 
-    def infer(self, doc_off, words, iters=100, seed=0, doc_keys=None):
-        """tmt_infer_batch: returns (theta [D x K] float32, ll [D] float64)."""
+    def set_graphs(self, enable):
+        """Sweeps as CUDA graph launches after the autotuner's first sweeps
+        (default) or as separate kernel launches; results are identical."""
+        check(lib.tmt_set_graphs(self.h, int(bool(enable))), self.h)
+
+    def infer(self, doc_off, words, iters=100, seed=0, doc_keys=None, weights=None):
+        """tmt_infer_batch (tmt_infer_batch_weighted with per-token weights):
+        returns (theta [D x K] float32, ll [D] float64)."""
         doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
         words = np.ascontiguousarray(words, dtype=np.uint32)
         D = len(doc_off) - 1
         theta = np.zeros((max(D, 1), self.K), dtype=np.float32)
         ll = np.zeros(max(D, 1), dtype=np.float64)
         keys = np.ascontiguousarray(doc_keys, dtype=np.uint64) if doc_keys is not None else None
-        check(lib.tmt_infer_batch(self.h, _p(words), _p(doc_off), D, int(iters), int(seed), _p(keys),
-                                  _p(theta), _p(ll)), self.h)
+        if weights is None:
+            check(lib.tmt_infer_batch(self.h, _p(words), _p(doc_off), D, int(iters), int(seed), _p(keys),
+                                      _p(theta), _p(ll)), self.h)
+        else:
+            wt = np.ascontiguousarray(weights, dtype=np.float32)
+            check(lib.tmt_infer_batch_weighted(self.h, _p(words), _p(doc_off), D, _p(wt), int(iters), int(seed),
+                                               _p(keys), _p(theta), _p(ll)), self.h)
         return theta[:D], ll[:D]
 
     @property
@@ -87,17 +109,35 @@ class Engine:
         return (a + b) / n if n else 0.0
 
     def state(self):
+        """(z, n_kw [V x K], n_k, alpha); float counts when weighted."""
         z = np.zeros(max(self.n_all, 1), dtype=np.uint16)
-        nkw = np.zeros((self.V, self.K), dtype=np.int32)
-        nk = np.zeros(self.K, dtype=np.int32)
         alpha = np.zeros(self.K, dtype=np.float32)
-        check(lib.tmt_download_state(self.h, _p(z), _p(nkw), _p(nk), _p(alpha)), self.h)
+        if getattr(self, "weighted", False):
+            nkw = np.zeros((self.V, self.K), dtype=np.float32)
+            nk = np.zeros(self.K, dtype=np.float32)
+            check(lib.tmt_download_state(self.h, _p(z), None, None, _p(alpha)), self.h)
+            check(lib.tmt_download_counts_f32(self.h, None, _p(nkw), _p(nk), None), self.h)
+        else:
+            nkw = np.zeros((self.V, self.K), dtype=np.int32)
+            nk = np.zeros(self.K, dtype=np.int32)
+            check(lib.tmt_download_state(self.h, _p(z), _p(nkw), _p(nk), _p(alpha)), self.h)
         return z[:self.n_all], nkw, nk, alpha
 
     def doc_topic(self):
-        ndk = np.zeros((max(self.D, 1), self.K), dtype=np.int32)
-        check(lib.tmt_download_doc_topic(self.h, _p(ndk)), self.h)
+        """n_dk [D x K]; float when weighted."""
+        if getattr(self, "weighted", False):
+            ndk = np.zeros((max(self.D, 1), self.K), dtype=np.float32)
+            check(lib.tmt_download_counts_f32(self.h, _p(ndk), None, None, None), self.h)
+        else:
+            ndk = np.zeros((max(self.D, 1), self.K), dtype=np.int32)
+            check(lib.tmt_download_doc_topic(self.h, _p(ndk)), self.h)
         return ndk[:self.D]
+
+    def doc_weight_sums(self):
+        """Per-document weight sums of a weighted corpus."""
+        out = np.zeros(max(self.D, 1), dtype=np.float32)
+        check(lib.tmt_download_counts_f32(self.h, None, None, None, _p(out)), self.h)
+        return out[:self.D]
 
     def info(self):
         i = TmtInfo()

@@ -7,8 +7,8 @@ the GPU.  Differences that a caller can see:
   - `workers` and `parallel` are accepted and ignored: the sweep runs on the
     device with its own parallel scheme (one worker per document, document
     groups; see the design notes);
-  - only TermWeight.ONE; word priors (set_word_prior) are not on the device
-    path and raise NotImplementedError;
+  - TermWeight ONE, IDF and PMI; word priors (set_word_prior) are not on
+    the device path and raise NotImplementedError;
   - log-likelihoods are computed in FP64 with exact lgamma (tomotopy uses a
     float lookup table; the two agree to ~1e-5 relative).
 """
@@ -28,7 +28,7 @@ isa = "cuda-sm_100a"
 
 
 class TermWeight(IntEnum):
-    """tomotopy.TermWeight (__init__.py:10-33); only ONE is supported here."""
+    """tomotopy.TermWeight (__init__.py:10-33)."""
     ONE = 0
     IDF = 1
     PMI = 2
@@ -134,8 +134,8 @@ class LDAModel:
                 tw = TermWeight[tw.upper()]
             except KeyError:
                 raise ValueError(f"Unknown term weight: {tw}")
-        if int(tw) != TermWeight.ONE:
-            raise NotImplementedError("only TermWeight.ONE is on the device path")
+        if int(tw) not in (TermWeight.ONE, TermWeight.IDF, TermWeight.PMI):
+            raise ValueError(f"Unknown term weight: {tw}")
         if corpus is not None:
             raise NotImplementedError("tomotopy.utils.Corpus ingestion is out of scope; use add_doc")
         if not 1 <= int(k) <= 32767:
@@ -145,7 +145,7 @@ class LDAModel:
             seed = int.from_bytes(os.urandom(4), "little")
         args = TmtModelArgs(K=int(k), alpha=al.ctypes.data_as(C.POINTER(C.c_float)), n_alpha=len(al), eta=float(eta),
                             seed=int(seed), min_cf=int(min_cf), min_df=int(min_df), rm_top=int(rm_top),
-                            device=int(device), sweep_groups=int(sweep_groups))
+                            device=int(device), sweep_groups=int(sweep_groups), tw=int(tw))
         h = C.c_void_p()
         st = lib.tmt_model_create(C.byref(args), C.byref(h))
         self._h = h
@@ -411,7 +411,7 @@ class LDAModel:
 
     @property
     def tw(self) -> int:
-        return int(TermWeight.ONE)
+        return int(self._info().tw)
 
     @property
     def global_step(self) -> int:
@@ -424,7 +424,8 @@ class LDAModel:
             return 0.0
         a, b = C.c_double(), C.c_double()
         _check(lib.tmt_model_ll(self._h, C.byref(a), C.byref(b)), self._h)
-        return (a.value + b.value) / i.N
+        # TopicModel::getLLPerWord divides by weightedN (TopicModel.hpp:757-760)
+        return (a.value + b.value) / (i.weighted_n or i.N)
 
     @property
     def perplexity(self) -> float:
