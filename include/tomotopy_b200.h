@@ -180,6 +180,15 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
  * (TopicModel::_loadModel, TopicModel.hpp:361-395).  Later sweeps and
  * inference use it. */
 tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k);
+/* Word priors: LDAModel::setWordPrior (LDAModel.hpp:1031-1045) as applied by
+ * prepareWordPriors (:724-737).  Word word_ids[p] (< V, each once) gets the
+ * K-vector priors[p*K .. p*K+K-1] (finite, >= 0) as its eta column; every
+ * other word keeps the scalar eta.  The conditional uses eta_kv and the
+ * per-topic sums of eta over the words (getZLikelihoods<true>, :273-285),
+ * z0 of every token is drawn from its word's eta column (updateStateWithDoc,
+ * :765-779), and the log-likelihood and inference use the same table
+ * (getLLRest, :636-651).  Call before the upload; P = 0 clears. */
+tmt_status tmt_set_word_priors(tmt_handle* h, uint32_t P, const uint32_t* word_ids, const float* priors);
 /* tmt_set_counts for weighted counts (tmt_upload_corpus_weighted): n_kw (V x K
  * floats, column v = K values) and n_k (K); values finite and >= 0. */
 tmt_status tmt_set_counts_f32(tmt_handle* h, const float* n_kw, const float* n_k);
@@ -376,6 +385,13 @@ typedef struct tmt_model_info {
 tmt_status tmt_model_create(const tmt_model_args* args, tmt_model** out);
 /* add_doc (TopicModel.hpp:397-449): *doc_id = -1 for an empty document. */
 tmt_status tmt_model_add_doc(tmt_model* m, const char* words, uint32_t n_words, int64_t* doc_id);
+/* set_word_prior (LDAModel.hpp:1031-1045, py_LDA.cpp:241-269): n == K priors >= 0
+ * for `word` (added to the dictionary); before train() only; a second call for
+ * the same word is ignored, as etaByWord.emplace ignores it. */
+tmt_status tmt_model_set_word_prior(tmt_model* m, const char* word, const float* prior, uint32_t n);
+/* get_word_prior (LDAModel.hpp:1047-1062): *n = K and the priors (the word's
+ * eta column once prepared with priors), or *n = 0 for none; out may be NULL. */
+tmt_status tmt_model_get_word_prior(tmt_model* m, const char* word, float* out, uint32_t* n);
 /* LDAModel::prepare (LDAModel.hpp:1073-1138); train() calls it when needed. */
 tmt_status tmt_model_prepare(tmt_model* m);
 /* TopicModel::train (TopicModel.hpp:684-755) for `iters` sweeps. */

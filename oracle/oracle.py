@@ -80,6 +80,13 @@ def _load():
         "orc_ll_docs_w_f64": (C.c_double, [C.c_uint64, C.c_uint32, V, V, V]),
         "orc_ll_rest_w_f64": (C.c_double, [C.c_uint32, C.c_uint32, V, V, C.c_float]),
         "orc_optimize_alpha_w": (None, [C.c_uint64, C.c_uint32, V, V, V]),
+        "orc_prior_esum": (None, [C.c_uint32, C.c_uint32, V, V, C.c_float, V]),
+        "orc_init_z_p": (None, [C.c_uint64, V, C.c_uint32, C.c_uint32, V, V, C.c_float, C.c_uint64, V]),
+        "orc_sweep_doc_live_p_subset": (None, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, C.c_uint64,
+                                               C.c_uint32] + [V] * 9 + [C.c_uint64]),
+        "orc_ll_rest_p_f64": (C.c_double, [C.c_uint32, C.c_uint32, V, V, C.c_float, V, V, V]),
+        "orc_infer_doc_p": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, V, V, C.c_uint32,
+                                         C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
         "orc_infer_doc_w": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, C.c_uint32,
                                          C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
     }
@@ -377,6 +384,70 @@ class StateW:
         weighted model divides by the token count."""
         a, b = self.ll_f64()
         return (a + b) / self.c.N
+
+
+class StateP(State):
+    """Integer counts with word priors (etaByTopicWord): prior_ids[p] gets
+    priors[p] (K floats) as its eta column."""
+
+    def __init__(self, corpus, K, alpha, eta, seed, prior_ids, priors, z0=None):
+        self.c = corpus
+        self.K = int(K)
+        self.alpha = f32(np.broadcast_to(np.asarray(alpha, dtype=np.float32), (self.K,)).copy())
+        self.eta = float(np.float32(eta))
+        self.seed = int(seed)
+        self.pidx = np.full(corpus.V, -1, dtype=np.int32)
+        self.pidx[np.asarray(prior_ids, dtype=np.int64)] = np.arange(len(prior_ids), dtype=np.int32)
+        self.prior = np.ascontiguousarray(priors, dtype=np.float32).reshape(len(prior_ids), self.K) \
+            if len(prior_ids) else np.zeros((1, self.K), np.float32)
+        self.esum = np.zeros(self.K, dtype=np.float32)
+        lib.orc_prior_esum(self.K, corpus.V, _ptr(self.pidx), _ptr(self.prior), self.eta, _ptr(self.esum))
+        n_all = len(corpus.words)
+        if z0 is None:
+            self.z = np.zeros(max(n_all, 1), dtype=np.uint16)
+            lib.orc_init_z_p(n_all, _ptr(corpus.words), corpus.V, self.K, _ptr(self.pidx), _ptr(self.prior),
+                             self.eta, self.seed, _ptr(self.z))
+            self.z = self.z[:n_all]
+        else:
+            self.z = np.ascontiguousarray(z0, dtype=np.uint16).copy()
+        self.recount()
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+        c = self.c
+        order, b = self.group_bounds(groups)
+        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
+        for it in range(iters):
+            for part in parts:
+                if len(part) == 0:
+                    continue
+                nkw2 = self.nkw.copy()
+                nk2 = self.nk.copy()
+                lib.orc_sweep_doc_live_p_subset(self.K, c.V, _ptr(self.alpha), self.eta, _ptr(self.pidx),
+                                                _ptr(self.prior), _ptr(self.esum), self.seed, start_step + it,
+                                                _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk), _ptr(self.nkw),
+                                                _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z), _ptr(part),
+                                                len(part))
+                self.nkw = nkw2
+                self.nk = nk2
+
+    def ll_f64(self):
+        c = self.c
+        a = lib.orc_ll_docs_f64(c.D, self.K, _ptr(self.ndk), _ptr(c.doc_len), _ptr(self.alpha))
+        b = lib.orc_ll_rest_p_f64(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), self.eta, _ptr(self.pidx),
+                                  _ptr(self.prior), _ptr(self.esum))
+        return a, b
+
+    def infer_doc(self, nkw, nk, alpha, words, iters, seed, doc_key):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        z = np.zeros(max(len(words), 1), dtype=np.uint16)
+        ndk = np.zeros(self.K, dtype=np.int32)
+        theta = np.zeros(self.K, dtype=np.float32)
+        a = f32(np.asarray(alpha, dtype=np.float32).copy())
+        ll = lib.orc_infer_doc_p(self.K, self.c.V, _ptr(a), self.eta, _ptr(self.pidx), _ptr(self.prior),
+                                 _ptr(self.esum), _ptr(np.ascontiguousarray(nkw, np.int32)),
+                                 _ptr(np.ascontiguousarray(nk, np.int32)), _ptr(words), len(words), iters, seed,
+                                 doc_key, _ptr(z), _ptr(ndk), _ptr(theta))
+        return ll, z[:len(words)], ndk, theta
 
 
 class Partition:

@@ -1343,15 +1343,19 @@ double orc_infer_doc_w(uint32_t K, uint32_t V, const float* alpha, float eta,
 /* Word priors: set_word_prior (LDAModel.hpp:1031-1045, 724-737, 99-117)     */
 /* ------------------------------------------------------------------------ */
 /* etaByTopicWord is eta everywhere except the columns of prior words (pidx[v]
- * >= 0 names row pidx[v] of `prior`, K floats); esum[k] = its row sums,
- * rounded once to float from a double sum over v = 0..V-1.  z0 of every token
+ * >= 0 names row pidx[v] of `prior`, K floats); esum[k] = its row sums:
+ * (V - P) * eta plus the prior words' values in ascending word id, summed
+ * in double and rounded once to float.  z0 of every token
  * ~ Discrete(its word's column) (updateStateWithDoc, :765-779), drawn like
  * orc_init_z from the column's sequential float cumulative sum. */
 void orc_prior_esum(uint32_t K, uint32_t V, const int32_t* pidx, const float* prior, float eta, float* esum)
 {
+    uint32_t P = 0;
+    for (uint32_t v = 0; v < V; ++v) P += pidx[v] >= 0;
     for (uint32_t k = 0; k < K; ++k) {
-        double s = 0;
-        for (uint32_t v = 0; v < V; ++v) s += (double)(pidx[v] >= 0 ? prior[(size_t)pidx[v] * K + k] : eta);
+        double s = (double)(V - P) * (double)eta;
+        for (uint32_t v = 0; v < V; ++v)
+            if (pidx[v] >= 0) s += (double)prior[(size_t)pidx[v] * K + k];
         esum[k] = (float)s;
     }
 }

@@ -87,6 +87,7 @@ SIGNATURES = {
     "tmt_ll": (C.c_int, [_H, _P, _P]),
     "tmt_set_counts": (C.c_int, [_H, _P, _P]),
     "tmt_set_counts_f32": (C.c_int, [_H, _P, _P]),
+    "tmt_set_word_priors": (C.c_int, [_H, C.c_uint32, _P, _P]),
     "tmt_set_alpha": (C.c_int, [_H, _P]),
     "tmt_corpus_counts": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P]),
     "tmt_prepare_corpus_counted": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint64, C.c_uint64,
@@ -123,6 +124,8 @@ SIGNATURES = {
     "tmt_model_create": (C.c_int, [C.POINTER(TmtModelArgs), C.POINTER(_H)]),
     "tmt_model_add_doc": (C.c_int, [_H, C.c_char_p, C.c_uint32, C.POINTER(C.c_int64)]),
     "tmt_model_prepare": (C.c_int, [_H]),
+    "tmt_model_set_word_prior": (C.c_int, [_H, C.c_char_p, _P, C.c_uint32]),
+    "tmt_model_get_word_prior": (C.c_int, [_H, C.c_char_p, _P, C.POINTER(C.c_uint32)]),
     "tmt_model_train": (C.c_int, [_H, C.c_uint32]),
     "tmt_model_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
     "tmt_model_set_seed": (C.c_int, [_H, C.c_uint64]),

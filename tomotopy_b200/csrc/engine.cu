@@ -43,17 +43,49 @@ constexpr int kSweepWarps = 8;           // warps per sweep block
 
 
 // ---------------------------------------------------------------------------
+// word priors (set_word_prior: etaByTopicWord, LDAModel.hpp:99-117, 724-737)
+// ---------------------------------------------------------------------------
+// eta is per (topic, word) only for the words given a prior: idx[v] >= 0 names
+// row idx[v] of val (K floats); every other word keeps the scalar eta.  esum[k]
+// replaces V*eta in the denominators.  All NULL: no priors.
+struct PriorArgs {
+    const int32_t* idx;
+    const float* val;
+    const float* esum;
+};
+
+__device__ __forceinline__ const float* prior_col(const PriorArgs& pr, uint64_t v, uint32_t K)
+{
+    if (!pr.idx) return nullptr;
+    const int p = __ldg(pr.idx + v);
+    return p >= 0 ? pr.val + (uint64_t)p * K : nullptr;
+}
+
+__device__ __forceinline__ float esum_of(const PriorArgs& pr, uint32_t k, float veta)
+{
+    return pr.esum ? __ldg(pr.esum + k) : veta;
+}
+
+// ---------------------------------------------------------------------------
 // initialisation: z0 ~ Discrete(alpha) (initializeDocState, LDAModel.hpp:781-813)
 // ---------------------------------------------------------------------------
+// With word priors (pidx != NULL) every token draws from its word's eta column
+// instead (updateStateWithDoc, LDAModel.hpp:765-779): pcum holds the sequential
+// float cumulative sums of the prior rows, ecum that of a column of eta.
 __global__ void k_init_z(const uint32_t* __restrict__ words, uint64_t n_all, uint32_t V, uint32_t K,
                          const float* __restrict__ acum, uint64_t seed, uint64_t tok_offset,
-                         uint16_t* __restrict__ z)
+                         uint16_t* __restrict__ z, const int32_t* __restrict__ pidx,
+                         const float* __restrict__ pcum, const float* __restrict__ ecum)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_all;
          i += (uint64_t)gridDim.x * blockDim.x) {
         if (words[i] >= V) { z[i] = 0xFFFF; continue; }
         const uint64_t gi = i + tok_offset;      // the token's index in the whole (unsharded) corpus
         float u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamInit, 0, seed));
+        if (pidx) {
+            const int p = pidx[words[i]];
+            acum = p >= 0 ? pcum + (uint64_t)p * K : ecum;
+        }
         float r = __fmul_rn(u, acum[K - 1]);
         uint32_t lo = 0, hi = K - 1;
         while (lo < hi) {
@@ -99,13 +131,13 @@ __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* _
 // next state, which the sweep then updates with the count deltas.
 __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __restrict__ nk, uint32_t V, uint32_t K,
                            uint32_t KP, float eta, float veta, float* __restrict__ phi, int32_t* __restrict__ nkw_next,
-                           int32_t* __restrict__ nk_next, uint32_t smem_k)
+                           int32_t* __restrict__ nk_next, uint32_t smem_k, PriorArgs pr)
 {
     extern __shared__ float s_R[];
     const bool r_smem = K <= smem_k;
     if (r_smem)
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
-            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
     if (blockIdx.x == 0)
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) nk_next[k] = nk[k];
     __syncthreads();
@@ -113,13 +145,14 @@ __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __res
         const int32_t* src = nkw + v * K;
         int32_t* dst = nkw_next + v * K;
         float* ph = phi + v * KP;
+        const float* pe = prior_col(pr, v, K);
         for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
             float val = 0.f;
             if (k < K) {
                 const int32_t n = src[k];
                 dst[k] = n;
-                const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
-                val = __fmul_rn(__fadd_rn((float)n, eta), R);
+                const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
+                val = __fmul_rn(__fadd_rn((float)n, pe ? pe[k] : eta), R);
             }
             ph[k] = val;
         }
@@ -139,18 +172,19 @@ __global__ void k_nk_apply(int32_t* __restrict__ nk, int32_t* __restrict__ dnk, 
 
 __global__ void k_phi_apply(int32_t* __restrict__ nkw, int32_t* __restrict__ delta, const int32_t* __restrict__ nk,
                             uint32_t V, uint32_t K, uint32_t KP, float eta, float veta, float* __restrict__ phi,
-                            uint32_t smem_k, int fold)
+                            uint32_t smem_k, int fold, PriorArgs pr)
 {
     extern __shared__ float s_R[];
     const bool r_smem = phi && K <= smem_k;
     if (r_smem)
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
-            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
+            s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
     __syncthreads();
     for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
         int32_t* col = nkw + v * K;
         int32_t* dcol = delta + v * K;
         float* ph = phi ? phi + v * KP : nullptr;
+        const float* pe = ph ? prior_col(pr, v, K) : nullptr;
         for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
             float val = 0.f;
             if (k < K) {
@@ -161,8 +195,8 @@ __global__ void k_phi_apply(int32_t* __restrict__ nkw, int32_t* __restrict__ del
                     dcol[k] = 0;
                 }
                 if (ph) {
-                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], veta));
-                    val = __fmul_rn(__fadd_rn((float)n, eta), R);
+                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
+                    val = __fmul_rn(__fadd_rn((float)n, pe ? pe[k] : eta), R);
                 }
             }
             if (ph) ph[k] = val;
@@ -198,17 +232,19 @@ __global__ void k_nk_fold_w(float* __restrict__ nk, long long* __restrict__ dk, 
 // n_kw fold (fold != 0) and, when phi != NULL, the word table of the state
 __global__ void k_phi_fold_w(float* __restrict__ nkw, long long* __restrict__ dkw, const float* __restrict__ nk,
                              uint32_t V, uint32_t K, uint32_t KP, float eta, float veta, float* __restrict__ phi,
-                             uint32_t smem_k, int fold)
+                             uint32_t smem_k, int fold, PriorArgs pr)
 {
     extern __shared__ float s_R[];
     const bool r_smem = phi && K <= smem_k;
     if (r_smem)
-        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) s_R[k] = __fdiv_rn(1.0f, __fadd_rn(nk[k], veta));
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            s_R[k] = __fdiv_rn(1.0f, __fadd_rn(nk[k], esum_of(pr, k, veta)));
     __syncthreads();
     for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
         float* col = nkw + v * K;
         long long* dcol = dkw + v * K;
         float* ph = phi ? phi + v * KP : nullptr;
+        const float* pe = ph ? prior_col(pr, v, K) : nullptr;
         for (uint32_t k = threadIdx.x; k < KP; k += blockDim.x) {
             float val = 0.f;
             if (k < K) {
@@ -219,8 +255,8 @@ __global__ void k_phi_fold_w(float* __restrict__ nkw, long long* __restrict__ dk
                     dcol[k] = 0;
                 }
                 if (ph) {
-                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn(nk[k], veta));
-                    val = __fmul_rn(__fadd_rn(n, eta), R);
+                    const float R = r_smem ? s_R[k] : __fdiv_rn(1.0f, __fadd_rn(nk[k], esum_of(pr, k, veta)));
+                    val = __fmul_rn(__fadd_rn(n, pe ? pe[k] : eta), R);
                 }
             }
             if (ph) ph[k] = val;
@@ -273,6 +309,7 @@ struct SweepArgs {
     const float* wt;          // token weights (doc-major)
     long long* dkw;           // V x K
     long long* dk;            // K
+    PriorArgs pr;             // word priors (all NULL: none)
     uint64_t D;
     uint32_t K, V, c;
     float eta, veta;
@@ -330,16 +367,32 @@ k_sweep_doc(SweepArgs a)
     const float eta = a.eta, veta = a.veta;
     const uint32_t iter = a.iter_ptr ? *a.iter_ptr : a.iter;
 
-    auto load_word = [&](uint32_t v, int zo, float4 (&pv)[CHR], CT& nkw_o, CT& nk_o, float& phu) {
+    // a token's word weights, the table's own-topic entry phu and the own
+    // topic's weight with the token removed, phio (w: the token's weight)
+    auto load_word = [&](uint32_t v, int zo, float w, float4 (&pv)[CHR], float& phu, float& phio) {
         const float* ph = a.phi + (uint64_t)v * KP;
         if (CH > 0) {
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
-        nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
-        nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
+        const CT nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
+        const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
         phu = __ldg(ph + zo);
+        float eo = eta, so = veta;
+        if (a.pr.idx) {
+            const float* pe = prior_col(a.pr, v, K);
+            if (pe) eo = __ldg(pe + zo);
+            so = __ldg(a.pr.esum + zo);
+        }
+        if constexpr (WT) {
+            float co = __fsub_rn(nkw_o, w), no = __fsub_rn(nk_o, w);
+            co = co > 0.f ? co : 0.f;
+            no = no > 0.f ? no : 0.f;
+            phio = __fmul_rn(__fadd_rn(co, eo), __fdiv_rn(1.0f, __fadd_rn(no, so)));
+        } else {
+            phio = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eo), __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), so)));
+        }
     };
 
     for (;;) {
@@ -382,20 +435,18 @@ k_sweep_doc(SweepArgs a)
                 uint32_t v = __shfl_sync(FULL, my_w, j);
                 int zo = (int)__shfl_sync(FULL, my_z, j);
                 float4 pv[CHR];
-                CT nkw_o, nk_o;
-                float phu;
-                load_word(v, zo, pv, nkw_o, nk_o, phu);
+                float phu, phi_own;
+                load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, pv, phu, phi_own);
                 for (;;) {
                     const int jn = vm ? __ffs(vm) - 1 : -1;
                     uint32_t vn = 0;
                     int zon = 0;
                     float4 pvn[CHR];
-                    CT nkw_on = 0, nk_on = 0;
-                    float phun = 0.f;
+                    float phun = 0.f, phion = 0.f;
                     if (PF && jn >= 0) {
                         vn = __shfl_sync(FULL, my_w, jn);
                         zon = (int)__shfl_sync(FULL, my_z, jn);
-                        load_word(vn, zon, pvn, nkw_on, nk_on, phun);
+                        load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, pvn, phun, phion);
                     }
                     const float u = __shfl_sync(FULL, my_u, j);
                     const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
@@ -413,16 +464,6 @@ k_sweep_doc(SweepArgs a)
                         }
                     }
                     __syncwarp();
-                    float phi_own;
-                    if constexpr (WT) {
-                        float co = __fsub_rn(nkw_o, wt), no = __fsub_rn(nk_o, wt);
-                        co = co > 0.f ? co : 0.f;
-                        no = no > 0.f ? no : 0.f;
-                        phi_own = __fmul_rn(__fadd_rn(co, eta), __fdiv_rn(1.0f, __fadd_rn(no, veta)));
-                    } else {
-                        phi_own = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eta),
-                                            __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), veta)));
-                    }
                     // pass 1: fma chain over this lane's topics
                     float s = 0.f;
                     if (CH > 0) {
@@ -557,13 +598,12 @@ k_sweep_doc(SweepArgs a)
                         zo = zon;
 #pragma unroll
                         for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
-                        nkw_o = nkw_on;
-                        nk_o = nk_on;
                         phu = phun;
+                        phi_own = phion;
                     } else {
                         v = __shfl_sync(FULL, my_w, j);
                         zo = (int)__shfl_sync(FULL, my_z, j);
-                        load_word(v, zo, pv, nkw_o, nk_o, phu);
+                        load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, pv, phu, phi_own);
                     }
                 }
             }
@@ -613,7 +653,7 @@ __global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K
                               const double* __restrict__ lg_alpha, const float* __restrict__ alpha,
                               const LT* __restrict__ doc_len, const double* __restrict__ asum_p,
                               const CT* __restrict__ nkw, uint32_t V, double eta, double lg_eta,
-                              double* __restrict__ partials)
+                              double* __restrict__ partials, PriorArgs pr)
 {
     __shared__ double s_d[32], s_r[32];
     const double asum = asum_p[0], lg_asum = asum_p[1];
@@ -633,9 +673,12 @@ __global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K
     // every rank of a sharded corpus and on one GPU holding all of it
     for (uint64_t v = gw; v < V; v += nw) {
         const CT* p = nkw + v * K;
+        const float* pe = prior_col(pr, v, K);
         for (uint32_t k = lane; k < K; k += 32) {
             const CT n = p[k];
-            if (n != CT(0)) accr += lgamma((double)n + eta) - lg_eta;
+            if (n == CT(0)) continue;
+            if (pe) accr += lgamma((double)n + (double)pe[k]) - lgamma((double)pe[k]);
+            else accr += lgamma((double)n + eta) - lg_eta;
         }
     }
     accd = warp_sum(accd);
@@ -651,15 +694,20 @@ __global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K
     }
 }
 
+// esum != NULL (word priors): the per-topic sums of eta replace V*eta
 template <typename CT>
 __global__ void k_ll_final(const double* __restrict__ partials, uint32_t nparts,
-                           const CT* __restrict__ nk, uint32_t K, double veta, double* __restrict__ out)
+                           const CT* __restrict__ nk, uint32_t K, double veta, double* __restrict__ out,
+                           const float* __restrict__ esum)
 {
     __shared__ double s_d[32], s_r[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double x = 0, y = 0;
     for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) { x += partials[2 * i]; y += partials[2 * i + 1]; }
-    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) y += lgamma(veta) - lgamma((double)nk[k] + veta);
+    for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+        const double es = esum ? (double)esum[k] : veta;
+        y += lgamma(es) - lgamma((double)nk[k] + es);
+    }
     x = warp_sum(x);
     y = warp_sum(y);
     if (lane == 0) { s_d[warp] = x; s_r[warp] = y; }
@@ -844,6 +892,16 @@ struct tmt_handle {
     long long* d_dkw = nullptr;      // V x K
     long long* d_dk = nullptr;       // K
     float* d_doc_wlen = nullptr;     // per document: the sum of its token weights
+    // word priors (tmt_set_word_priors): host copies, and their device tables
+    // (allocated by the upload)
+    std::vector<uint32_t> prior_ids;
+    std::vector<float> prior_vals;   // P x K
+    int32_t* d_prior_idx = nullptr;  // V: row of d_prior, -1 for no prior
+    float* d_prior = nullptr;        // P x K
+    float* d_esum = nullptr;         // K: sum over the words of eta_kv
+    float* d_prior_cum = nullptr;    // P x K: cumulative rows (z0 draws)
+    float* d_cum_eta = nullptr;      // K: cumulative column of eta
+    PriorArgs prior_args() const { return PriorArgs{ d_prior_idx, d_prior, d_esum }; }
     // sweep-kernel autotuner: variants give bit-identical results, so the
     // first sweeps each time one variant and the fastest is kept
     int variant = 0;                 // the variant of the sweep being tuned
@@ -1112,6 +1170,7 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.pos_begin = pos_begin;
     a.pos_end = pos_end;
     a.tok_offset = h->tok_offset;
+    a.pr = h->prior_args();
     return a;
 }
 
@@ -1140,7 +1199,7 @@ void do_sweep_sharded(tmt_handle* h)
             launch_check(h);
         }
         k_phi_apply<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta,
-                                                        veta, h->d_phi, smem_k, pending ? 1 : 0);
+                                                        veta, h->d_phi, smem_k, pending ? 1 : 0, h->prior_args());
         launch_check(h);
         if (h->group_bounds[g] < h->group_bounds[g + 1]) {
             CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
@@ -1156,7 +1215,7 @@ void do_sweep_sharded(tmt_handle* h)
         k_nk_apply<<<1, 1024, 0, h->stream>>>(h->d_nk[0], dnk, K);
         launch_check(h);
         k_phi_apply<<<grid, 256, 0, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta, veta,
-                                                nullptr, 0, 1);
+                                                nullptr, 0, 1, h->prior_args());
         launch_check(h);
     }
     CK(cudaEventRecord(h->kev1, h->stream));
@@ -1186,7 +1245,7 @@ void do_sweep_w(tmt_handle* h, bool capture)
             launch_check(h);
         }
         k_phi_fold_w<<<grid, 256, smem_k * 4, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta,
-                                                         h->d_phi, smem_k, pending ? 1 : 0);
+                                                         h->d_phi, smem_k, pending ? 1 : 0, h->prior_args());
         launch_check(h);
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
         SweepArgs a = sweep_args(h, h->d_nkw[0], h->d_nk[0], nullptr, nullptr, h->group_bounds[g],
@@ -1206,7 +1265,8 @@ void do_sweep_w(tmt_handle* h, bool capture)
     if (pending) {
         k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
         launch_check(h);
-        k_phi_fold_w<<<grid, 256, 0, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta, nullptr, 0, 1);
+        k_phi_fold_w<<<grid, 256, 0, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta, nullptr, 0, 1,
+                                                 h->prior_args());
         launch_check(h);
     }
     if (!capture) {
@@ -1235,7 +1295,8 @@ void do_sweep(tmt_handle* h, bool capture = false)
         const uint32_t smem_k = K <= 12288 ? K : 0;
         uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
         k_phi_copy<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[cur], h->d_nk[cur], V, K, round4(K), h->cfg.eta,
-                                                        veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k);
+                                                        veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k,
+                                                        h->prior_args());
         launch_check(h);
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
         SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
@@ -1343,17 +1404,19 @@ void do_ll(tmt_handle* h, double* d_out)
     if (h->weighted) {
         k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(
             reinterpret_cast<const float*>(h->d_ndk), h->D, K, h->d_lg_alpha, h->d_alpha, (const float*)h->d_doc_wlen,
-            h->d_asum_ll, reinterpret_cast<const float*>(h->d_nkw[0]), h->cfg.V, eta, std::lgamma(eta), h->d_partials);
+            h->d_asum_ll, reinterpret_cast<const float*>(h->d_nkw[0]), h->cfg.V, eta, std::lgamma(eta), h->d_partials,
+            h->prior_args());
         launch_check(h);
         k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, reinterpret_cast<const float*>(h->d_nk[0]),
-                                             K, veta, d_out);
+                                             K, veta, d_out, h->d_esum);
     } else {
         k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
                                                             h->d_doc_len, h->d_asum_ll,
                                                             h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
-                                                            h->d_partials);
+                                                            h->d_partials, h->prior_args());
         launch_check(h);
-        k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out);
+        k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out,
+                                             h->d_esum);
     }
     launch_check(h);
     exchange(h, d_out, 1, TMT_F64);     // LLDocs over every rank's documents; LLRest is replicated
@@ -1533,6 +1596,45 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             h->d_nk[1] = h->dalloc<int32_t>(K);
         }
         h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
+        h->d_prior_idx = nullptr;
+        h->d_prior = h->d_esum = h->d_prior_cum = h->d_cum_eta = nullptr;
+        if (!h->prior_ids.empty()) {
+            // etaByTopicWord as a sparse table (prepareWordPriors, LDAModel.hpp:724-737)
+            const uint32_t P = (uint32_t)h->prior_ids.size();
+            std::vector<int32_t> idx(V, -1);
+            for (uint32_t p = 0; p < P; ++p) idx[h->prior_ids[p]] = (int32_t)p;
+            std::vector<float> esum(K), pcum((uint64_t)P * K), ecum(K);
+            // the row sums of etaByTopicWord in double, rounded once: (V - P) * eta,
+            // then the prior words' values in ascending word id
+            std::vector<uint32_t> by_id(h->prior_ids.begin(), h->prior_ids.end());
+            std::sort(by_id.begin(), by_id.end());
+            for (uint32_t k = 0; k < K; ++k) {
+                double sd = (double)(V - P) * (double)h->cfg.eta;
+                for (uint32_t v : by_id) sd += (double)h->prior_vals[(uint64_t)idx[v] * K + k];
+                esum[k] = (float)sd;
+            }
+            for (uint32_t p = 0; p < P; ++p) {
+                float acc = 0.f;
+                for (uint32_t k = 0; k < K; ++k) {
+                    acc = acc + h->prior_vals[(uint64_t)p * K + k];
+                    pcum[(uint64_t)p * K + k] = acc;
+                }
+            }
+            float acc = 0.f;
+            for (uint32_t k = 0; k < K; ++k) { acc = acc + h->cfg.eta; ecum[k] = acc; }
+            h->d_prior_idx = h->dalloc<int32_t>(V);
+            h->d_prior = h->dalloc<float>((uint64_t)P * K);
+            h->d_esum = h->dalloc<float>(K);
+            h->d_prior_cum = h->dalloc<float>((uint64_t)P * K);
+            h->d_cum_eta = h->dalloc<float>(K);
+            cudaStream_t s0 = h->stream;
+            CK(cudaMemcpyAsync(h->d_prior_idx, idx.data(), V * sizeof(int32_t), cudaMemcpyHostToDevice, s0));
+            CK(cudaMemcpyAsync(h->d_prior, h->prior_vals.data(), (uint64_t)P * K * sizeof(float), cudaMemcpyHostToDevice, s0));
+            CK(cudaMemcpyAsync(h->d_esum, esum.data(), K * sizeof(float), cudaMemcpyHostToDevice, s0));
+            CK(cudaMemcpyAsync(h->d_prior_cum, pcum.data(), (uint64_t)P * K * sizeof(float), cudaMemcpyHostToDevice, s0));
+            CK(cudaMemcpyAsync(h->d_cum_eta, ecum.data(), K * sizeof(float), cudaMemcpyHostToDevice, s0));
+            CK(cudaStreamSynchronize(s0));
+        }
         {
             // the first n_variants sweeps run eagerly, one variant each, and
             // every group keeps its fastest
@@ -1585,7 +1687,8 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             float* d_acum = h->dalloc<float>(K);
             CK(cudaMemcpyAsync(d_acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (n_all + 255) / 256);
-            k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->tok_offset, h->d_z);
+            k_init_z<<<grid, 256, 0, st>>>(h->d_words, n_all, V, K, d_acum, h->cfg.seed, h->tok_offset, h->d_z,
+                                           h->d_prior_idx, h->d_prior_cum, h->d_cum_eta);
             launch_check(h);
         }
         if (D && h->weighted) {
@@ -1601,7 +1704,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             const uint32_t g2 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
             k_phi_fold_w<<<g2, 256, 0, st>>>(reinterpret_cast<float*>(h->d_nkw[0]), h->d_dkw,
                                              reinterpret_cast<const float*>(h->d_nk[0]), V, K, round4(K), h->cfg.eta,
-                                             h->cfg.eta * (float)V, nullptr, 0, 1);
+                                             h->cfg.eta * (float)V, nullptr, 0, 1, h->prior_args());
             launch_check(h);
             // the token counts per document as well (the shard planner's facts)
             CK(cudaMemcpyAsync(h->d_doc_len, len.data(), D * sizeof(int32_t), cudaMemcpyHostToDevice, st));
@@ -1898,6 +2001,28 @@ tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k
     });
 }
 
+tmt_status tmt_set_word_priors(tmt_handle* h, uint32_t P, const uint32_t* word_ids, const float* priors)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (h->uploaded) throw StateError("word priors must be set before the corpus is uploaded");
+        if (P && (!word_ids || !priors)) throw ArgError("word_ids / priors is NULL");
+        const uint32_t K = h->cfg.K, V = h->cfg.V;
+        if (P > V) throw ArgError("more prior words than words");
+        std::vector<uint8_t> seen(V, 0);
+        for (uint32_t p = 0; p < P; ++p) {
+            if (word_ids[p] >= V) throw ArgError("prior word id " + std::to_string(word_ids[p]) + " >= V");
+            if (seen[word_ids[p]]++) throw ArgError("prior word id " + std::to_string(word_ids[p]) + " given twice");
+            for (uint32_t k = 0; k < K; ++k) {
+                const float x = priors[(uint64_t)p * K + k];
+                if (!(x >= 0.f) || !std::isfinite(x)) throw ArgError("priors must be finite and not less than 0");
+            }
+        }
+        h->prior_ids.assign(word_ids, word_ids + P);
+        h->prior_vals.assign(priors, priors + (uint64_t)P * K);
+    });
+}
+
 tmt_status tmt_set_counts_f32(tmt_handle* h, const float* n_kw, const float* n_k)
 {
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
@@ -2101,6 +2226,11 @@ tmt_status infer_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_of
         a.n_work = (uint32_t)D;
         a.counter = B.counter;
         a.wt = weights ? B.wt : nullptr;
+        a.pidx = h->d_prior_idx;
+        a.pval = h->d_prior;
+        a.esum = h->d_esum;
+        a.pcum = h->d_prior_cum;
+        a.ecum = h->d_cum_eta;
         launch_infer(a, h->num_sms, h->stream);
         ++h->launches;
         if (theta) CK(cudaMemcpyAsync(theta, B.theta, D * (uint64_t)K * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -2181,8 +2311,8 @@ tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, co
     const double etad = (double)eta;
     k_ll_prep<<<1, 256, 0, st>>>(alpha, K, lg_alpha, asum);
     k_ll_partials<<<blocks, 256, 0, st>>>(n_dk, D, K, lg_alpha, alpha, doc_len, asum, n_kw, V, etad,
-                                          std::lgamma(etad), partials);
-    k_ll_final<<<1, 256, 0, st>>>(partials, blocks, n_k, K, (double)V * etad, ll_out);
+                                          std::lgamma(etad), partials, PriorArgs{});
+    k_ll_final<<<1, 256, 0, st>>>(partials, blocks, n_k, K, (double)V * etad, ll_out, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     return say(TMT_OK, "");

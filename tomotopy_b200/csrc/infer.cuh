@@ -57,6 +57,14 @@ struct InferArgs {
     // within a document (IDF: the word's weight; PMI: a function of the word's
     // count in the document)
     const float* wt;
+    // word priors (etaByTopicWord): pidx[v] >= 0 names row pidx[v] of pval
+    // (K floats); esum[k] replaces V*eta; z0 draws from pcum (the rows'
+    // cumulative sums) or ecum (a column of eta).  pidx == NULL: no priors.
+    const int32_t* pidx;
+    const float* pval;
+    const float* esum;
+    const float* pcum;
+    const float* ecum;
 };
 
 // WT: weighted counts.  The document's counts n_dk are float sums of weights
@@ -111,11 +119,16 @@ k_infer_slots(InferArgs a)
                 uint16_t zz = 0xFFFF;
                 if (w < a.V) {
                     const float u = tmt::u01(tmt::philox_u32(j, 0xFFFFFFFFu, klo, khi, a.key));
-                    const float r = __fmul_rn(u, a.acum[K - 1]);
+                    const float* cum = a.acum;
+                    if (a.pidx) {
+                        const int p = a.pidx[w];
+                        cum = p >= 0 ? a.pcum + (uint64_t)p * K : a.ecum;
+                    }
+                    const float r = __fmul_rn(u, cum[K - 1]);
                     uint32_t lo = 0, hi = K - 1;
                     while (lo < hi) {
                         const uint32_t mid = (lo + hi) >> 1;
-                        if (r < a.acum[mid]) hi = mid; else lo = mid + 1;
+                        if (r < cum[mid]) hi = mid; else lo = mid + 1;
                     }
                     zz = (uint16_t)lo;
                     if (!WT) atomicAdd(reinterpret_cast<int*>(rowi) + lo, 1);
@@ -146,8 +159,9 @@ k_infer_slots(InferArgs a)
         __syncwarp();
         // R_k's denominator: (float)(n_k + n_dk) for integer counts, (n_k + n_dk) in float for weights
         auto rden = [&](int k, CT n) -> float {
-            if constexpr (WT) return __fadd_rn(__fadd_rn(__ldg(nkv + k), n), veta);
-            else return __fadd_rn((float)(__ldg(nkv + k) + n), veta);
+            const float es = a.esum ? __ldg(a.esum + k) : veta;
+            if constexpr (WT) return __fadd_rn(__fadd_rn(__ldg(nkv + k), n), es);
+            else return __fadd_rn((float)(__ldg(nkv + k) + n), es);
         };
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f, g = 0.f;
@@ -229,10 +243,16 @@ k_infer_slots(InferArgs a)
                     const bool multi = j < run_e;
                     const CT* gcol = nkw + (uint64_t)v * K;
                     if (CH > 0 && v != v_have) { load_col(v, gv); v_have = v; }
+                    const float* pe = nullptr;           // the word's prior column, if any
+                    if (a.pidx) {
+                        const int p = __ldg(a.pidx + v);
+                        if (p >= 0) pe = a.pval + (uint64_t)p * K;
+                    }
                     // B_k before the multiplication by R_k
-                    auto bk = [&](CT g, int o) -> float {
-                        if constexpr (WT) return __fadd_rn(__fadd_rn(g, __fmul_rn((float)o, wt)), eta);
-                        else return __fadd_rn((float)(g + o), eta);
+                    auto bk = [&](CT g, int o, int k) -> float {
+                        const float ek = pe ? __ldg(pe + k) : eta;
+                        if constexpr (WT) return __fadd_rn(__fadd_rn(g, __fmul_rn((float)o, wt)), ek);
+                        else return __fadd_rn((float)(g + o), ek);
                     };
                     if (lane == 0) {
                         if (multi) own[zo] -= 1;
@@ -259,17 +279,17 @@ k_infer_slots(InferArgs a)
                                 const float4 R4 = *reinterpret_cast<const float4*>(rr + k0);
                                 int4 O4 = make_int4(0, 0, 0, 0);
                                 if (multi) O4 = *reinterpret_cast<const int4*>(own + k0);
-                                s = __fmaf_rn(A4.x, __fmul_rn(bk(gv[jj].x, O4.x), R4.x), s);
-                                s = __fmaf_rn(A4.y, __fmul_rn(bk(gv[jj].y, O4.y), R4.y), s);
-                                s = __fmaf_rn(A4.z, __fmul_rn(bk(gv[jj].z, O4.z), R4.z), s);
-                                s = __fmaf_rn(A4.w, __fmul_rn(bk(gv[jj].w, O4.w), R4.w), s);
+                                s = __fmaf_rn(A4.x, __fmul_rn(bk(gv[jj].x, O4.x, k0), R4.x), s);
+                                s = __fmaf_rn(A4.y, __fmul_rn(bk(gv[jj].y, O4.y, k0 + 1), R4.y), s);
+                                s = __fmaf_rn(A4.z, __fmul_rn(bk(gv[jj].z, O4.z, k0 + 2), R4.z), s);
+                                s = __fmaf_rn(A4.w, __fmul_rn(bk(gv[jj].w, O4.w, k0 + 3), R4.w), s);
                             }
                         }
                     } else {
                         for (int jj = 0; jj < nch; ++jj)
                             for (int i = 0; i < 4; ++i) {
                                 const int k = 128 * jj + 4 * lane + i;
-                                if (k < K) s = __fmaf_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), own[k]), rr[k]), s);
+                                if (k < K) s = __fmaf_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), own[k], k), rr[k]), s);
                             }
                     }
                     const float x = hs_scan32(s, lane);
@@ -292,7 +312,7 @@ k_infer_slots(InferArgs a)
                             const int k = 128 * (t >> 2) + 4 * h + (t & 3);
                             float x2 = 0.f;
                             if (t < nh)
-                                x2 = __fmul_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), multi ? own[k] : 0), rr[k]));
+                                x2 = __fmul_rn(rowf[k], __fmul_rn(bk(__ldg(gcol + k), multi ? own[k] : 0, k), rr[k]));
                             x2 = hs_scan32(x2, lane);
                             const unsigned mb = __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
                             if (mb) { found = mm + __ffs(mb) - 1; break; }
@@ -334,7 +354,8 @@ k_infer_slots(InferArgs a)
             if (a.theta) a.theta[(uint64_t)sl * K + k] = __fdiv_rn(__fadd_rn((float)n, __ldg(a.alpha + k)), denom);
             if (n != CT(0)) {
                 const double gk = (double)__ldg(nkv + k);
-                acc += lgamma(gk + a.veta_d) - lgamma(gk + (double)n + a.veta_d);
+                const double es = a.esum ? (double)__ldg(a.esum + k) : a.veta_d;
+                acc += lgamma(gk + es) - lgamma(gk + (double)n + es);
                 const double al = (double)__ldg(a.alpha + k);
                 acc += lgamma((double)n + al) - lgamma(al);
             }
@@ -354,15 +375,21 @@ k_infer_slots(InferArgs a)
                 for (uint32_t j = rb + lane; j < re; j += 32) atomicAdd(&own[a.z[b + j]], 1);
                 __syncwarp();
                 const float wr = WT ? a.wt[b + rb] : 1.f;    // the run's weight
+                const float* pe = nullptr;
+                if (a.pidx) {
+                    const int p = a.pidx[v];
+                    if (p >= 0) pe = a.pval + (uint64_t)p * K;
+                }
                 for (uint32_t j = rb + lane; j < re; j += 32) {
                     const int k = a.z[b + j];
                     const int c = atomicExch(&own[k], 0);
                     if (c) {
                         const CT gk = __ldg(nkw + (uint64_t)v * K + k);
+                        const double ek = pe ? (double)pe[k] : (double)a.eta;
                         double after;
-                        if constexpr (WT) after = lgamma(((double)gk + (double)__fmul_rn((float)c, wr)) + (double)a.eta);
-                        else after = lgamma((double)(gk + c) + (double)a.eta);
-                        acc += after - (gk != CT(0) ? lgamma((double)gk + (double)a.eta) : a.lg_eta);
+                        if constexpr (WT) after = lgamma(((double)gk + (double)__fmul_rn((float)c, wr)) + ek);
+                        else after = lgamma((double)(gk + c) + ek);
+                        acc += after - (gk != CT(0) ? lgamma((double)gk + ek) : (pe ? lgamma(ek) : a.lg_eta));
                     }
                 }
                 __syncwarp();

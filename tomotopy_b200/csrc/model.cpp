@@ -180,6 +180,9 @@ struct tmt_model {
     uint64_t realV = 0, realN = 0, globalStep = 0;
     bool prepared = false;
     std::vector<float> vocabWeights;
+    // set_word_prior (LDAModel.hpp:1031-1045): word -> K priors, in insertion
+    // (or file) order; the first call for a word wins (etaByWord.emplace)
+    std::vector<std::pair<std::string, std::vector<float>>> etaByWord;
     // device state
     tmt_handle* eng = nullptr;
     // host copies, refreshed on demand
@@ -345,6 +348,28 @@ struct tmt_model {
         }
     }
 
+    // prepareWordPriors (LDAModel.hpp:724-737): the prior words still in the
+    // vocabulary (id < realV) get their columns
+    void apply_word_priors()
+    {
+        std::vector<uint32_t> ids;
+        std::vector<float> vals;
+        for (auto& e : etaByWord) {
+            auto it = dict.find(e.first);
+            if (it == dict.end() || it->second >= realV) continue;
+            ids.push_back(it->second);
+            vals.insert(vals.end(), e.second.begin(), e.second.end());
+        }
+        check(tmt_set_word_priors(eng, (uint32_t)ids.size(), ids.data(), vals.data()));
+    }
+
+    const std::vector<float>* prior_of(const std::string& w) const
+    {
+        for (auto& e : etaByWord)
+            if (e.first == w) return &e.second;
+        return nullptr;
+    }
+
     void make_engine()
     {
         if (eng) { tmt_destroy(eng); eng = nullptr; }
@@ -421,6 +446,7 @@ struct tmt_model {
             for (auto w : d.words) weightedN += w < realV;
         if (tw) compute_weights();
         make_engine();
+        apply_word_priors();
         upload(false);
         prepared = true;
     }
@@ -458,7 +484,11 @@ struct tmt_model {
             as.raw(alphas.data(), K * sizeof(float));
             e.pod<float>(eta);
             k.pod<uint16_t>((uint16_t)K);
-            ebw.pod<uint32_t>(0);
+            ebw.pod<uint32_t>((uint32_t)etaByWord.size());
+            for (auto& e : etaByWord) {
+                ebw.str(e.first);
+                ebw.vec(e.second);
+            }
             bi.pod<uint32_t>(burn_in);
             oi.pod<uint32_t>(optim_interval);
             w.tagged("vocabWeights", vw, 7);
@@ -570,7 +600,13 @@ struct tmt_model {
             { Reader q = g("K"); K = q.pod<uint16_t>(); }
             if (f.count("etaByWord")) {
                 Reader q = g("etaByWord");
-                if (q.pod<uint32_t>() != 0) throw FormatErr("word priors are not supported");
+                const uint32_t n = q.pod<uint32_t>();
+                etaByWord.clear();
+                for (uint32_t i = 0; i < n; ++i) {
+                    std::string w = q.str();
+                    std::vector<float> pr = q.vec<float>();
+                    etaByWord.emplace_back(std::move(w), std::move(pr));
+                }
             }
             if (f.count("burnIn")) { Reader q = g("burnIn"); burn_in = q.pod<uint32_t>(); }
             if (f.count("optimInterval")) { Reader q = g("optimInterval"); optim_interval = q.pod<uint32_t>(); }
@@ -675,7 +711,10 @@ struct tmt_model {
             host_fresh = true;
             return;
         }
+        for (auto& e : etaByWord)
+            if (e.second.size() != K) throw FormatErr("a word prior does not have K values");
         make_engine();
+        apply_word_priors();
         upload(true);
         if (tw) check(tmt_set_counts_f32(eng, nkw_f.data(), nk_f.data()));
         else check(tmt_set_counts(eng, nkw.data(), nk.data()));
@@ -783,6 +822,51 @@ tmt_status tmt_model_add_doc(tmt_model* m, const char* words, uint32_t n_words, 
         for (auto w : uniq) ++m->vocabDf[w];
         m->docs.push_back(std::move(d));
         *doc_id = (int64_t)m->docs.size() - 1;
+    });
+}
+
+tmt_status tmt_model_set_word_prior(tmt_model* m, const char* word, const float* prior, uint32_t n)
+{
+    if (!m || !word || (n && !prior)) return TMT_ERR_INVALID_ARGUMENT;
+    return guard(m, [&] {
+        if (m->prepared) throw ArgErr("cannot set_word_prior() after train()");
+        if (n != m->K) throw ArgErr("priors.size() must be equal to K.");
+        for (uint32_t k = 0; k < n; ++k)
+            if (!(prior[k] >= 0.f)) throw ArgErr("priors must not be less than 0.");
+        const std::string w(word);
+        m->add_word(w);
+        m->vocabCf.resize(m->id2word.size());
+        m->vocabDf.resize(m->id2word.size());
+        if (!m->prior_of(w)) m->etaByWord.emplace_back(w, std::vector<float>(prior, prior + n));
+    });
+}
+
+tmt_status tmt_model_get_word_prior(tmt_model* m, const char* word, float* out, uint32_t* n)
+{
+    if (!m || !word || !n) return TMT_ERR_INVALID_ARGUMENT;
+    return guard(m, [&] {
+        // getWordPrior (LDAModel.hpp:1047-1062): after preparation with any
+        // prior, a word's column of etaByTopicWord (eta for words without one);
+        // before, the stored priors
+        *n = 0;
+        const std::string w(word);
+        bool any = false;
+        for (auto& e : m->etaByWord) {
+            auto it = m->dict.find(e.first);
+            if (it != m->dict.end() && it->second < m->realV) any = true;
+        }
+        if (m->prepared && any) {
+            auto it = m->dict.find(w);
+            if (it == m->dict.end() || it->second >= m->realV) return;
+            const auto* p = m->prior_of(w);
+            for (uint32_t k = 0; k < m->K; ++k) if (out) out[k] = p ? (*p)[k] : m->eta;
+            *n = m->K;
+            return;
+        }
+        if (const auto* p = m->prior_of(w)) {
+            if (out) std::copy(p->begin(), p->end(), out);
+            *n = (uint32_t)p->size();
+        }
     });
 }
 

@@ -71,6 +71,15 @@ class Engine:
         check(lib.tmt_train(self.h, int(iters), int(ll_every), _p(out) if n else None), self.h)
         return out[:n]
 
+    def set_word_priors(self, word_ids, priors):
+        """tmt_set_word_priors: word_ids[p] gets priors[p] (K floats) as its eta
+        column; call before upload()."""
+        ids = np.ascontiguousarray(word_ids, dtype=np.uint32)
+        pr = np.ascontiguousarray(priors, dtype=np.float32).reshape(len(ids), self.K) if len(ids) else \
+            np.zeros((0, self.K), np.float32)
+        self._prior_ids, self._prior = ids, pr
+        check(lib.tmt_set_word_priors(self.h, len(ids), _p(ids), _p(pr)), self.h)
+
     def set_graphs(self, enable):
         """Sweeps as CUDA graph launches after the autotuner's first sweeps
         (default) or as separate kernel launches; results are identical."""
@@ -202,6 +211,10 @@ class Server:
         return mid.value
 
     def add_engine_model(self, eng):
+        """A trained engine's frozen state; integer counts without word priors
+        (the served pool infers with the scalar eta)."""
+        if getattr(eng, "weighted", False) or len(getattr(eng, "_prior_ids", ())):
+            raise ValueError("the served pool takes integer-count models without word priors")
         _, nkw, nk, alpha = eng.state()
         return self.add_model(eng.K, eng.V, alpha, eng.eta, nkw, nk)
 

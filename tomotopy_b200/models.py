@@ -7,8 +7,8 @@ the GPU.  Differences that a caller can see:
   - `workers` and `parallel` are accepted and ignored: the sweep runs on the
     device with its own parallel scheme (one worker per document, document
     groups; see the design notes);
-  - TermWeight ONE, IDF and PMI; word priors (set_word_prior) are not on
-    the device path and raise NotImplementedError;
+  - TermWeight ONE, IDF and PMI, and word priors (set_word_prior), all on the
+    device path;
   - log-likelihoods are computed in FP64 with exact lgamma (tomotopy uses a
     float lookup table; the two agree to ~1e-5 relative).
 """
@@ -303,11 +303,35 @@ class LDAModel:
         _check(lib.tmt_model_count_by_topics(self._h, _p(out)), self._h)
         return out
 
-    def get_word_prior(self, word):
-        raise NotImplementedError("word priors are not on the device path")
+    def get_word_prior(self, word) -> List[float]:
+        """The topic distribution prior of `word` (tomotopy's get_word_prior):
+        its K priors, or [] when it has none."""
+        n = C.c_uint32()
+        _check(lib.tmt_model_get_word_prior(self._h, word.encode(), None, C.byref(n)), self._h)
+        out = np.zeros(max(n.value, 1), dtype=np.float32)
+        _check(lib.tmt_model_get_word_prior(self._h, word.encode(), _p(out), C.byref(n)), self._h)
+        return [float(x) for x in out[:n.value]]
 
     def set_word_prior(self, word, prior):
-        raise NotImplementedError("word priors are not on the device path")
+        """Sets the topic distribution prior of `word` (tomotopy's set_word_prior,
+        py_LDA.cpp:241-269): a list of K floats, or a dict {topic_id: float}
+        whose missing topics keep eta.  Before train() only."""
+        if self._info().prepared:
+            raise RuntimeError("cannot set_word_prior() after train()")
+        k = self.k
+        if isinstance(prior, dict):
+            vals = np.full(k, self.eta, dtype=np.float32)
+            for t, v in prior.items():
+                t = int(t)
+                if t < 0 or t >= k:
+                    raise ValueError("`prior` must be a dict of {topic_id: float}")
+                vals[t] = float(v)
+        else:
+            try:
+                vals = np.asarray([float(x) for x in prior], dtype=np.float32)
+            except (TypeError, ValueError):
+                raise ValueError("`prior` must be a list of floats with len = k")
+        _check(lib.tmt_model_set_word_prior(self._h, str(word).encode(), _p(vals), len(vals)), self._h)
 
     def summary(self, initial_hp=True, params=True, topic_word_top_n=5, file=None, flush=False):
         import sys
