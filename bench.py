@@ -439,6 +439,58 @@ def cpu_infer_baseline(engines, which, docs, iters, seconds=10.0):
             "sample": f"{n} request documents, per-document infer on {cores} host threads"}
 
 
+def run_prepare(args, w):
+    """Corpus preparation (tomotopy's removeStopwords + prepareDoc) of the
+    workload's raw ids: tmt_prepare_corpus_device against the host
+    tmt_prepare_corpus on all host threads, host buffers in and out, outputs
+    compared bit for bit.  One JSON line (tokens/s of the device path)."""
+    import torch
+    import tomotopy_b200 as T
+    from tomotopy_b200._lib import lib
+    torch.cuda.set_device(0)
+    off, words = T.synth_corpus(w["V"], w["T"], w["D"], w["length"], seed=w["seed"], threads=os.cpu_count())
+    nv = int(words.max()) + 1
+    D, N = len(off) - 1, len(words)
+
+    def p(a):
+        return a.ctypes.data_as(C.c_void_p)
+
+    def once(device):
+        out = np.zeros(N, np.uint32)
+        wo = np.zeros(N, np.uint32)
+        order = np.zeros(nv, np.uint32)
+        cf = np.zeros(nv, np.uint64)
+        df = np.zeros(nv, np.uint64)
+        rv = C.c_uint32()
+        t0 = time.perf_counter()
+        if device:
+            err = C.create_string_buffer(512)
+            st = lib.tmt_prepare_corpus_device(0, D, p(off), p(words), nv, 0, 0, 0, p(out), p(wo), p(order), p(cf),
+                                               p(df), C.byref(rv), err, len(err))
+        else:
+            st = lib.tmt_prepare_corpus(D, p(off), p(words), nv, 0, 0, 0, p(out), p(wo), p(order), p(cf), p(df),
+                                        C.byref(rv))
+        dt = time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError("preparation failed: %d" % st)
+        return dt, (out, wo, order, cf, df, rv.value)
+
+    for _ in range(args.warmup):
+        once(True)
+    td = min(once(True)[0] for _ in range(max(args.steps, 1)))
+    th = min(once(False)[0] for _ in range(2))
+    a, b = once(True)[1], once(False)[1]
+    same = all(np.array_equal(x, y) for x, y in zip(a[:5], b[:5])) and a[5] == b[5]
+    print(json.dumps({
+        "metric": "corpus preparation tokens/s (vocab reorder + per-document sort)", "value": N / td,
+        "unit": "tokens/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": td * 1e3,
+        "higher_is_better": True, "dtype": "u32", "data": "synthetic (seeded LDA generative process)",
+        "config": {"workload": args.config, "D": D, "tokens": N, "n_vocab": nv,
+                   "timing": "wall clock around one call, host buffers in and out, best of the timed calls"},
+        "host": {"value": N / th, "ms": th * 1e3, "threads": os.cpu_count(), "kind": "tmt_prepare_corpus"},
+        "identical": bool(same)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,7 +502,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI pass")
     ap.add_argument("--docs", type=int, default=0, help="override the document count (smaller case)")
     ap.add_argument("--groups", type=int, default=0, help="document groups per sweep (0: engine default)")
-    ap.add_argument("--mode", default="train", choices=["train", "infer"])
+    ap.add_argument("--mode", default="train", choices=["train", "infer", "prepare"])
     ap.add_argument("--requests", type=int, default=20000, help="infer mode: documents per run")
     ap.add_argument("--slots", type=int, default=8192, help="infer mode: server slots per model")
     ap.add_argument("--step-tokens", type=int, default=4096, help="infer mode: token-sweeps per document per step")
@@ -463,6 +515,8 @@ def main():
     w = dict(WORKLOADS[args.config])
     if args.docs:
         w["D"] = args.docs
+    if args.mode == "prepare":
+        return run_prepare(args, w)
     if args.impl == "reference":
         return run_reference(args, w)
 

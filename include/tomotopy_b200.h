@@ -314,6 +314,17 @@ tmt_status tmt_prepare_corpus(uint64_t D, const uint64_t* doc_off, const uint32_
                               uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
                               uint64_t* vocab_cf, uint64_t* vocab_df, uint32_t* real_v);
 
+/* tmt_prepare_corpus on GPU `device`, for large corpora: the same outputs, bit
+ * for bit (the per-document sorts run on the device, the vocabulary order on
+ * the host).  Every document holds at most 16384 tokens; a longer one returns
+ * TMT_ERR_INVALID_ARGUMENT with a message in err (use tmt_prepare_corpus).
+ * Allocates and frees its own device memory. */
+tmt_status tmt_prepare_corpus_device(int32_t device, uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                                     uint32_t n_vocab, uint64_t min_cf, uint64_t min_df, uint64_t rm_top,
+                                     uint32_t* words_out, uint32_t* w_order, uint32_t* vocab_order,
+                                     uint64_t* vocab_cf, uint64_t* vocab_df, uint32_t* real_v, char* err,
+                                     uint64_t err_len);
+
 /* tmt_prepare_corpus in two halves, for a corpus split across processes:
  * the (cf, df) of one shard's words (by old id), and the preparation of one
  * shard from the counts summed over all shards, so that every shard gets the

@@ -1535,3 +1535,79 @@ double orc_infer_doc_p(uint32_t K, uint32_t V, const float* alpha, float eta,
     free(own); free(A); free(BR); free(cum);
     return ll;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Per-document topic masks and alphas: the derived models' conditionals    */
+/* ------------------------------------------------------------------------ */
+/* LLDA / PLDA multiply the conditional by the document's label mask
+ * (LLDAModel.hpp:37-48, PLDAModel.hpp:39); DMR replaces alpha by the
+ * document's alpha (getCachedAlpha, DMRModel.hpp:193-206).  Device
+ * semantics: A_k = ((float)n_dk + alpha_dk) * m_dk with m_dk in {0, 1}; a
+ * masked topic's weight is exactly 0 and an unmasked one's is unchanged.
+ * mask: D rows of ceil(K/32) words (bit k of row d), NULL = all topics;
+ * arow: D indices into alpha_rows (M x K), NULL = the model's alpha. */
+static inline float mask_bit(const uint32_t* mask, uint32_t mw, uint64_t d, uint32_t k)
+{
+    return mask ? (float)((mask[d * mw + (k >> 5)] >> (k & 31)) & 1u) : 1.f;
+}
+
+void orc_sweep_doc_live_m_subset(uint32_t K, uint32_t V, const float* alpha, const float* alpha_rows,
+                                 const uint32_t* arow, const uint32_t* mask, float eta,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, int32_t* ndk,
+                                 const int32_t* nkw, const int32_t* nk,
+                                 int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                                 const uint64_t* docs, uint64_t n_docs)
+{
+    float veta = eta * (float)V;
+    uint32_t mw = (K + 31) / 32;
+    float* R = (float*)malloc(K * sizeof(float));
+    float* A = (float*)malloc(K * sizeof(float));
+    float* phi = (float*)malloc(K * sizeof(float));
+    for (uint32_t k = 0; k < K; ++k) R[k] = 1.0f / ((float)nk[k] + veta);
+    for (uint64_t di = 0; di < n_docs; ++di) {
+        uint64_t d = docs ? docs[di] : di;
+        const float* al = arow ? alpha_rows + (size_t)arow[d] * K : alpha;
+        int32_t* row = ndk + d * K;
+        for (uint32_t k = 0; k < K; ++k) A[k] = ((float)row[k] + al[k]) * mask_bit(mask, mw, d, k);
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            uint16_t zo = z[i];
+            const int32_t* col = nkw + (size_t)v * K;
+            row[zo]--;
+            A[zo] = ((float)row[zo] + al[zo]) * mask_bit(mask, mw, d, zo);
+            for (uint32_t k = 0; k < K; ++k) phi[k] = ((float)col[k] + eta) * R[k];
+            float phi_own = ((float)(col[zo] - 1) + eta) * (1.0f / ((float)(nk[zo] - 1) + veta));
+            float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, iter, seed));
+            uint16_t zn = (uint16_t)blocked_draw(A, phi, K, zo, phi_own, u);
+            row[zn]++;
+            A[zn] = ((float)row[zn] + al[zn]) * mask_bit(mask, mw, d, zn);
+            z[i] = zn;
+            if (zn != zo) {
+                nkw_next[(size_t)v * K + zo]--; nkw_next[(size_t)v * K + zn]++;
+                nk_next[zo]--; nk_next[zn]++;
+            }
+        }
+    }
+    free(R); free(A); free(phi);
+}
+
+/* getLLDocs with per-document alphas (DMR's getLLDocTopic, DMRModel.hpp:208-224), FP64 */
+double orc_ll_docs_m_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                         const float* alpha_rows, const uint32_t* arow)
+{
+    double ll = 0;
+    for (uint64_t d = 0; d < D; ++d) {
+        const float* al = alpha_rows + (size_t)arow[d] * K;
+        double as = 0, s = 0;
+        for (uint32_t k = 0; k < K; ++k) as += (double)al[k];
+        for (uint32_t k = 0; k < K; ++k) {
+            int32_t c = ndk[d * K + k];
+            if (!c) continue;
+            s += lgamma((double)c + (double)al[k]) - lgamma((double)al[k]);
+        }
+        ll += s - (lgamma((double)doc_len[d] + as) - lgamma(as));
+    }
+    return ll;
+}

@@ -223,6 +223,19 @@ double orc_infer_doc_p(uint32_t K, uint32_t V, const float* alpha, float eta,
                        const uint32_t* words, uint32_t len, uint32_t iters,
                        uint64_t seed, uint64_t doc_key, uint16_t* z, int32_t* ndk, float* theta);
 
+/* ---- per-document topic masks and alphas (LLDA / PLDA / DMR conditionals) -- */
+/* A_k = ((float)n_dk + alpha_dk) * m_dk; mask: D rows of ceil(K/32) words or
+ * NULL; arow: per-document rows of alpha_rows (M x K) or NULL */
+void orc_sweep_doc_live_m_subset(uint32_t K, uint32_t V, const float* alpha, const float* alpha_rows,
+                                 const uint32_t* arow, const uint32_t* mask, float eta,
+                                 uint64_t seed, uint32_t iter, const uint64_t* doc_off,
+                                 const uint32_t* words, int32_t* ndk,
+                                 const int32_t* nkw, const int32_t* nk,
+                                 int32_t* nkw_next, int32_t* nk_next, uint16_t* z,
+                                 const uint64_t* docs, uint64_t n_docs);
+double orc_ll_docs_m_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
+                         const float* alpha_rows, const uint32_t* arow);
+
 #ifdef __cplusplus
 }
 #endif

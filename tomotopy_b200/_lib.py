@@ -107,6 +107,9 @@ SIGNATURES = {
     "tmt_destroy": (None, [_H]),
     "tmt_prepare_corpus": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
                                      _P, _P, _P, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_prepare_corpus_device": (C.c_int, [C.c_int32, C.c_uint64, _P, _P, C.c_uint32, C.c_uint64, C.c_uint64,
+                                            C.c_uint64, _P, _P, _P, _P, _P, C.POINTER(C.c_uint32), C.c_char_p,
+                                            C.c_uint64]),
     "tmt_ll_counts_noalloc": (C.c_int, [_P, C.c_uint64, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_float, _P, _P,
                                         C.c_char_p, C.c_size_t]),
     "tmt_server_start": (C.c_int, [C.POINTER(TmtServerConfig), C.POINTER(_H)]),

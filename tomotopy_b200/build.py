@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libtomotopy_b200.so")
 
-SOURCES = ["engine.cu", "server.cu", "model.cpp", "synth.cpp", "prepare.cpp"]
+SOURCES = ["engine.cu", "server.cu", "ingest.cu", "model.cpp", "synth.cpp", "prepare.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1045,13 +1045,15 @@ struct SweepShape {
     uint32_t rowi_smem, dnk_smem;
 };
 
-SweepShape sweep_shape(uint32_t K, bool weighted)
+// rowi_global: the document's count row stays in global memory (L1-cached),
+// halving the shared memory of a warp (the occupancy variant)
+SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false)
 {
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
     SweepShape s{};
     s.dnk_smem = K <= (weighted ? 8192u : 16384u);
-    s.rowi_smem = K <= 8192;
+    s.rowi_smem = K <= 8192 && !rowi_global;
     const uint32_t per_warp = 4 * KP + (s.rowi_smem ? 4 * KP : 0);
     const uint32_t fixed = s.dnk_smem ? (weighted ? 8 : 4) * KP : 0;
     uint32_t w = (budget - fixed) / per_warp;
@@ -1083,12 +1085,14 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 }
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
-// topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM.
+// topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
+// document row in global memory, 4 blocks/SM.
 template <int CH, bool WT>
 void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, int variant)
 {
     constexpr bool kPrefetch = CH <= 8;   // above, the prefetch registers spill
-    if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
+    if (variant == 2) launch_sweep_t<CH, 4, false, WT>(h, a, sh);
+    else if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
     else launch_sweep_t<CH, 2, kPrefetch, WT>(h, a, sh);
 }
 
@@ -1109,7 +1113,7 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const uint32_t KP = round4(a.K);
     const uint32_t ch = (KP + 127) / 128;
     const bool wt = a.wt != nullptr;
-    const SweepShape sh = sweep_shape(a.K, wt);
+    const SweepShape sh = sweep_shape(a.K, wt, variant == 2);
     SweepArgs b = a;
     b.rowi_smem = sh.rowi_smem;
     b.dnk_smem = sh.dnk_smem;
@@ -1639,7 +1643,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             // the first n_variants sweeps run eagerly, one variant each, and
             // every group keeps its fastest
             const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
-            h->n_variants = round4(K) <= 4096 ? 2 : 1;
+            h->n_variants = round4(K) <= 4096 ? 3 : 1;
             h->variant = 0;
             h->tuned = -1;
             h->group_variant.assign(G, 0);
