@@ -180,6 +180,19 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
  * (TopicModel::_loadModel, TopicModel.hpp:361-395).  Later sweeps and
  * inference use it. */
 tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k);
+/* Per-document topic masks: the label masks of LLDAModel (getZLikelihoods
+ * multiplies the conditional by doc.labelMask, LLDAModel.hpp:37-48) and
+ * PLDAModel (PLDAModel.hpp:39).  mask_bits holds D rows of ceil(K/32) words;
+ * bit k of row d allows topic k in document d.  A masked topic's weight is
+ * exactly 0; unmasked topics are unchanged.  After the upload (pass z0 drawn
+ * inside the masks to the upload); NULL clears.  Single GPU. */
+tmt_status tmt_set_doc_topic_mask(tmt_handle* h, const uint32_t* mask_bits);
+/* Per-document alphas: DMRModel's getCachedAlpha (DMRModel.hpp:193-206).
+ * alpha_rows is M x K (> 0); document d uses row doc_row[d] in the
+ * conditional and in the log-likelihood (DMR's getLLDocTopic, :208-224); the
+ * alpha optimiser is skipped (DMR fits its own lambda).  After the upload;
+ * alpha_rows == NULL clears.  Single GPU. */
+tmt_status tmt_set_doc_alpha(tmt_handle* h, uint32_t M, const float* alpha_rows, const uint32_t* doc_row);
 /* Word priors: LDAModel::setWordPrior (LDAModel.hpp:1031-1045) as applied by
  * prepareWordPriors (:724-737).  Word word_ids[p] (< V, each once) gets the
  * K-vector priors[p*K .. p*K+K-1] (finite, >= 0) as its eta column; every

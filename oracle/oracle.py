@@ -87,6 +87,9 @@ def _load():
         "orc_ll_rest_p_f64": (C.c_double, [C.c_uint32, C.c_uint32, V, V, C.c_float, V, V, V]),
         "orc_infer_doc_p": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, V, V, C.c_uint32,
                                          C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
+        "orc_sweep_doc_live_m_subset": (None, [C.c_uint32, C.c_uint32, V, V, V, V, C.c_float, C.c_uint64,
+                                               C.c_uint32] + [V] * 9 + [C.c_uint64]),
+        "orc_ll_docs_m_f64": (C.c_double, [C.c_uint64, C.c_uint32, V, V, V, V]),
         "orc_infer_doc_w": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, C.c_uint32,
                                          C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
     }
@@ -448,6 +451,50 @@ class StateP(State):
                                  _ptr(np.ascontiguousarray(nk, np.int32)), _ptr(words), len(words), iters, seed,
                                  doc_key, _ptr(z), _ptr(ndk), _ptr(theta))
         return ll, z[:len(words)], ndk, theta
+
+
+class StateM(State):
+    """Per-document topic masks (LLDA / PLDA) and alphas (DMR) on top of the
+    doc-major sweep: A_k = ((float)n_dk + alpha_dk) * m_dk.  mask: D x K bool
+    or None; alpha_rows (M x K) with doc_row (D) or None.  z0 is the caller's."""
+
+    def __init__(self, corpus, K, alpha, eta, seed, z0, mask=None, alpha_rows=None, doc_row=None):
+        super().__init__(corpus, K, alpha, eta, seed, z0=z0)
+        self.mask_bits = None
+        if mask is not None:
+            mw = (self.K + 31) // 32
+            bits = np.zeros((corpus.D, mw * 32), dtype=bool)
+            bits[:, :self.K] = np.asarray(mask, dtype=bool)
+            w = np.packbits(bits.reshape(corpus.D, mw, 32)[:, :, ::-1], axis=2, bitorder="big")
+            self.mask_bits = np.ascontiguousarray(w.view(">u4").reshape(corpus.D, mw).astype(np.uint32))
+        self.alpha_rows = None if alpha_rows is None else np.ascontiguousarray(alpha_rows, np.float32)
+        self.doc_row = None if doc_row is None else np.ascontiguousarray(doc_row, np.uint32)
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+        c = self.c
+        order, b = self.group_bounds(groups)
+        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
+        for it in range(iters):
+            for part in parts:
+                if len(part) == 0:
+                    continue
+                nkw2 = self.nkw.copy()
+                nk2 = self.nk.copy()
+                lib.orc_sweep_doc_live_m_subset(self.K, c.V, _ptr(self.alpha), _ptr(self.alpha_rows),
+                                                _ptr(self.doc_row), _ptr(self.mask_bits), self.eta, self.seed,
+                                                start_step + it, _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk),
+                                                _ptr(self.nkw), _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z),
+                                                _ptr(part), len(part))
+                self.nkw = nkw2
+                self.nk = nk2
+
+    def ll_f64(self):
+        a, b = super().ll_f64()
+        if self.alpha_rows is not None:
+            c = self.c
+            a = lib.orc_ll_docs_m_f64(c.D, self.K, _ptr(self.ndk), _ptr(c.doc_len), _ptr(self.alpha_rows),
+                                      _ptr(self.doc_row))
+        return a, b
 
 
 class Partition:

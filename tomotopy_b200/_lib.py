@@ -88,6 +88,8 @@ SIGNATURES = {
     "tmt_set_counts": (C.c_int, [_H, _P, _P]),
     "tmt_set_counts_f32": (C.c_int, [_H, _P, _P]),
     "tmt_set_word_priors": (C.c_int, [_H, C.c_uint32, _P, _P]),
+    "tmt_set_doc_topic_mask": (C.c_int, [_H, _P]),
+    "tmt_set_doc_alpha": (C.c_int, [_H, C.c_uint32, _P, _P]),
     "tmt_set_alpha": (C.c_int, [_H, _P]),
     "tmt_corpus_counts": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P]),
     "tmt_prepare_corpus_counted": (C.c_int, [C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint64, C.c_uint64,

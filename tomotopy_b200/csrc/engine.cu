@@ -310,6 +310,12 @@ struct SweepArgs {
     long long* dkw;           // V x K
     long long* dk;            // K
     PriorArgs pr;             // word priors (all NULL: none)
+    // per-document conditionals of the derived models (all NULL: none):
+    // A_k = ((float)n_dk + alpha_dk) * m_dk
+    const float* alpha_rows;  // M x K
+    const uint32_t* arow;     // D: the document's row of alpha_rows
+    const uint32_t* mask;     // D x mw words: bit k = topic k allowed
+    uint32_t mw;
     uint64_t D;
     uint32_t K, V, c;
     float eta, veta;
@@ -404,12 +410,19 @@ k_sweep_doc(SweepArgs a)
         const uint64_t d = a.doc_order[pos];
         CT* grow = reinterpret_cast<CT*>(a.ndk) + d * (uint64_t)K;
         CT* rowi = a.rowi_smem ? reinterpret_cast<CT*>(s_rowi + warp * KP) : grow;
+        // the document's alphas and topic mask (the derived models' conditionals)
+        const float* alpha = a.arow ? a.alpha_rows + (uint64_t)a.arow[d] * K : a.alpha;
+        const uint32_t* dmask = a.mask ? a.mask + d * (uint64_t)a.mw : nullptr;
+        auto afold = [&](float n, int k) -> float {
+            const float x = __fadd_rn(n, __ldg(alpha + k));
+            return dmask ? __fmul_rn(x, (float)((__ldg(dmask + (k >> 5)) >> (k & 31)) & 1u)) : x;
+        };
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f;
             if (k < K) {
                 const CT n = grow[k];
                 if (a.rowi_smem) rowi[k] = n;
-                f = __fadd_rn((float)n, __ldg(a.alpha + k));
+                f = afold((float)n, k);
             }
             rowf[k] = f;
         }
@@ -456,11 +469,11 @@ k_sweep_doc(SweepArgs a)
                             float n = __fsub_rn(rowi[zo], wt);
                             n = n > 0.f ? n : 0.f;
                             rowi[zo] = n;
-                            rowf[zo] = __fadd_rn(n, __ldg(a.alpha + zo));
+                            rowf[zo] = afold(n, zo);
                         } else {
                             const int n = rowi[zo] - 1;
                             rowi[zo] = n;
-                            rowf[zo] = __fadd_rn((float)n, __ldg(a.alpha + zo));
+                            rowf[zo] = afold((float)n, zo);
                         }
                     }
                     __syncwarp();
@@ -565,7 +578,7 @@ k_sweep_doc(SweepArgs a)
                         if constexpr (WT) {
                             const float n = __fadd_rn(rowi[znew], wt);
                             rowi[znew] = n;
-                            rowf[znew] = __fadd_rn(n, __ldg(a.alpha + znew));
+                            rowf[znew] = afold(n, znew);
                             if (znew != zo) {
                                 const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(wt, 16777216.f));
                                 unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
@@ -579,7 +592,7 @@ k_sweep_doc(SweepArgs a)
                         } else {
                             const int n = rowi[znew] + 1;
                             rowi[znew] = n;
-                            rowf[znew] = __fadd_rn((float)n, __ldg(a.alpha + znew));
+                            rowf[znew] = afold((float)n, znew);
                             if (znew != zo) {
                                 atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
                                 atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
@@ -653,7 +666,8 @@ __global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K
                               const double* __restrict__ lg_alpha, const float* __restrict__ alpha,
                               const LT* __restrict__ doc_len, const double* __restrict__ asum_p,
                               const CT* __restrict__ nkw, uint32_t V, double eta, double lg_eta,
-                              double* __restrict__ partials, PriorArgs pr)
+                              double* __restrict__ partials, PriorArgs pr, const float* __restrict__ alpha_rows,
+                              const uint32_t* __restrict__ arow, const double* __restrict__ row_asum)
 {
     __shared__ double s_d[32], s_r[32];
     const double asum = asum_p[0], lg_asum = asum_p[1];
@@ -663,6 +677,17 @@ __global__ void k_ll_partials(const CT* __restrict__ ndk, uint64_t D, uint32_t K
     double accd = 0, accr = 0;
     for (uint64_t r = gw; r < D; r += nw) {
         const CT* p = ndk + r * K;
+        if (arow) {
+            // the document's own alphas (DMR's getLLDocTopic, DMRModel.hpp:208-224)
+            const float* al = alpha_rows + (uint64_t)arow[r] * K;
+            for (uint32_t k = lane; k < K; k += 32) {
+                const CT n = p[k];
+                if (n != CT(0)) accd += lgamma((double)n + (double)al[k]) - lgamma((double)al[k]);
+            }
+            const double as_r = row_asum[2 * arow[r]], lgas_r = row_asum[2 * arow[r] + 1];
+            if (lane == 0) accd -= lgamma((double)doc_len[r] + as_r) - lgas_r;
+            continue;
+        }
         for (uint32_t k = lane; k < K; k += 32) {
             const CT n = p[k];
             if (n != CT(0)) accd += lgamma((double)n + (double)alpha[k]) - lg_alpha[k];
@@ -902,6 +927,11 @@ struct tmt_handle {
     float* d_prior_cum = nullptr;    // P x K: cumulative rows (z0 draws)
     float* d_cum_eta = nullptr;      // K: cumulative column of eta
     PriorArgs prior_args() const { return PriorArgs{ d_prior_idx, d_prior, d_esum }; }
+    // per-document alphas and topic masks (tmt_set_doc_alpha / tmt_set_doc_topic_mask)
+    float* d_alpha_rows = nullptr;   // M x K
+    uint32_t* d_arow = nullptr;      // D
+    double* d_row_asum = nullptr;    // M x 2: sum of a row, lgamma of it
+    uint32_t* d_mask = nullptr;      // D x ceil(K/32)
     // sweep-kernel autotuner: variants give bit-identical results, so the
     // first sweeps each time one variant and the fastest is kept
     int variant = 0;                 // the variant of the sweep being tuned
@@ -1175,6 +1205,10 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.pos_end = pos_end;
     a.tok_offset = h->tok_offset;
     a.pr = h->prior_args();
+    a.alpha_rows = h->d_alpha_rows;
+    a.arow = h->d_arow;
+    a.mask = h->d_mask;
+    a.mw = (h->cfg.K + 31) / 32;
     return a;
 }
 
@@ -1409,7 +1443,7 @@ void do_ll(tmt_handle* h, double* d_out)
         k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(
             reinterpret_cast<const float*>(h->d_ndk), h->D, K, h->d_lg_alpha, h->d_alpha, (const float*)h->d_doc_wlen,
             h->d_asum_ll, reinterpret_cast<const float*>(h->d_nkw[0]), h->cfg.V, eta, std::lgamma(eta), h->d_partials,
-            h->prior_args());
+            h->prior_args(), h->d_alpha_rows, h->d_arow, h->d_row_asum);
         launch_check(h);
         k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, reinterpret_cast<const float*>(h->d_nk[0]),
                                              K, veta, d_out, h->d_esum);
@@ -1417,7 +1451,8 @@ void do_ll(tmt_handle* h, double* d_out)
         k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
                                                             h->d_doc_len, h->d_asum_ll,
                                                             h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
-                                                            h->d_partials, h->prior_args());
+                                                            h->d_partials, h->prior_args(), h->d_alpha_rows,
+                                                            h->d_arow, h->d_row_asum);
         launch_check(h);
         k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, h->d_nk[h->cur], K, veta, d_out,
                                              h->d_esum);
@@ -1602,6 +1637,10 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
         h->d_prior_idx = nullptr;
         h->d_prior = h->d_esum = h->d_prior_cum = h->d_cum_eta = nullptr;
+        h->d_alpha_rows = nullptr;
+        h->d_arow = nullptr;
+        h->d_row_asum = nullptr;
+        h->d_mask = nullptr;
         if (!h->prior_ids.empty()) {
             // etaByTopicWord as a sparse table (prepareWordPriors, LDAModel.hpp:724-737)
             const uint32_t P = (uint32_t)h->prior_ids.size();
@@ -1902,7 +1941,7 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
             const bool opt = gs >= h->cfg.burn_in && h->cfg.optim_interval && (gs + 1) % h->cfg.optim_interval == 0;
             const bool llp = npts && (i + 1) % ll_every == 0 && pt < npts;
             if (opt || llp) end_run();
-            if (opt) do_optimize(h);
+            if (opt && !h->d_arow) do_optimize(h);   // per-document alphas are the caller's (DMR fits lambda)
             ++h->global_step;
             if (llp) do_ll(h, h->d_ll + 2 * pt++);
         }
@@ -2001,6 +2040,52 @@ tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k
         const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
         if (kv) CK(cudaMemcpyAsync(h->d_nkw[h->cur], n_kw, kv * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_nk[h->cur], n_k, h->cfg.K * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_set_doc_topic_mask(tmt_handle* h, const uint32_t* mask_bits)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_doc_topic_mask before the corpus was uploaded");
+        if (h->world > 1) throw ArgError("per-document masks on a corpus sharded across GPUs are not supported");
+        h->drop_graphs();
+        if (!mask_bits) { h->d_mask = nullptr; return; }
+        const uint64_t mw = (h->cfg.K + 31) / 32;
+        if (!h->d_mask) h->d_mask = h->dalloc<uint32_t>(std::max<uint64_t>(1, h->D * mw));
+        if (h->D) CK(cudaMemcpyAsync(h->d_mask, mask_bits, h->D * mw * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+tmt_status tmt_set_doc_alpha(tmt_handle* h, uint32_t M, const float* alpha_rows, const uint32_t* doc_row)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_doc_alpha before the corpus was uploaded");
+        if (h->world > 1) throw ArgError("per-document alphas on a corpus sharded across GPUs are not supported");
+        h->drop_graphs();
+        if (!alpha_rows) { h->d_arow = nullptr; h->d_alpha_rows = nullptr; h->d_row_asum = nullptr; return; }
+        const uint32_t K = h->cfg.K;
+        if (M == 0 || !doc_row) throw ArgError("alpha rows need M > 0 and doc_row");
+        for (uint64_t i = 0; i < (uint64_t)M * K; ++i)
+            if (!(alpha_rows[i] > 0.f) || !std::isfinite(alpha_rows[i])) throw ArgError("alphas must be finite and > 0");
+        for (uint64_t d = 0; d < h->D; ++d)
+            if (doc_row[d] >= M) throw ArgError("doc_row[" + std::to_string(d) + "] >= M");
+        std::vector<double> ras(2 * (size_t)M);
+        for (uint32_t m = 0; m < M; ++m) {
+            double sd = 0;
+            for (uint32_t k = 0; k < K; ++k) sd += (double)alpha_rows[(uint64_t)m * K + k];
+            ras[2 * m] = sd;
+            ras[2 * m + 1] = std::lgamma(sd);
+        }
+        h->d_alpha_rows = h->dalloc<float>((uint64_t)M * K);
+        h->d_row_asum = h->dalloc<double>(2 * (size_t)M);
+        if (!h->d_arow) h->d_arow = h->dalloc<uint32_t>(std::max<uint64_t>(1, h->D));
+        CK(cudaMemcpyAsync(h->d_alpha_rows, alpha_rows, (uint64_t)M * K * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_row_asum, ras.data(), ras.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        if (h->D) CK(cudaMemcpyAsync(h->d_arow, doc_row, h->D * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     });
 }
@@ -2315,7 +2400,7 @@ tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, co
     const double etad = (double)eta;
     k_ll_prep<<<1, 256, 0, st>>>(alpha, K, lg_alpha, asum);
     k_ll_partials<<<blocks, 256, 0, st>>>(n_dk, D, K, lg_alpha, alpha, doc_len, asum, n_kw, V, etad,
-                                          std::lgamma(etad), partials, PriorArgs{});
+                                          std::lgamma(etad), partials, PriorArgs{}, nullptr, nullptr, nullptr);
     k_ll_final<<<1, 256, 0, st>>>(partials, blocks, n_k, K, (double)V * etad, ll_out, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));

@@ -80,6 +80,29 @@ class Engine:
         self._prior_ids, self._prior = ids, pr
         check(lib.tmt_set_word_priors(self.h, len(ids), _p(ids), _p(pr)), self.h)
 
+    def set_doc_topic_mask(self, mask):
+        """tmt_set_doc_topic_mask from a boolean D x K array (None clears):
+        topic k is allowed in document d where mask[d, k]."""
+        if mask is None:
+            check(lib.tmt_set_doc_topic_mask(self.h, None), self.h)
+            return
+        m = np.asarray(mask, dtype=bool)
+        mw = (self.K + 31) // 32
+        bits = np.zeros((self.D, mw * 32), dtype=bool)
+        bits[:, :self.K] = m
+        words = np.packbits(bits.reshape(self.D, mw, 32)[:, :, ::-1], axis=2, bitorder="big")
+        self._mask = np.ascontiguousarray(words.view(">u4").reshape(self.D, mw).astype(np.uint32))
+        check(lib.tmt_set_doc_topic_mask(self.h, _p(self._mask)), self.h)
+
+    def set_doc_alpha(self, rows, doc_row):
+        """tmt_set_doc_alpha: alpha rows (M x K) and each document's row (None clears)."""
+        if rows is None:
+            check(lib.tmt_set_doc_alpha(self.h, 0, None, None), self.h)
+            return
+        self._arows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, self.K)
+        self._arow = np.ascontiguousarray(doc_row, dtype=np.uint32)
+        check(lib.tmt_set_doc_alpha(self.h, len(self._arows), _p(self._arows), _p(self._arow)), self.h)
+
     def set_graphs(self, enable):
         """Sweeps as CUDA graph launches after the autotuner's first sweeps
         (default) or as separate kernel launches; results are identical."""
