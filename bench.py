@@ -512,6 +512,10 @@ def main():
             args.config = "c4"
         return run_infer(args)
     args.warmup = max(args.warmup, 3)
+    if args.mode == "train":
+        # the engine's autotuner runs its first 6 sweeps eagerly, timing each
+        # sweep-kernel variant twice per document group; the warm-up covers them
+        args.warmup = max(args.warmup, 6)
     w = dict(WORKLOADS[args.config])
     if args.docs:
         w["D"] = args.docs
@@ -619,6 +623,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
             "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1) * world,
                        "tokens": N_all_ranks, "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups),
+                       "sweep_variants": eng.sweep_variants() if hasattr(eng, "sweep_variants") else None,
                        "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
                                        if world > 1 else "dp1"),
                        "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},

@@ -222,6 +222,9 @@ tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_i
  * nothing in tomotopy: the loop it captures is TopicModel::train's
  * (TopicModel.hpp:684-755) iteration over trainOne. */
 tmt_status tmt_set_graphs(tmt_handle* h, int32_t enable);
+/* The sweep-kernel variant the autotuner chose for each document group
+ * (-1 while tuning); *n = the number of groups.  Diagnostics only. */
+tmt_status tmt_get_sweep_variants(const tmt_handle* h, int32_t* out, uint32_t cap, uint32_t* n);
 
 /* Weighted counts (tmt_upload_corpus_weighted): n_dk (D x K row-major),
  * n_kw (V x K, column v = K floats: numByTopicWord of ModelStateLDA<float>),

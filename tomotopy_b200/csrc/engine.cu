@@ -375,13 +375,20 @@ k_sweep_doc(SweepArgs a)
 
     // a token's word weights, the table's own-topic entry phu and the own
     // topic's weight with the token removed, phio (w: the token's weight)
-    auto load_word = [&](uint32_t v, int zo, float w, float4 (&pv)[CHR], float& phu, float& phio) {
+    // A word's weights: this lane's blocks of four of its table column.  A
+    // document's tokens are sorted by word, so about 40% of the tokens of the
+    // benchmark corpora repeat the previous token's word: the column stays in
+    // registers (the table is the group's snapshot, so it cannot change).
+    auto load_col = [&](uint32_t v, float4 (&pv)[CHR]) {
         const float* ph = a.phi + (uint64_t)v * KP;
         if (CH > 0) {
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
+    };
+    auto load_word = [&](uint32_t v, int zo, float w, float& phu, float& phio) {
+        const float* ph = a.phi + (uint64_t)v * KP;
         const CT nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
         const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
         phu = __ldg(ph + zo);
@@ -401,6 +408,8 @@ k_sweep_doc(SweepArgs a)
         }
     };
 
+    float4 pv[CHR];                      // the column of word v_have (see load_col)
+    uint32_t v_have = 0xFFFFFFFFu;
     for (;;) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
@@ -447,19 +456,25 @@ k_sweep_doc(SweepArgs a)
                 vm &= vm - 1;
                 uint32_t v = __shfl_sync(FULL, my_w, j);
                 int zo = (int)__shfl_sync(FULL, my_z, j);
-                float4 pv[CHR];
+                if (v != v_have) {
+                    load_col(v, pv);
+                    v_have = v;
+                }
                 float phu, phi_own;
-                load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, pv, phu, phi_own);
+                load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phu, phi_own);
                 for (;;) {
                     const int jn = vm ? __ffs(vm) - 1 : -1;
                     uint32_t vn = 0;
                     int zon = 0;
                     float4 pvn[CHR];
                     float phun = 0.f, phion = 0.f;
+                    bool new_col = false;
                     if (PF && jn >= 0) {
                         vn = __shfl_sync(FULL, my_w, jn);
                         zon = (int)__shfl_sync(FULL, my_z, jn);
-                        load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, pvn, phun, phion);
+                        new_col = vn != v;
+                        if (new_col) load_col(vn, pvn);
+                        load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, phun, phion);
                     }
                     const float u = __shfl_sync(FULL, my_u, j);
                     const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
@@ -607,16 +622,23 @@ k_sweep_doc(SweepArgs a)
                     j = jn;
                     vm &= vm - 1;
                     if (PF) {
+                        if (new_col) {
+#pragma unroll
+                            for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
+                            v_have = vn;
+                        }
                         v = vn;
                         zo = zon;
-#pragma unroll
-                        for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
                         phu = phun;
                         phi_own = phion;
                     } else {
                         v = __shfl_sync(FULL, my_w, j);
                         zo = (int)__shfl_sync(FULL, my_z, j);
-                        load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, pv, phu, phi_own);
+                        if (v != v_have) {
+                            load_col(v, pv);
+                            v_have = v;
+                        }
+                        load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phu, phi_own);
                     }
                 }
             }
@@ -933,8 +955,12 @@ struct tmt_handle {
     double* d_row_asum = nullptr;    // M x 2: sum of a row, lgamma of it
     uint32_t* d_mask = nullptr;      // D x ceil(K/32)
     // sweep-kernel autotuner: variants give bit-identical results, so the
-    // first sweeps each time one variant and the fastest is kept
+    // first sweeps each time one variant and the fastest is kept.  With
+    // several variants they run in the order 0, 1, .., n-1, n-1, .., 0 and
+    // each group sums its two timings: sweep times still fall over the first
+    // sweeps, and the mirrored order cancels a linear drift.
     int variant = 0;                 // the variant of the sweep being tuned
+    int tune_step = 0;
     int n_variants = 1;
     int tuned = -1;                  // 0 once every group has its variant, -1 while tuning
     std::vector<int> group_variant;  // per document group, the fastest variant
@@ -1684,9 +1710,10 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
             h->n_variants = round4(K) <= 4096 ? 3 : 1;
             h->variant = 0;
+            h->tune_step = 0;
             h->tuned = -1;
             h->group_variant.assign(G, 0);
-            h->group_ms.assign(G, {});
+            h->group_ms.assign(G, std::vector<float>(h->n_variants, 0.f));
             while (h->gev.size() < 2 * (size_t)G) {
                 cudaEvent_t e;
                 CK(cudaEventCreate(&e));
@@ -1923,17 +1950,20 @@ tmt_status tmt_train(tmt_handle* h, uint32_t iters, uint32_t ll_every, double* l
                         if (h->group_bounds[g] == h->group_bounds[g + 1]) continue;
                         float gm = 0.f;
                         CK(cudaEventElapsedTime(&gm, h->gev[2 * g], h->gev[2 * g + 1]));
-                        h->group_ms[g].push_back(gm);
+                        h->group_ms[g][h->variant] += gm;
                     }
-                    if (++h->variant >= h->n_variants) {
+                    const int nv = h->n_variants;
+                    const int steps = nv > 1 ? 2 * nv : 1;
+                    if (++h->tune_step >= steps) {
                         for (uint32_t g = 0; g < G; ++g) {
                             const auto& v = h->group_ms[g];
-                            h->group_variant[g] =
-                                v.empty() ? 0 : (int)(std::min_element(v.begin(), v.end()) - v.begin());
+                            h->group_variant[g] = (int)(std::min_element(v.begin(), v.end()) - v.begin());
                         }
                         h->variant = 0;
                         h->tuned = 0;
                         h->drop_graphs();
+                    } else {
+                        h->variant = h->tune_step < nv ? h->tune_step : 2 * nv - 1 - h->tune_step;
                     }
                 }
             }
@@ -2155,6 +2185,15 @@ tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed)
     if (!h) return TMT_ERR_INVALID_ARGUMENT;
     h->cfg.seed = seed;
     return guarded(h, [&] { h->drop_graphs(); });   // the seed is an argument of the captured launches
+}
+
+tmt_status tmt_get_sweep_variants(const tmt_handle* h, int32_t* out, uint32_t cap, uint32_t* n)
+{
+    if (!h || !n) return TMT_ERR_INVALID_ARGUMENT;
+    *n = (uint32_t)h->group_variant.size();
+    if (out)
+        for (uint32_t g = 0; g < *n && g < cap; ++g) out[g] = h->tuned < 0 ? -1 : h->group_variant[g];
+    return TMT_OK;
 }
 
 tmt_status tmt_set_graphs(tmt_handle* h, int32_t enable)

@@ -103,6 +103,14 @@ class Engine:
         self._arow = np.ascontiguousarray(doc_row, dtype=np.uint32)
         check(lib.tmt_set_doc_alpha(self.h, len(self._arows), _p(self._arows), _p(self._arow)), self.h)
 
+    def sweep_variants(self):
+        """The autotuner's sweep-kernel variant per document group (-1 while tuning)."""
+        n = C.c_uint32()
+        check(lib.tmt_get_sweep_variants(self.h, None, 0, C.byref(n)), self.h)
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        check(lib.tmt_get_sweep_variants(self.h, _p(out), n.value, C.byref(n)), self.h)
+        return out[:n.value].tolist()
+
     def set_graphs(self, enable):
         """Sweeps as CUDA graph launches after the autotuner's first sweeps
         (default) or as separate kernel launches; results are identical."""
