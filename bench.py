@@ -578,6 +578,7 @@ def main():
     eng.train(args.steps)
     wall = time.perf_counter() - t0
     info = eng.info()
+    variants = eng.sweep_variants() if hasattr(eng, "sweep_variants") else None
     launches = info.kernel_launches - launches0
     clk = clocks.stop()
     kernel_ms = info.sweep_kernel_ms / max(info.sweeps_timed, 1)
@@ -623,7 +624,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
             "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1) * world,
                        "tokens": N_all_ranks, "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups),
-                       "sweep_variants": eng.sweep_variants() if hasattr(eng, "sweep_variants") else None,
+                       "sweep_variants": variants,
                        "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
                                        if world > 1 else "dp1"),
                        "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},
