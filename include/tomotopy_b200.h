@@ -294,6 +294,11 @@ tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out);
 tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
                                 const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id);
 /* Queues one document (ids in the model's vocabulary); returns at once. */
+/* Word priors of a resident model (tmt_set_word_priors' table: word_ids[p] < V
+ * gets the K-vector priors[p*K ..] as its eta column); only before the model's
+ * first request (TMT_ERR_STATE after). */
+tmt_status tmt_server_set_model_priors(tmt_server* s, uint32_t model_id, uint32_t P, const uint32_t* word_ids,
+                                       const float* priors);
 tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* wid, uint32_t len, uint32_t iters,
                              uint64_t seed, uint64_t key, uint64_t* request_id);
 /* Waits up to wait_ms for a finished document; TMT_ERR_TIMEOUT when none.

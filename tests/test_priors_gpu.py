@@ -144,3 +144,6 @@ def test_word_prior_model_api(tmp_path):
     np.testing.assert_array_equal(m2.docs[5].topics, mdl.docs[5].topics)
     t, _ = mdl.infer(mdl.make_doc(["w1", "w1", "w2", "w7"]), iterations=20)
     assert abs(t.sum() - 1) < 1e-4
+    ts, ll = mdl.infer([mdl.make_doc(["w1", "w1", "w2", "w7"]), mdl.make_doc(["w1", "w3"])], iterations=20,
+                       together=True)
+    assert np.isfinite(ll) and all(abs(x.sum() - 1) < 1e-4 for x in ts)

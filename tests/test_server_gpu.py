@@ -152,3 +152,34 @@ def test_batch_submit_and_poll():
     st = srv.stats()
     assert st.kernel_ms > 0 and st.busy_ms >= st.kernel_ms * 0.5 and st.token_sweeps > 0
     srv.close()
+
+
+def test_served_model_with_word_priors():
+    """A resident model with word priors: served results equal tmt_infer_batch
+    on the engine holding the same priors; priors are refused once the model
+    has served a request."""
+    off, w = T.synth_corpus(600, 8, 120, ("poisson", 70, 1, 700), seed=5)
+    off, w, Vr, _ = T.prepare_ids(off, w)
+    K = 24
+    ids = np.array([0, 3, 7], np.uint32)
+    pr = np.full((3, K), 0.01, np.float32)
+    pr[0, :] = 0.0
+    pr[0, 2] = 1.0
+    pr[1, 5:9] = 0.3
+    eng = T.Engine(K, Vr, alpha=0.1, eta=0.01, seed=5, optim_interval=0)
+    eng.set_word_priors(ids, pr)
+    eng.upload(off, w)
+    eng.train(10)
+    ds = docs(eng.V, 20, seed=8)
+    keys = np.arange(20, dtype=np.uint64)
+    theta, ll = batch_ref(eng, ds, 25, 3, keys)
+    srv = T.Server(max_slots=8, token_budget=4000, step_token_sweeps=300, max_doc_len=1000)
+    mid = srv.add_engine_model(eng)
+    rids = [srv.submit(mid, d, iters=25, seed=3, key=int(k)) for d, k in zip(ds, keys)]
+    out = drain(srv, len(rids))
+    for i, rid in enumerate(rids):
+        np.testing.assert_array_equal(out[rid][2], theta[i])
+        assert out[rid][3] == ll[i]
+    with pytest.raises(TmtError):
+        srv.set_model_priors(mid, ids, pr)
+    srv.close()

@@ -34,6 +34,7 @@
 #include "special.cuh"
 #include "common.cuh"
 #include "infer.cuh"
+#include "priors.h"
 #include "../../include/tomotopy_b200.h"
 
 namespace {
@@ -131,7 +132,7 @@ __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* _
 // next state, which the sweep then updates with the count deltas.
 __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __restrict__ nk, uint32_t V, uint32_t K,
                            uint32_t KP, float eta, float veta, float* __restrict__ phi, int32_t* __restrict__ nkw_next,
-                           int32_t* __restrict__ nk_next, uint32_t smem_k, PriorArgs pr)
+                           int32_t* __restrict__ nk_next, uint32_t smem_k, PriorArgs pr, float* __restrict__ rm1)
 {
     extern __shared__ float s_R[];
     const bool r_smem = K <= smem_k;
@@ -139,7 +140,10 @@ __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __res
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
             s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
     if (blockIdx.x == 0)
-        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) nk_next[k] = nk[k];
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+            nk_next[k] = nk[k];
+            rm1[k] = __fdiv_rn(1.0f, __fadd_rn((float)(nk[k] - 1), esum_of(pr, k, veta)));
+        }
     __syncthreads();
     for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
         const int32_t* src = nkw + v * K;
@@ -172,13 +176,16 @@ __global__ void k_nk_apply(int32_t* __restrict__ nk, int32_t* __restrict__ dnk, 
 
 __global__ void k_phi_apply(int32_t* __restrict__ nkw, int32_t* __restrict__ delta, const int32_t* __restrict__ nk,
                             uint32_t V, uint32_t K, uint32_t KP, float eta, float veta, float* __restrict__ phi,
-                            uint32_t smem_k, int fold, PriorArgs pr)
+                            uint32_t smem_k, int fold, PriorArgs pr, float* __restrict__ rm1)
 {
     extern __shared__ float s_R[];
     const bool r_smem = phi && K <= smem_k;
     if (r_smem)
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
             s_R[k] = __fdiv_rn(1.0f, __fadd_rn((float)nk[k], esum_of(pr, k, veta)));
+    if (phi && rm1 && blockIdx.x == 0)
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            rm1[k] = __fdiv_rn(1.0f, __fadd_rn((float)(nk[k] - 1), esum_of(pr, k, veta)));
     __syncthreads();
     for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
         int32_t* col = nkw + v * K;
@@ -310,6 +317,9 @@ struct SweepArgs {
     long long* dkw;           // V x K
     long long* dk;            // K
     PriorArgs pr;             // word priors (all NULL: none)
+    // integer counts: rm1[k] = 1 / ((float)(n_k[k] - 1) + esum_k), the own
+    // topic's reciprocal, built with the group's word table (NULL: divide)
+    const float* rm1;
     // per-document conditionals of the derived models (all NULL: none):
     // A_k = ((float)n_dk + alpha_dk) * m_dk
     const float* alpha_rows;  // M x K
@@ -390,21 +400,28 @@ k_sweep_doc(SweepArgs a)
     auto load_word = [&](uint32_t v, int zo, float w, float& phu, float& phio) {
         const float* ph = a.phi + (uint64_t)v * KP;
         const CT nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
-        const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
         phu = __ldg(ph + zo);
-        float eo = eta, so = veta;
+        float eo = eta;
         if (a.pr.idx) {
             const float* pe = prior_col(a.pr, v, K);
             if (pe) eo = __ldg(pe + zo);
-            so = __ldg(a.pr.esum + zo);
         }
+        auto so = [&]() { return a.pr.idx ? __ldg(a.pr.esum + zo) : veta; };
         if constexpr (WT) {
+            const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
             float co = __fsub_rn(nkw_o, w), no = __fsub_rn(nk_o, w);
             co = co > 0.f ? co : 0.f;
             no = no > 0.f ? no : 0.f;
-            phio = __fmul_rn(__fadd_rn(co, eo), __fdiv_rn(1.0f, __fadd_rn(no, so)));
+            phio = __fmul_rn(__fadd_rn(co, eo), __fdiv_rn(1.0f, __fadd_rn(no, so())));
         } else {
-            phio = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eo), __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), so)));
+            float rinv;
+            if (a.rm1) {
+                rinv = __ldg(a.rm1 + zo);
+            } else {
+                const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
+                rinv = __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), so()));
+            }
+            phio = __fmul_rn(__fadd_rn((float)(nkw_o - 1), eo), rinv);
         }
     };
 
@@ -518,6 +535,16 @@ k_sweep_doc(SweepArgs a)
                     if (lane == ((zo >> 2) & 31)) {   // the own topic: exclude the token from n_kw, n_k
                         const float Ao = rowf[zo];
                         s = fmaxf(__fadd_rn(__fsub_rn(s, __fmul_rn(Ao, phu)), __fmul_rn(Ao, phi_own)), 0.f);
+                    }
+                    // without the prefetch registers: above 256 topics pass 1 was the column's
+                    // last use (pass 2 reads the table), so the next token's column loads now,
+                    // behind this token's scans and draw
+                    if (!PF && CH >= 4 && jn >= 0) {
+                        const uint32_t vnx = __shfl_sync(FULL, my_w, jn);
+                        if (vnx != v_have) {
+                            load_col(vnx, pv);
+                            v_have = vnx;
+                        }
                     }
                     // lanes at or above min(32, ceil(K/4)) hold no topics: a Hillis-Steele
                     // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
@@ -923,6 +950,7 @@ struct tmt_handle {
     int32_t* d_nkw[2] = { nullptr, nullptr };
     int32_t* d_nk[2] = { nullptr, nullptr };
     float* d_phi = nullptr;          // per-word topic weights of the current snapshot
+    float* d_rm1 = nullptr;          // K: the own topic's reciprocal of the snapshot
     uint32_t groups = 1;             // document groups per sweep
     std::vector<uint64_t> group_bounds;   // doc_order positions: group g = [b[g], b[g+1])
     // a corpus sharded across GPUs (tmt_upload_shard); world == 1: this GPU holds all of it
@@ -1231,6 +1259,7 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.pos_end = pos_end;
     a.tok_offset = h->tok_offset;
     a.pr = h->prior_args();
+    a.rm1 = h->weighted ? nullptr : h->d_rm1;
     a.alpha_rows = h->d_alpha_rows;
     a.arow = h->d_arow;
     a.mask = h->d_mask;
@@ -1263,7 +1292,8 @@ void do_sweep_sharded(tmt_handle* h)
             launch_check(h);
         }
         k_phi_apply<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta,
-                                                        veta, h->d_phi, smem_k, pending ? 1 : 0, h->prior_args());
+                                                        veta, h->d_phi, smem_k, pending ? 1 : 0, h->prior_args(),
+                                                        h->d_rm1);
         launch_check(h);
         if (h->group_bounds[g] < h->group_bounds[g + 1]) {
             CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
@@ -1279,7 +1309,7 @@ void do_sweep_sharded(tmt_handle* h)
         k_nk_apply<<<1, 1024, 0, h->stream>>>(h->d_nk[0], dnk, K);
         launch_check(h);
         k_phi_apply<<<grid, 256, 0, h->stream>>>(h->d_nkw[0], dnkw, h->d_nk[0], V, K, round4(K), h->cfg.eta, veta,
-                                                nullptr, 0, 1, h->prior_args());
+                                                nullptr, 0, 1, h->prior_args(), nullptr);
         launch_check(h);
     }
     CK(cudaEventRecord(h->kev1, h->stream));
@@ -1360,7 +1390,7 @@ void do_sweep(tmt_handle* h, bool capture = false)
         uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
         k_phi_copy<<<grid, 256, smem_k * 4, h->stream>>>(h->d_nkw[cur], h->d_nk[cur], V, K, round4(K), h->cfg.eta,
                                                         veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k,
-                                                        h->prior_args());
+                                                        h->prior_args(), h->d_rm1);
         launch_check(h);
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
         SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
@@ -1661,6 +1691,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             h->d_nk[1] = h->dalloc<int32_t>(K);
         }
         h->d_phi = h->dalloc<float>((uint64_t)round4(K) * V);
+        h->d_rm1 = h->dalloc<float>(K);
         h->d_prior_idx = nullptr;
         h->d_prior = h->d_esum = h->d_prior_cum = h->d_cum_eta = nullptr;
         h->d_alpha_rows = nullptr;
@@ -1670,27 +1701,12 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         if (!h->prior_ids.empty()) {
             // etaByTopicWord as a sparse table (prepareWordPriors, LDAModel.hpp:724-737)
             const uint32_t P = (uint32_t)h->prior_ids.size();
-            std::vector<int32_t> idx(V, -1);
-            for (uint32_t p = 0; p < P; ++p) idx[h->prior_ids[p]] = (int32_t)p;
-            std::vector<float> esum(K), pcum((uint64_t)P * K), ecum(K);
-            // the row sums of etaByTopicWord in double, rounded once: (V - P) * eta,
-            // then the prior words' values in ascending word id
-            std::vector<uint32_t> by_id(h->prior_ids.begin(), h->prior_ids.end());
-            std::sort(by_id.begin(), by_id.end());
-            for (uint32_t k = 0; k < K; ++k) {
-                double sd = (double)(V - P) * (double)h->cfg.eta;
-                for (uint32_t v : by_id) sd += (double)h->prior_vals[(uint64_t)idx[v] * K + k];
-                esum[k] = (float)sd;
-            }
-            for (uint32_t p = 0; p < P; ++p) {
-                float acc = 0.f;
-                for (uint32_t k = 0; k < K; ++k) {
-                    acc = acc + h->prior_vals[(uint64_t)p * K + k];
-                    pcum[(uint64_t)p * K + k] = acc;
-                }
-            }
-            float acc = 0.f;
-            for (uint32_t k = 0; k < K; ++k) { acc = acc + h->cfg.eta; ecum[k] = acc; }
+            PriorTables t;
+            build_prior_tables(K, V, h->cfg.eta, h->prior_ids, h->prior_vals, t);
+            const std::vector<int32_t>& idx = t.idx;
+            const std::vector<float>& esum = t.esum;
+            const std::vector<float>& pcum = t.pcum;
+            const std::vector<float>& ecum = t.ecum;
             h->d_prior_idx = h->dalloc<int32_t>(V);
             h->d_prior = h->dalloc<float>((uint64_t)P * K);
             h->d_esum = h->dalloc<float>(K);

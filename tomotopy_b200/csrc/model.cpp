@@ -350,16 +350,23 @@ struct tmt_model {
 
     // prepareWordPriors (LDAModel.hpp:724-737): the prior words still in the
     // vocabulary (id < realV) get their columns
-    void apply_word_priors()
+    void prior_table(std::vector<uint32_t>& ids, std::vector<float>& vals) const
     {
-        std::vector<uint32_t> ids;
-        std::vector<float> vals;
+        ids.clear();
+        vals.clear();
         for (auto& e : etaByWord) {
             auto it = dict.find(e.first);
             if (it == dict.end() || it->second >= realV) continue;
             ids.push_back(it->second);
             vals.insert(vals.end(), e.second.begin(), e.second.end());
         }
+    }
+
+    void apply_word_priors()
+    {
+        std::vector<uint32_t> ids;
+        std::vector<float> vals;
+        prior_table(ids, vals);
         check(tmt_set_word_priors(eng, (uint32_t)ids.size(), ids.data(), vals.data()));
     }
 
@@ -1138,6 +1145,12 @@ tmt_status tmt_model_infer_together(tmt_model* m, const char* words, const uint6
             if (s2 != TMT_OK) throw EngineErr(s2, tmp ? tmt_last_error(tmp) : "tmt_create failed");
         }
         auto ck = [&](tmt_status s2) { if (s2 != TMT_OK) throw EngineErr(s2, tmt_last_error(tmp)); };
+        {   // the model's word priors apply to the private state too
+            std::vector<uint32_t> pids;
+            std::vector<float> pvals;
+            m->prior_table(pids, pvals);
+            ck(tmt_set_word_priors(tmp, (uint32_t)pids.size(), pids.data(), pvals.data()));
+        }
         if (m->tw) {
             // weighted: the new documents' weights; the private state adds the
             // model's float counts to the documents' (float adds)

@@ -25,6 +25,7 @@
 #include <vector>
 #include "common.cuh"
 #include "infer.cuh"
+#include "priors.h"
 #include "philox.cuh"
 #include "../../include/tomotopy_b200.h"
 
@@ -158,6 +159,13 @@ struct Model {
     double* d_ll = nullptr;
     uint32_t* d_work = nullptr;
     uint32_t* d_counter = nullptr;
+    // word priors (tmt_server_set_model_priors; all NULL: none)
+    int32_t* d_pidx = nullptr;
+    float* d_pval = nullptr;
+    float* d_esum = nullptr;
+    float* d_pcum = nullptr;
+    float* d_ecum = nullptr;
+    bool used = false;                  // a request was submitted: the model is frozen
 };
 
 } // namespace
@@ -352,6 +360,11 @@ bool server_step(tmt_server* s)
         a.work = m->d_work;
         a.n_work = (uint32_t)work.size();
         a.counter = m->d_counter;
+        a.pidx = m->d_pidx;
+        a.pval = m->d_pval;
+        a.esum = m->d_esum;
+        a.pcum = m->d_pcum;
+        a.ecum = m->d_ecum;
         // every request of a model shares the draw key base; the per-request seed is folded in below
         a.key = 0;
         // requests may carry different seeds: launch per distinct seed (usually one)
@@ -589,6 +602,51 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
     return TMT_OK;
 }
 
+tmt_status tmt_server_set_model_priors(tmt_server* s, uint32_t model_id, uint32_t P, const uint32_t* word_ids,
+                                       const float* priors)
+{
+    if (!s || (P && (!word_ids || !priors))) return TMT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (model_id >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
+    Model* m = s->models[model_id].get();
+    if (m->used) return TMT_ERR_STATE;           // only before the model's first request
+    const uint32_t K = m->K, V = m->V;
+    std::vector<uint8_t> seen(V, 0);
+    for (uint32_t p = 0; p < P; ++p) {
+        if (word_ids[p] >= V || seen[word_ids[p]]++) return TMT_ERR_INVALID_ARGUMENT;
+        for (uint32_t k = 0; k < K; ++k)
+            if (!(priors[(uint64_t)p * K + k] >= 0.f) || !std::isfinite(priors[(uint64_t)p * K + k]))
+                return TMT_ERR_INVALID_ARGUMENT;
+    }
+    if (P == 0) {
+        m->d_pidx = nullptr;
+        m->d_pval = m->d_esum = m->d_pcum = m->d_ecum = nullptr;
+        return TMT_OK;
+    }
+    try {
+        CK(cudaSetDevice(s->device));
+        std::vector<uint32_t> ids(word_ids, word_ids + P);
+        std::vector<float> vals(priors, priors + (uint64_t)P * K);
+        PriorTables t;
+        build_prior_tables(K, V, m->eta, ids, vals, t);
+        m->d_pidx = s->dalloc<int32_t>(V);
+        m->d_pval = s->dalloc<float>((uint64_t)P * K);
+        m->d_esum = s->dalloc<float>(K);
+        m->d_pcum = s->dalloc<float>((uint64_t)P * K);
+        m->d_ecum = s->dalloc<float>(K);
+        CK(cudaMemcpy(m->d_pidx, t.idx.data(), V * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_pval, vals.data(), (uint64_t)P * K * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_esum, t.esum.data(), K * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_pcum, t.pcum.data(), (uint64_t)P * K * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_ecum, t.ecum.data(), K * sizeof(float), cudaMemcpyHostToDevice));
+    } catch (const OomError&) {
+        return TMT_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return TMT_ERR_CUDA;
+    }
+    return TMT_OK;
+}
+
 tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* wid, uint32_t len, uint32_t iters,
                              uint64_t seed, uint64_t key, uint64_t* request_id)
 {
@@ -605,6 +663,7 @@ tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* w
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
         if (model_id >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
+        s->models[model_id]->used = true;
         r.model = model_id;
         r.id = s->next_id++;
         *request_id = r.id;
@@ -662,6 +721,7 @@ tmt_status tmt_server_submit_batch(tmt_server* s, const uint32_t* model_ids, con
         for (uint64_t d = 0; d < n; ++d) {
             Request& r = rs[d];
             r.model = model_ids[d];
+            s->models[r.model]->used = true;
             r.id = s->next_id++;
             r.t_submit = now;
             request_ids[d] = r.id;

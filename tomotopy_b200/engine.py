@@ -242,12 +242,23 @@ class Server:
         return mid.value
 
     def add_engine_model(self, eng):
-        """A trained engine's frozen state; integer counts without word priors
-        (the served pool infers with the scalar eta)."""
-        if getattr(eng, "weighted", False) or len(getattr(eng, "_prior_ids", ())):
-            raise ValueError("the served pool takes integer-count models without word priors")
+        """A trained engine's frozen state, with its word priors; integer counts
+        only (the served pool has no weighted inference)."""
+        if getattr(eng, "weighted", False):
+            raise ValueError("the served pool takes integer-count models")
         _, nkw, nk, alpha = eng.state()
-        return self.add_model(eng.K, eng.V, alpha, eng.eta, nkw, nk)
+        mid = self.add_model(eng.K, eng.V, alpha, eng.eta, nkw, nk)
+        ids = getattr(eng, "_prior_ids", None)
+        if ids is not None and len(ids):
+            self.set_model_priors(mid, ids, eng._prior)
+        return mid
+
+    def set_model_priors(self, model_id, word_ids, priors):
+        """tmt_server_set_model_priors, before the model's first request."""
+        ids = np.ascontiguousarray(word_ids, dtype=np.uint32)
+        pr = np.ascontiguousarray(priors, dtype=np.float32)
+        check(lib.tmt_server_set_model_priors(self.h, int(model_id), len(ids), _p(ids), _p(pr)), None,
+              "tmt_server_set_model_priors")
 
     def submit(self, model_id, words, iters=100, seed=0, key=0):
         w = np.ascontiguousarray(words, dtype=np.uint32)
