@@ -294,6 +294,18 @@ tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out);
 tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
                                 const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id);
 /* Queues one document (ids in the model's vocabulary); returns at once. */
+/* tmt_server_add_model for a model with weighted counts (TermWeight IDF /
+ * PMI: n_kw V x K and n_k K as floats); its requests come through
+ * tmt_server_submit_weighted / tmt_server_submit_batch_weighted, which carry
+ * each token's weight (the same weight for every token of one word in a
+ * document, as the weights of tmt_infer_batch_weighted). */
+tmt_status tmt_server_add_model_f32(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
+                                    const float* n_kw, const float* n_k, uint32_t* model_id);
+tmt_status tmt_server_submit_weighted(tmt_server* s, uint32_t model_id, const uint32_t* wid, const float* weights,
+                                      uint32_t len, uint32_t iters, uint64_t seed, uint64_t key, uint64_t* request_id);
+tmt_status tmt_server_submit_batch_weighted(tmt_server* s, const uint32_t* model_ids, const uint32_t* wid,
+                                            const float* weights, const uint64_t* doc_off, uint64_t n, uint32_t iters,
+                                            uint64_t seed, const uint64_t* keys, uint64_t* request_ids);
 /* Word priors of a resident model (tmt_set_word_priors' table: word_ids[p] < V
  * gets the K-vector priors[p*K ..] as its eta column); only before the model's
  * first request (TMT_ERR_STATE after). */

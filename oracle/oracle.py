@@ -90,6 +90,9 @@ def _load():
         "orc_sweep_doc_live_m_subset": (None, [C.c_uint32, C.c_uint32, V, V, V, V, C.c_float, C.c_uint64,
                                                C.c_uint32] + [V] * 9 + [C.c_uint64]),
         "orc_ll_docs_m_f64": (C.c_double, [C.c_uint64, C.c_uint32, V, V, V, V]),
+        "orc_gibbs_none_w": (None, [C.c_uint64, V, V, V, C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, V]),
+        "orc_gibbs_none_p": (None, [C.c_uint64, V, V, C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, V, V, V,
+                                    V]),
         "orc_infer_doc_w": (C.c_double, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, V, C.c_uint32,
                                          C.c_uint32, C.c_uint64, C.c_uint64, V, V, V]),
     }
@@ -372,6 +375,15 @@ class StateW:
                                                 _ptr(self.z), _ptr(part), len(part))
             lib.orc_fold_w(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), _ptr(dkw), _ptr(dk))
 
+    def gibbs_none(self, iters, rng_state):
+        """tomotopy's sequential sampler with these weights (live float counts)."""
+        st = np.array([rng_state], dtype=np.uint64)
+        c = self.c
+        for _ in range(iters):
+            lib.orc_gibbs_none_w(c.D, _ptr(c.doc_off), _ptr(c.words), _ptr(self.wt), c.V, self.K, _ptr(self.alpha),
+                                 self.eta, _ptr(self.z), _ptr(self.ndk), _ptr(self.nkw), _ptr(self.nk), _ptr(st))
+        return int(st[0])
+
     def optimize_alpha(self):
         lib.orc_optimize_alpha_w(self.c.D, self.K, _ptr(self.ndk), _ptr(self.doc_wlen), _ptr(self.alpha))
 
@@ -439,6 +451,16 @@ class StateP(State):
         b = lib.orc_ll_rest_p_f64(self.K, c.V, _ptr(self.nkw), _ptr(self.nk), self.eta, _ptr(self.pidx),
                                   _ptr(self.prior), _ptr(self.esum))
         return a, b
+
+    def gibbs_none(self, iters, rng_state):
+        """tomotopy's sequential sampler with these word priors."""
+        st = np.array([rng_state], dtype=np.uint64)
+        c = self.c
+        for _ in range(iters):
+            lib.orc_gibbs_none_p(c.D, _ptr(c.doc_off), _ptr(c.words), c.V, self.K, _ptr(self.alpha), self.eta,
+                                 _ptr(self.pidx), _ptr(self.prior), _ptr(self.esum), _ptr(self.z), _ptr(self.ndk),
+                                 _ptr(self.nkw), _ptr(self.nk), _ptr(st))
+        return int(st[0])
 
     def infer_doc(self, nkw, nk, alpha, words, iters, seed, doc_key):
         words = np.ascontiguousarray(words, dtype=np.uint32)

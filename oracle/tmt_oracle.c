@@ -1611,3 +1611,70 @@ double orc_ll_docs_m_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32
     }
     return ll;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The reference's sequential sampler (ParallelScheme::NONE) with weighted    */
+/* counts or word priors: the statistical gate for those paths               */
+/* ------------------------------------------------------------------------ */
+/* Weighted: addWordTo with float weights, decrements clamped at 0
+ * (LDAModel.hpp:287-299, Utils.hpp:132-155); the conditional of
+ * getZLikelihoods (:273-285) in tomotopy's (A*B)/C order. */
+void orc_gibbs_none_w(uint64_t D, const uint64_t* doc_off, const uint32_t* words, const float* wt,
+                      uint32_t V, uint32_t K, const float* alpha, float eta,
+                      uint16_t* z, float* ndk, float* nkw, float* nk, uint64_t* rng_state)
+{
+    float veta = eta * (float)V;
+    float* dist = (float*)malloc(K * sizeof(float));
+    uint64_t* order = (uint64_t*)malloc((D + 1) * sizeof(uint64_t));
+    orc_shuffled_order(D, (size_t)(splitmix64(rng_state) & 0xFFFFFFFFu), order);
+    for (uint64_t j = 0; j < D; ++j) {
+        uint64_t d = order[j];
+        float* row = ndk + d * K;
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            float w = wt[i];
+            uint16_t k0 = z[i];
+            float* col = nkw + (size_t)v * K;
+            row[k0] = fmaxf(row[k0] - w, 0.f);
+            nk[k0] = fmaxf(nk[k0] - w, 0.f);
+            col[k0] = fmaxf(col[k0] - w, 0.f);
+            for (uint32_t k = 0; k < K; ++k) dist[k] = (row[k] + alpha[k]) * (col[k] + eta) / (nk[k] + veta);
+            orc_prefix_sum_sse(dist, (int)K);
+            uint16_t k1 = (uint16_t)orc_sample_acc(dist, K, sm_u01(rng_state));
+            z[i] = k1;
+            row[k1] += w; nk[k1] += w; col[k1] += w;
+        }
+    }
+    free(dist); free(order);
+}
+
+/* Word priors: getZLikelihoods<true> with etaByTopicWord / etaSumByTopic. */
+void orc_gibbs_none_p(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                      uint32_t V, uint32_t K, const float* alpha, float eta,
+                      const int32_t* pidx, const float* prior, const float* esum,
+                      uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk, uint64_t* rng_state)
+{
+    float* dist = (float*)malloc(K * sizeof(float));
+    uint64_t* order = (uint64_t*)malloc((D + 1) * sizeof(uint64_t));
+    orc_shuffled_order(D, (size_t)(splitmix64(rng_state) & 0xFFFFFFFFu), order);
+    for (uint64_t j = 0; j < D; ++j) {
+        uint64_t d = order[j];
+        int32_t* row = ndk + d * K;
+        for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) {
+            uint32_t v = words[i];
+            if (v >= V) continue;
+            uint16_t k0 = z[i];
+            int32_t* col = nkw + (size_t)v * K;
+            const float* pe = pidx[v] >= 0 ? prior + (size_t)pidx[v] * K : NULL;
+            row[k0]--; nk[k0]--; col[k0]--;
+            for (uint32_t k = 0; k < K; ++k)
+                dist[k] = ((float)row[k] + alpha[k]) * ((float)col[k] + (pe ? pe[k] : eta)) / ((float)nk[k] + esum[k]);
+            orc_prefix_sum_sse(dist, (int)K);
+            uint16_t k1 = (uint16_t)orc_sample_acc(dist, K, sm_u01(rng_state));
+            z[i] = k1;
+            row[k1]++; nk[k1]++; col[k1]++;
+        }
+    }
+    free(dist); free(order);
+}

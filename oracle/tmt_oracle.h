@@ -236,6 +236,15 @@ void orc_sweep_doc_live_m_subset(uint32_t K, uint32_t V, const float* alpha, con
 double orc_ll_docs_m_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
                          const float* alpha_rows, const uint32_t* arow);
 
+/* ---- the reference's sequential sampler with weights / word priors ------- */
+void orc_gibbs_none_w(uint64_t D, const uint64_t* doc_off, const uint32_t* words, const float* wt,
+                      uint32_t V, uint32_t K, const float* alpha, float eta,
+                      uint16_t* z, float* ndk, float* nkw, float* nk, uint64_t* rng_state);
+void orc_gibbs_none_p(uint64_t D, const uint64_t* doc_off, const uint32_t* words,
+                      uint32_t V, uint32_t K, const float* alpha, float eta,
+                      const int32_t* pidx, const float* prior, const float* esum,
+                      uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk, uint64_t* rng_state);
+
 #ifdef __cplusplus
 }
 #endif

@@ -147,3 +147,27 @@ def test_word_prior_model_api(tmp_path):
     ts, ll = mdl.infer([mdl.make_doc(["w1", "w1", "w2", "w7"]), mdl.make_doc(["w1", "w3"])], iterations=20,
                        together=True)
     assert np.isfinite(ll) and all(abs(x.sum() - 1) < 1e-4 for x in ts)
+
+
+def test_prior_ll_per_word_matches_reference_sampler():
+    """(d) with word priors: the device's ll_per_word within 1% of tomotopy's
+    sequential sampler with the same etaByTopicWord, averaged over 5 seeds."""
+    off, w = T.synth_corpus(5000, 20, 400, ("poisson", 500, 1, 10000), seed=22)
+    off, w, Vr, _ = T.prepare_ids(off, w)
+    c = O.Corpus(off, w, Vr)
+    K, iters = 20, 150
+    ids = np.arange(0, 40, 2, dtype=np.uint32)                 # 20 frequent words, one pinned per topic
+    pr = np.full((len(ids), K), 0.0, np.float32)
+    pr[np.arange(len(ids)), np.arange(len(ids)) % K] = 1.0
+    gpu, ref = [], []
+    for seed in (1, 2, 3, 4, 5):
+        eng = T.Engine(K, Vr, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
+        eng.set_word_priors(ids, pr)
+        eng.upload(off, w)
+        eng.train(iters)
+        gpu.append(eng.ll_per_word())
+        st = O.StateP(c, K, 0.1, 0.01, seed, ids, pr)
+        st.gibbs_none(iters, seed)
+        ref.append(sum(st.ll_f64()) / c.N)
+    g, r = np.mean(gpu), np.mean(ref)
+    assert abs(g - r) / abs(r) < 0.01, (gpu, ref)

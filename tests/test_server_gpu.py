@@ -183,3 +183,34 @@ def test_served_model_with_word_priors():
     with pytest.raises(TmtError):
         srv.set_model_priors(mid, ids, pr)
     srv.close()
+
+
+def test_served_weighted_model():
+    """A resident model with weighted counts (TermWeight IDF): served results,
+    one by one and in a batch, equal tmt_infer_batch_weighted on the engine."""
+    import oracle as O
+    off, w = T.synth_corpus(600, 8, 150, ("poisson", 70, 1, 700), seed=6)
+    off, w, Vr, _ = T.prepare_ids(off, w, min_cf=1)      # every kept word occurs: finite IDF
+    c = O.Corpus(off, w, Vr)
+    wt, vw = O.weights_idf(c)
+    K = 16
+    eng = T.Engine(K, Vr, alpha=0.1, eta=0.01, seed=6, optim_interval=0)
+    eng.upload(off, w, weights=wt)
+    eng.train(10)
+    ds = docs(eng.V, 24, seed=9)
+    wts = [np.where(d < Vr, vw[np.minimum(d, Vr - 1)], 0).astype(np.float32) for d in ds]
+    keys = np.arange(24, dtype=np.uint64)
+    doff = np.concatenate([[0], np.cumsum([len(d) for d in ds])]).astype(np.uint64)
+    theta, ll = eng.infer(doff, np.concatenate(ds), iters=20, seed=2, doc_keys=keys, weights=np.concatenate(wts))
+    srv = T.Server(max_slots=8, token_budget=4000, step_token_sweeps=300, max_doc_len=1000)
+    mid = srv.add_engine_model(eng)
+    rids = [srv.submit(mid, d, iters=20, seed=2, key=int(k), weights=x) for d, x, k in zip(ds[:12], wts[:12], keys)]
+    rids += list(srv.submit_batch(mid, doff[12:] - doff[12], np.concatenate(ds[12:]), iters=20, seed=2,
+                                  keys=keys[12:], weights=np.concatenate(wts[12:])))
+    out = drain(srv, len(rids))
+    for i, rid in enumerate(rids):
+        np.testing.assert_array_equal(out[int(rid)][2], theta[i])
+        assert out[int(rid)][3] == ll[i]
+    with pytest.raises(ValueError):
+        srv.submit(mid, ds[0], iters=5)                 # a weighted model takes weighted requests only
+    srv.close()

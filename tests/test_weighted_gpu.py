@@ -207,3 +207,26 @@ def test_weighted_model_api(tw, tmp_path):
     mdl.train(10)
     assert m2.global_step == mdl.global_step == 50
     assert m2.ll_per_word * m2._info().weighted_n == pytest.approx(mdl.ll_per_word * mdl.num_words, rel=0.02)
+
+
+@pytest.mark.parametrize("kind", ["idf", "pmi"])
+def test_weighted_ll_per_word_matches_reference_sampler(kind):
+    """(d) for weighted counts: at the same iteration count the device's
+    ll_per_word is within 1% of tomotopy's sequential sampler with the same
+    weights (live float counts, clamped decrements), averaged over 5 seeds."""
+    off, w = T.synth_corpus(5000, 20, 400, ("poisson", 500, 1, 10000), seed=21)
+    off, w, Vr, _ = T.prepare_ids(off, w)
+    c = O.Corpus(off, w, Vr)
+    wt = weights(c, kind)
+    K, iters = 20, 150
+    gpu, ref = [], []
+    for seed in (1, 2, 3, 4, 5):
+        eng = T.Engine(K, Vr, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
+        eng.upload(off, w, weights=wt)
+        eng.train(iters)
+        gpu.append(sum(eng.ll()) / c.N)
+        st = O.StateW(c, K, 0.1, 0.01, seed, wt)
+        st.gibbs_none(iters, seed)
+        ref.append(sum(st.ll_f64()) / c.N)
+    g, r = np.mean(gpu), np.mean(ref)
+    assert abs(g - r) / abs(r) < 0.01, (gpu, ref)

@@ -118,6 +118,10 @@ SIGNATURES = {
     "tmt_server_start": (C.c_int, [C.POINTER(TmtServerConfig), C.POINTER(_H)]),
     "tmt_server_add_model": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P, C.c_float, _P, _P, C.POINTER(C.c_uint32)]),
     "tmt_server_set_model_priors": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P, _P]),
+    "tmt_server_add_model_f32": (C.c_int, [_H, C.c_uint32, C.c_uint32, _P, C.c_float, _P, _P, C.POINTER(C.c_uint32)]),
+    "tmt_server_submit_weighted": (C.c_int, [_H, C.c_uint32, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64,
+                                             C.POINTER(C.c_uint64)]),
+    "tmt_server_submit_batch_weighted": (C.c_int, [_H, _P, _P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P]),
     "tmt_server_submit": (C.c_int, [_H, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64,
                                     C.POINTER(C.c_uint64)]),
     "tmt_server_poll": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), _P, C.c_uint32,

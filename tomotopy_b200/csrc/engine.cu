@@ -536,16 +536,6 @@ k_sweep_doc(SweepArgs a)
                         const float Ao = rowf[zo];
                         s = fmaxf(__fadd_rn(__fsub_rn(s, __fmul_rn(Ao, phu)), __fmul_rn(Ao, phi_own)), 0.f);
                     }
-                    // without the prefetch registers: above 256 topics pass 1 was the column's
-                    // last use (pass 2 reads the table), so the next token's column loads now,
-                    // behind this token's scans and draw
-                    if (!PF && CH >= 4 && jn >= 0) {
-                        const uint32_t vnx = __shfl_sync(FULL, my_w, jn);
-                        if (vnx != v_have) {
-                            load_col(vnx, pv);
-                            v_have = vnx;
-                        }
-                    }
                     // lanes at or above min(32, ceil(K/4)) hold no topics: a Hillis-Steele
                     // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
                     // the values of the full scan, and the total sits in lane

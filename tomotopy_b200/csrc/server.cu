@@ -70,6 +70,7 @@ struct Request {
     uint64_t id;
     uint32_t model;
     std::vector<uint32_t> words;   // sorted by id
+    std::vector<float> wts;        // weighted models: the tokens' weights, in the same order
     uint32_t iters;
     uint64_t seed, key;
     Clock::time_point t_submit;
@@ -166,6 +167,7 @@ struct Model {
     float* d_pcum = nullptr;
     float* d_ecum = nullptr;
     bool used = false;                  // a request was submitted: the model is frozen
+    bool weighted = false;              // float counts (TermWeight IDF / PMI); requests carry weights
 };
 
 } // namespace
@@ -179,6 +181,10 @@ struct tmt_server {
     uint16_t* d_z = nullptr;
     uint32_t* d_staging = nullptr;               // admitted documents of one step, contiguous
     uint32_t* h_staging = nullptr;               // pinned
+    // token weights beside the arena's words, allocated with the first weighted model
+    float* d_wt = nullptr;
+    float* d_wstaging = nullptr;
+    float* h_wstaging = nullptr;
     uint64_t *h_sc_src = nullptr, *h_sc_dst = nullptr, *d_sc_src = nullptr, *d_sc_dst = nullptr;
     uint32_t *h_sc_len = nullptr, *d_sc_len = nullptr;
     std::vector<void*> pinned_allocs;
@@ -277,6 +283,7 @@ bool server_step(tmt_server* s)
             const uint32_t len = m->h_tok_len[sl];
             if (!len) continue;
             std::memcpy(s->h_staging + off, m->req[sl].words.data(), len * sizeof(uint32_t));
+            if (m->weighted) std::memcpy(s->h_wstaging + off, m->req[sl].wts.data(), len * sizeof(float));
             s->h_sc_src[n] = off;
             s->h_sc_dst[n] = m->h_tok_begin[sl];
             s->h_sc_len[n] = len;
@@ -291,6 +298,15 @@ bool server_step(tmt_server* s)
             k_scatter_docs<<<std::min<uint32_t>(n, 4096), 128, 0, s->stream>>>(s->d_staging, s->d_sc_src, s->d_sc_dst,
                                                                               s->d_sc_len, n, s->d_words);
             CK(cudaGetLastError());
+            if (s->d_wt) {
+                // the weights (4-byte values, moved by the same scatter; stale for unweighted documents)
+                CK(cudaMemcpyAsync(s->d_wstaging, s->h_wstaging, off * sizeof(float), cudaMemcpyHostToDevice,
+                                   s->stream));
+                k_scatter_docs<<<std::min<uint32_t>(n, 4096), 128, 0, s->stream>>>(
+                    reinterpret_cast<const uint32_t*>(s->d_wstaging), s->d_sc_src, s->d_sc_dst, s->d_sc_len, n,
+                    reinterpret_cast<uint32_t*>(s->d_wt));
+                CK(cudaGetLastError());
+            }
         }
     }
     bool any = false;
@@ -360,6 +376,7 @@ bool server_step(tmt_server* s)
         a.work = m->d_work;
         a.n_work = (uint32_t)work.size();
         a.counter = m->d_counter;
+        a.wt = m->weighted ? s->d_wt : nullptr;
         a.pidx = m->d_pidx;
         a.pval = m->d_pval;
         a.esum = m->d_esum;
@@ -521,8 +538,13 @@ tmt_status tmt_server_start(const tmt_server_config* cfg, tmt_server** out)
     return TMT_OK;
 }
 
-tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
-                                const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id)
+} // extern "C"
+
+namespace {
+
+// n_kw / n_k: int32 counts, or floats when `weighted` (4 bytes either way)
+tmt_status add_model_impl(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta, const void* n_kw,
+                          const void* n_k, bool weighted, uint32_t* model_id)
 {
     if (!s || !alpha || !n_k || (V && !n_kw) || !model_id || K == 0 || K > 32767 || !(eta > 0))
         return TMT_ERR_INVALID_ARGUMENT;
@@ -543,6 +565,7 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
     }
     m->asum_f = sf;
     m->asum_d = sd;
+    m->weighted = weighted;
     const uint32_t S = s->cfg.max_slots;
     m->slots = S;
     m->active.assign(S, -1);
@@ -587,9 +610,14 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
         m->d_ll = s->dalloc<double>(S);
         m->d_work = s->dalloc<uint32_t>(S);
         m->d_counter = s->dalloc<uint32_t>(1);
+        if (weighted && !s->d_wt) {
+            s->d_wstaging = s->dalloc<float>(s->cfg.token_budget);
+            s->h_wstaging = s->palloc<float>(s->cfg.token_budget);
+            s->d_wt = s->dalloc<float>(s->cfg.token_budget);
+        }
         if ((uint64_t)K * V)
-            CK(cudaMemcpy(m->d_nkw, n_kw, (uint64_t)K * V * sizeof(int32_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(m->d_nk, n_k, K * sizeof(int32_t), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(m->d_nkw, n_kw, (uint64_t)K * V * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_nk, n_k, K * 4, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(m->d_alpha, alpha, K * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(m->d_acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice));
     } catch (const OomError&) {
@@ -600,6 +628,79 @@ tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const flo
     *model_id = (uint32_t)s->models.size();
     s->models.push_back(std::move(m));
     return TMT_OK;
+}
+
+// a request from host arrays: sorted by word id, the weights following their
+// tokens; every token of one word must carry the same weight
+tmt_status make_request(tmt_server* s, const uint32_t* wid, const float* wts, uint64_t len, uint32_t iters,
+                        uint64_t seed, uint64_t key, Request& r)
+{
+    if (len > s->cfg.max_doc_len || (len && !wid)) return TMT_ERR_INVALID_ARGUMENT;
+    if (wts) {
+        std::vector<std::pair<uint32_t, float>> pw(len);
+        for (uint64_t i = 0; i < len; ++i) {
+            if (!(wts[i] >= 0.f) || !(wts[i] <= 65536.f)) return TMT_ERR_INVALID_ARGUMENT;
+            pw[i] = { wid[i], wts[i] };
+        }
+        std::stable_sort(pw.begin(), pw.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        r.words.resize(len);
+        r.wts.resize(len);
+        for (uint64_t i = 0; i < len; ++i) {
+            r.words[i] = pw[i].first;
+            r.wts[i] = pw[i].second;
+            if (i && r.words[i] == r.words[i - 1] && r.wts[i] != r.wts[i - 1]) return TMT_ERR_INVALID_ARGUMENT;
+        }
+    } else {
+        r.words.assign(wid, wid + len);
+        std::stable_sort(r.words.begin(), r.words.end());
+    }
+    r.iters = iters;
+    r.seed = seed;
+    r.key = key;
+    return TMT_OK;
+}
+
+// queue requests (under the lock): each model must match its requests' kind
+tmt_status enqueue(tmt_server* s, std::vector<Request>& rs, const uint32_t* model_ids, uint64_t* request_ids)
+{
+    const auto now = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
+        for (uint64_t d = 0; d < rs.size(); ++d) {
+            if (model_ids[d] >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
+            if (s->models[model_ids[d]]->weighted != !rs[d].wts.empty() && !rs[d].words.empty())
+                return TMT_ERR_INVALID_ARGUMENT;
+        }
+        for (uint64_t d = 0; d < rs.size(); ++d) {
+            Request& r = rs[d];
+            r.model = model_ids[d];
+            if (s->models[r.model]->weighted && r.wts.size() != r.words.size()) r.wts.assign(r.words.size(), 0.f);
+            s->models[r.model]->used = true;
+            r.id = s->next_id++;
+            r.t_submit = now;
+            request_ids[d] = r.id;
+            s->queue.push_back(std::move(r));
+        }
+    }
+    s->cv_work.notify_one();
+    return TMT_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+tmt_status tmt_server_add_model(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
+                                const int32_t* n_kw, const int32_t* n_k, uint32_t* model_id)
+{
+    return add_model_impl(s, K, V, alpha, eta, n_kw, n_k, false, model_id);
+}
+
+tmt_status tmt_server_add_model_f32(tmt_server* s, uint32_t K, uint32_t V, const float* alpha, float eta,
+                                    const float* n_kw, const float* n_k, uint32_t* model_id)
+{
+    return add_model_impl(s, K, V, alpha, eta, n_kw, n_k, true, model_id);
 }
 
 tmt_status tmt_server_set_model_priors(tmt_server* s, uint32_t model_id, uint32_t P, const uint32_t* word_ids,
@@ -651,26 +752,20 @@ tmt_status tmt_server_submit(tmt_server* s, uint32_t model_id, const uint32_t* w
                              uint64_t seed, uint64_t key, uint64_t* request_id)
 {
     if (!s || (len && !wid) || !request_id) return TMT_ERR_INVALID_ARGUMENT;
-    if (len > s->cfg.max_doc_len) return TMT_ERR_INVALID_ARGUMENT;
-    Request r;
-    r.words.assign(wid, wid + len);
-    std::stable_sort(r.words.begin(), r.words.end());
-    r.iters = iters;
-    r.seed = seed;
-    r.key = key;
-    r.t_submit = Clock::now();
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
-        if (model_id >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
-        s->models[model_id]->used = true;
-        r.model = model_id;
-        r.id = s->next_id++;
-        *request_id = r.id;
-        s->queue.push_back(std::move(r));
-    }
-    s->cv_work.notify_one();
-    return TMT_OK;
+    std::vector<Request> rs(1);
+    tmt_status st = make_request(s, wid, nullptr, len, iters, seed, key, rs[0]);
+    if (st != TMT_OK) return st;
+    return enqueue(s, rs, &model_id, request_id);
+}
+
+tmt_status tmt_server_submit_weighted(tmt_server* s, uint32_t model_id, const uint32_t* wid, const float* weights,
+                                      uint32_t len, uint32_t iters, uint64_t seed, uint64_t key, uint64_t* request_id)
+{
+    if (!s || (len && (!wid || !weights)) || !request_id) return TMT_ERR_INVALID_ARGUMENT;
+    std::vector<Request> rs(1);
+    tmt_status st = make_request(s, wid, weights, len, iters, seed, key, rs[0]);
+    if (st != TMT_OK) return st;
+    return enqueue(s, rs, &model_id, request_id);
 }
 
 tmt_status tmt_server_poll(tmt_server* s, uint32_t wait_ms, uint64_t* request_id, uint32_t* model_id,
@@ -699,37 +794,24 @@ tmt_status tmt_server_submit_batch(tmt_server* s, const uint32_t* model_ids, con
                                    const uint64_t* doc_off, uint64_t n, uint32_t iters, uint64_t seed,
                                    const uint64_t* keys, uint64_t* request_ids)
 {
+    return tmt_server_submit_batch_weighted(s, model_ids, wid, nullptr, doc_off, n, iters, seed, keys, request_ids);
+}
+
+tmt_status tmt_server_submit_batch_weighted(tmt_server* s, const uint32_t* model_ids, const uint32_t* wid,
+                                            const float* weights, const uint64_t* doc_off, uint64_t n, uint32_t iters,
+                                            uint64_t seed, const uint64_t* keys, uint64_t* request_ids)
+{
     if (!s || (n && (!model_ids || !doc_off || !request_ids))) return TMT_ERR_INVALID_ARGUMENT;
     std::vector<Request> rs(n);
     for (uint64_t d = 0; d < n; ++d) {
         if (doc_off[d + 1] < doc_off[d]) return TMT_ERR_INVALID_ARGUMENT;
         const uint64_t len = doc_off[d + 1] - doc_off[d];
-        if (len > s->cfg.max_doc_len || (len && !wid)) return TMT_ERR_INVALID_ARGUMENT;
-        Request& r = rs[d];
-        r.words.assign(wid + doc_off[d], wid + doc_off[d + 1]);
-        std::stable_sort(r.words.begin(), r.words.end());
-        r.iters = iters;
-        r.seed = seed;
-        r.key = keys ? keys[d] : 0;
+        if (len && weights == nullptr && !wid) return TMT_ERR_INVALID_ARGUMENT;
+        tmt_status st = make_request(s, wid ? wid + doc_off[d] : nullptr, weights ? weights + doc_off[d] : nullptr,
+                                     len, iters, seed, keys ? keys[d] : 0, rs[d]);
+        if (st != TMT_OK) return st;
     }
-    const auto now = Clock::now();
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        if (s->stop) return s->worker_status != TMT_OK ? s->worker_status : TMT_ERR_CANCELLED;
-        for (uint64_t d = 0; d < n; ++d)
-            if (model_ids[d] >= s->models.size()) return TMT_ERR_INVALID_ARGUMENT;
-        for (uint64_t d = 0; d < n; ++d) {
-            Request& r = rs[d];
-            r.model = model_ids[d];
-            s->models[r.model]->used = true;
-            r.id = s->next_id++;
-            r.t_submit = now;
-            request_ids[d] = r.id;
-            s->queue.push_back(std::move(r));
-        }
-    }
-    s->cv_work.notify_one();
-    return TMT_OK;
+    return enqueue(s, rs, model_ids, request_ids);
 }
 
 tmt_status tmt_server_poll_batch(tmt_server* s, uint32_t wait_ms, uint64_t max_n, uint64_t* request_ids,

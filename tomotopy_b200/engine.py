@@ -232,20 +232,26 @@ class Server:
         self.K = {}
 
     def add_model(self, K, V, alpha, eta, n_kw, n_k):
+        """A frozen model: int32 counts, or float counts (weighted: its requests
+        then carry token weights)."""
         a = np.ascontiguousarray(np.broadcast_to(np.asarray(alpha, np.float32), (K,)))
-        nkw = np.ascontiguousarray(n_kw, dtype=np.int32)
-        nk = np.ascontiguousarray(n_k, dtype=np.int32)
         mid = C.c_uint32()
-        check(lib.tmt_server_add_model(self.h, K, V, _p(a), float(eta), _p(nkw), _p(nk), C.byref(mid)), None,
-              "tmt_server_add_model")
+        if np.asarray(n_kw).dtype == np.float32:
+            nkw = np.ascontiguousarray(n_kw, dtype=np.float32)
+            nk = np.ascontiguousarray(n_k, dtype=np.float32)
+            check(lib.tmt_server_add_model_f32(self.h, K, V, _p(a), float(eta), _p(nkw), _p(nk), C.byref(mid)),
+                  None, "tmt_server_add_model_f32")
+        else:
+            nkw = np.ascontiguousarray(n_kw, dtype=np.int32)
+            nk = np.ascontiguousarray(n_k, dtype=np.int32)
+            check(lib.tmt_server_add_model(self.h, K, V, _p(a), float(eta), _p(nkw), _p(nk), C.byref(mid)), None,
+                  "tmt_server_add_model")
         self.K[mid.value] = int(K)
         return mid.value
 
     def add_engine_model(self, eng):
-        """A trained engine's frozen state, with its word priors; integer counts
-        only (the served pool has no weighted inference)."""
-        if getattr(eng, "weighted", False):
-            raise ValueError("the served pool takes integer-count models")
+        """A trained engine's frozen state, with its word priors; float counts
+        for a weighted engine."""
         _, nkw, nk, alpha = eng.state()
         mid = self.add_model(eng.K, eng.V, alpha, eng.eta, nkw, nk)
         ids = getattr(eng, "_prior_ids", None)
@@ -260,11 +266,17 @@ class Server:
         check(lib.tmt_server_set_model_priors(self.h, int(model_id), len(ids), _p(ids), _p(pr)), None,
               "tmt_server_set_model_priors")
 
-    def submit(self, model_id, words, iters=100, seed=0, key=0):
+    def submit(self, model_id, words, iters=100, seed=0, key=0, weights=None):
         w = np.ascontiguousarray(words, dtype=np.uint32)
         rid = C.c_uint64()
-        check(lib.tmt_server_submit(self.h, int(model_id), _p(w), len(w), int(iters), int(seed), int(key),
-                                    C.byref(rid)), None, "tmt_server_submit")
+        if weights is None:
+            check(lib.tmt_server_submit(self.h, int(model_id), _p(w), len(w), int(iters), int(seed), int(key),
+                                        C.byref(rid)), None, "tmt_server_submit")
+        else:
+            wt = np.ascontiguousarray(weights, dtype=np.float32)
+            check(lib.tmt_server_submit_weighted(self.h, int(model_id), _p(w), _p(wt), len(w), int(iters),
+                                                 int(seed), int(key), C.byref(rid)), None,
+                  "tmt_server_submit_weighted")
         return rid.value
 
     def poll(self, wait_ms=1000):
@@ -281,7 +293,7 @@ class Server:
             raise TmtError(st, lib.tmt_server_last_error(self.h).decode())
         return rid.value, mid.value, theta[:self.K[mid.value]].copy(), ll.value, lat.value
 
-    def submit_batch(self, model_ids, doc_off, words, iters=100, seed=0, keys=None):
+    def submit_batch(self, model_ids, doc_off, words, iters=100, seed=0, keys=None, weights=None):
         """Queues len(doc_off) - 1 documents at once; returns their request ids."""
         off = np.ascontiguousarray(doc_off, dtype=np.uint64)
         w = np.ascontiguousarray(words, dtype=np.uint32)
@@ -289,8 +301,9 @@ class Server:
         mids = np.ascontiguousarray(np.broadcast_to(np.asarray(model_ids, np.uint32), (n,)))
         k = np.ascontiguousarray(keys, dtype=np.uint64) if keys is not None else None
         rids = np.zeros(max(n, 1), dtype=np.uint64)
-        check(lib.tmt_server_submit_batch(self.h, _p(mids), _p(w), _p(off), n, int(iters), int(seed), _p(k),
-                                          _p(rids)), None, "tmt_server_submit_batch")
+        wt = np.ascontiguousarray(weights, dtype=np.float32) if weights is not None else None
+        check(lib.tmt_server_submit_batch_weighted(self.h, _p(mids), _p(w), _p(wt), _p(off), n, int(iters),
+                                                   int(seed), _p(k), _p(rids)), None, "tmt_server_submit_batch")
         return rids[:n]
 
     def poll_batch(self, max_n=4096, wait_ms=1000):
