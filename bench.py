@@ -391,7 +391,10 @@ def run_infer(args):
         "token_sweeps_per_s": sat["docs_per_s"] * tok_per_doc * iters,
         "results_identical_to_plain": bool(agree),
         "mean_ll_per_word_plain": float(np.sum(plain_ll) / max(1, sum(len(docs[i]) for i in range(n_plain)))),
-        "server": {"steps": int(st.steps), "mean_active": st.mean_active},
+        "server": {"steps": int(st.steps), "mean_active": st.mean_active,
+                   "saturation_steps": int(st1.steps - st0.steps),
+                   "saturation_mean_active": ((st1.mean_active * st1.steps - st0.mean_active * st0.steps)
+                                              / max(1, st1.steps - st0.steps))},
         "batched_docs_per_s": batched_dps,
     }
     # the saturation run: device time of the inference launches against the
