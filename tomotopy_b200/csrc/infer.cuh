@@ -214,6 +214,7 @@ k_infer_slots(InferArgs a)
             for (uint32_t base = 0; base < L; base += 32) {
                 const uint32_t jl = base + lane;
                 uint32_t my_w = 0xFFFFFFFFu, my_z = 0;
+                uint32_t my_zc = 0;              // my token's current topic (updated when it is drawn)
                 bool my_same = false;            // my token's word equals the next token's
                 float my_u = 0.f, my_wt = 1.f;
                 if (jl < L) {
@@ -223,6 +224,7 @@ k_infer_slots(InferArgs a)
                     my_same = jl + 1 < L && a.words[b + jl + 1] == my_w;
                     my_u = tmt::u01(tmt::philox_u32(jl, it, klo, khi, a.key));
                 }
+                my_zc = my_z;
                 const unsigned same_m = __ballot_sync(FULL, my_same);
                 const int nb = (int)min(32u, L - base);
                 for (int q2 = 0; q2 < nb; ++q2) {
@@ -234,10 +236,18 @@ k_infer_slots(InferArgs a)
                     if (v >= a.V) continue;
                     const bool in_run = j < run_e;
                     if (!in_run && ((same_m >> q2) & 1u)) {
-                        // a multi-token run starts here: histogram of its tokens' topics
+                        // a multi-token run starts here: histogram of its tokens' topics.  A run
+                        // inside this chunk of 32 tokens takes them from the lanes' registers.
                         run_b = j;
-                        run_e = run_end(j, v);
-                        for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicAdd(&own[a.z[b + t]], 1);
+                        const unsigned rest = ~same_m & (0xFFFFFFFFu << q2);
+                        if (rest) {
+                            const int qe = __ffs(rest) - 1;           // the run's last token in the chunk
+                            run_e = base + qe + 1;
+                            if (lane >= q2 && lane <= qe) atomicAdd(&own[my_z], 1);
+                        } else {
+                            run_e = run_end(j, v);
+                            for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicAdd(&own[a.z[b + t]], 1);
+                        }
                         __syncwarp();
                     }
                     const bool multi = j < run_e;
@@ -331,10 +341,17 @@ k_infer_slots(InferArgs a)
                         rr[znew] = __frcp_rn(rden(znew, n));
                         a.z[b + j] = (uint16_t)znew;
                     }
+                    if (lane == q2) my_zc = (uint32_t)znew;
                     __syncwarp();
                     if (multi && j + 1 == run_e) {
-                        // the run is done: clear its histogram
-                        for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicSub(&own[a.z[b + t]], 1);
+                        // the run is done: clear its histogram (from the registers when the
+                        // run lies inside this chunk)
+                        if (run_b >= base) {
+                            const uint32_t lb = run_b - base, le = run_e - base;
+                            if (lane >= lb && lane < le) atomicSub(&own[my_zc], 1);
+                        } else {
+                            for (uint32_t t = run_b + lane; t < run_e; t += 32) atomicSub(&own[a.z[b + t]], 1);
+                        }
                         __syncwarp();
                     }
                 }
