@@ -71,3 +71,40 @@ def test_weighted_counts_invariants():
     np.testing.assert_allclose(sw.ndk.sum(1), sw.doc_wlen[:c.D], rtol=1e-4, atol=1e-3)
     np.testing.assert_allclose(sw.nkw.sum(0), sw.nk, rtol=1e-5, atol=1e-3)
     assert np.all(sw.ndk >= 0) and np.all(sw.nkw >= 0)
+
+
+def test_unit_weight_infer_equals_integer_infer():
+    """The weighted inference restatement with every weight 1 and the model's
+    counts as floats reproduces the integer restatement exactly."""
+    c = small_corpus(seed=12)
+    K = 9
+    st = O.State(c, K, 0.1, 0.01, 3)
+    st.doc_live_sweeps(4, groups=2)
+    rng = np.random.default_rng(2)
+    for _ in range(5):
+        doc = np.sort(rng.integers(0, c.V + 3, 40).astype(np.uint32))
+        ll, z, ndk, th = O.infer_doc(K, c.V, st.alpha, 0.01, st.nkw, st.nk, doc, 15, 7, 3)
+        llw, zw, ndkw, thw = O.infer_doc_w(K, c.V, st.alpha, 0.01, st.nkw.astype(np.float32),
+                                           st.nk.astype(np.float32), doc, np.ones(len(doc), np.float32), 15, 7, 3)
+        np.testing.assert_array_equal(z, zw)
+        np.testing.assert_array_equal(th, thw)
+        np.testing.assert_array_equal(ndk.astype(np.float32), ndkw)
+        assert ll == pytest.approx(llw, rel=1e-13)
+
+
+def test_open_masks_and_global_alpha_rows_equal_plain_sweep():
+    """Masks allowing every topic and per-document alpha rows equal to the
+    model's alpha reproduce the plain doc-major sweep exactly."""
+    c = small_corpus(seed=13)
+    K = 11
+    a = (0.05 * (1 + np.arange(K) % 3)).astype(np.float32)
+    st = O.State(c, K, a, 0.01, 5)
+    sm = O.StateM(c, K, a, 0.01, 5, st.z.copy(), mask=np.ones((c.D, K), bool),
+                  alpha_rows=a[None, :].copy(), doc_row=np.zeros(c.D, np.uint32))
+    st.doc_live_sweeps(3, groups=3)
+    sm.doc_live_sweeps(3, groups=3)
+    np.testing.assert_array_equal(st.z, sm.z)
+    np.testing.assert_array_equal(st.nkw, sm.nkw)
+    a1, _ = st.ll_f64()
+    a2, _ = sm.ll_f64()
+    assert a1 == pytest.approx(a2, rel=1e-12)

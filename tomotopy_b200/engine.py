@@ -86,12 +86,9 @@ class Engine:
         if mask is None:
             check(lib.tmt_set_doc_topic_mask(self.h, None), self.h)
             return
-        m = np.asarray(mask, dtype=bool)
-        mw = (self.K + 31) // 32
-        bits = np.zeros((self.D, mw * 32), dtype=bool)
-        bits[:, :self.K] = m
-        words = np.packbits(bits.reshape(self.D, mw, 32)[:, :, ::-1], axis=2, bitorder="big")
-        self._mask = np.ascontiguousarray(words.view(">u4").reshape(self.D, mw).astype(np.uint32))
+        self._mask = pack_topic_mask(mask, self.K)
+        if self._mask.shape[0] != self.D:
+            raise ValueError("the mask needs one row per document")
         check(lib.tmt_set_doc_topic_mask(self.h, _p(self._mask)), self.h)
 
     def set_doc_alpha(self, rows, doc_row):
@@ -183,6 +180,18 @@ class Engine:
         i = TmtInfo()
         check(lib.tmt_get_info(self.h, C.byref(i)), self.h)
         return i
+
+
+def pack_topic_mask(mask, K):
+    """A boolean D x K topic mask as the C ABI's bit rows: D rows of ceil(K/32)
+    uint32 words, bit (k % 32) of word k // 32 set where topic k is allowed."""
+    m = np.asarray(mask, dtype=bool).reshape(-1, K)
+    D = m.shape[0]
+    mw = (K + 31) // 32
+    bits = np.zeros((D, mw * 32), dtype=bool)
+    bits[:, :K] = m
+    words = np.packbits(bits.reshape(D, mw, 32)[:, :, ::-1], axis=2, bitorder="big")
+    return np.ascontiguousarray(words.view(">u4").reshape(D, mw).astype(np.uint32))
 
 
 def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1.07, threads=0, doc_offset=0):

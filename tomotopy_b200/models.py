@@ -338,7 +338,8 @@ class LDAModel:
         file = file or sys.stdout
         i = self._info()
         print(f"<Basic Info>\n| LDAModel (current version: {_version})\n| {i.n_docs} docs, {i.N} words\n"
-              f"| Total Vocabs: {i.n_vocab}, Used Vocabs: {i.V}", file=file)
+              f"| Total Vocabs: {i.n_vocab}, Used Vocabs: {i.V}\n| Term Weighting: {TermWeight(i.tw).name}",
+              file=file)
         print(f"<Training Info>\n| Iterations: {i.global_step}", file=file)
         if i.prepared:
             print(f"| Log-likelihood per word: {self.ll_per_word:.5f}", file=file)
