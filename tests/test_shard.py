@@ -68,6 +68,25 @@ def test_plan_matches_single_corpus(G):
     assert seen == want
 
 
+@pytest.mark.parametrize("case", ["ties", "zipf", "huge"])
+def test_plan_order_is_stable_longest_first(case):
+    """The planner sorts by counting (lengths up to 4D + 65536) or by a
+    comparison sort (longer documents); both give numpy's stable order."""
+    rng = np.random.default_rng(5)
+    if case == "ties":
+        lens = rng.integers(0, 6, 5000).astype(np.uint64)
+    elif case == "zipf":
+        lens = np.minimum(rng.zipf(1.3, 20000), 10 ** 5).astype(np.uint64)
+    else:
+        lens = rng.integers(0, 3, 3000).astype(np.uint64)
+        lens[[5, 17, 2900]] = [10 ** 7, 3 * 10 ** 6, 10 ** 7]
+    for G in (1, 5, 8):
+        order, bounds = single_groups(lens, G)
+        lo, lb, gb, toff = shard.plan(lens, G, 0, len(lens))
+        np.testing.assert_array_equal(lo, order)
+        np.testing.assert_array_equal(lb, bounds)
+
+
 def test_plan_rejects_bad_shards():
     lens = np.array([3, 4, 5], np.uint64)
     with pytest.raises(Exception):

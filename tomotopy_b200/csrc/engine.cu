@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <stdexcept>
 #include <mutex>
+#include <thread>
 #include "philox.cuh"
 #include "special.cuh"
 #include "common.cuh"
@@ -97,12 +98,20 @@ __global__ void k_init_z(const uint32_t* __restrict__ words, uint64_t n_all, uin
     }
 }
 
-// counts from assignments: warp per document (resetStatistics, LDAModel.hpp:301-316)
+// counts from assignments: warp per document (resetStatistics, LDAModel.hpp:301-316).
+// With nk_smem the block sums n_k in shared memory (K ints) and adds its
+// nonzero totals once at the end: n_k's K addresses would otherwise take one
+// global atomic per token.
 __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* __restrict__ words,
                          const uint16_t* __restrict__ z, uint64_t D, uint32_t K, uint32_t V,
                          int32_t* __restrict__ ndk, int32_t* __restrict__ nkw, int32_t* __restrict__ nk,
-                         int32_t* __restrict__ doc_len)
+                         int32_t* __restrict__ doc_len, bool nk_smem)
 {
+    extern __shared__ int32_t s_nk[];
+    if (nk_smem) {
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) s_nk[k] = 0;
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -114,12 +123,18 @@ __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* _
             uint32_t k = z[i];
             atomicAdd(&ndk[d * K + k], 1);
             atomicAdd(&nkw[(uint64_t)w * K + k], 1);
-            atomicAdd(&nk[k], 1);
+            if (nk_smem) atomicAdd(&s_nk[k], 1);
+            else atomicAdd(&nk[k], 1);
             ++cnt;
         }
 #pragma unroll
         for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
         if (lane == 0 && doc_len) doc_len[d] = cnt;
+    }
+    if (nk_smem) {
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            if (s_nk[k]) atomicAdd(&nk[k], s_nk[k]);
     }
 }
 
@@ -925,6 +940,8 @@ struct tmt_handle {
     uint32_t sweeps_timed = 0;
     int num_sms = 0;
     std::string err;
+    void* stage[2] = {nullptr, nullptr};          // pinned staging of downloads to pageable memory
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 
     uint64_t D = 0, N_all = 0, N = 0, global_step = 0, bytes = 0, launches = 0;
     int sampler_used = 0;
@@ -1062,6 +1079,10 @@ struct tmt_handle {
     ~tmt_handle()
     {
         release();
+        for (int i = 0; i < 2; ++i) {
+            if (stage[i]) cudaFreeHost(stage[i]);
+            if (stage_ev[i]) cudaEventDestroy(stage_ev[i]);
+        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (kev0) cudaEventDestroy(kev0);
@@ -1111,6 +1132,73 @@ void launch_check(tmt_handle* h)
 {
     ++h->launches;
     CK(cudaGetLastError());
+}
+
+// Copies host memory with up to 16 threads: the first touch of freshly
+// allocated pageable pages (a page fault each) then runs on all of them.
+void host_copy_parallel(char* dst, const char* src, uint64_t bytes)
+{
+    const uint64_t per = 1ull << 20;
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t T = (uint32_t)std::min<uint64_t>(std::min(16u, hw), (bytes + per - 1) / per);
+    if (T <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const uint64_t slice = ((bytes + T - 1) / T + 4095) & ~4095ull;
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (uint32_t t = 0; t < T; ++t) {
+        const uint64_t b = (uint64_t)t * slice;
+        if (b >= bytes) break;
+        const uint64_t n = std::min(slice, bytes - b);
+        th.emplace_back([=] { std::memcpy(dst + b, src + b, n); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// Device -> host copy on the handle's stream, synchronous on return.  A
+// pinned destination (or a small copy) takes one cudaMemcpyAsync; a large
+// pageable one goes through two pinned staging buffers, the device copy of a
+// chunk overlapping the threaded host copy of the one before (the driver's
+// own path to pageable memory copies and takes its page faults on a single
+// host thread).
+void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
+{
+    if (!bytes) return;
+    constexpr uint64_t kChunk = 16ull << 20;
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned || bytes < 2 * kChunk) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return;
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (!h->stage[i]) {
+            if (cudaHostAlloc(&h->stage[i], kChunk, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                h->stage[i] = nullptr;
+                throw OomError("pinned staging buffer allocation failed");
+            }
+        }
+        if (!h->stage_ev[i]) CK(cudaEventCreateWithFlags(&h->stage_ev[i], cudaEventDisableTiming));
+    }
+    const uint64_t n = (bytes + kChunk - 1) / kChunk;
+    auto len = [&](uint64_t c) { return std::min(kChunk, bytes - c * kChunk); };
+    auto issue = [&](uint64_t c) {
+        CK(cudaMemcpyAsync(h->stage[c & 1], static_cast<const char*>(src) + c * kChunk, len(c),
+                           cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
+    };
+    issue(0);
+    for (uint64_t c = 0; c < n; ++c) {
+        // buffer (c+1)&1 last held chunk c-1, whose host copy has finished
+        if (c + 1 < n) issue(c + 1);
+        CK(cudaEventSynchronize(h->stage_ev[c & 1]));
+        host_copy_parallel(static_cast<char*>(dst) + c * kChunk, static_cast<const char*>(h->stage[c & 1]), len(c));
+    }
 }
 
 struct SweepShape {
@@ -1523,8 +1611,19 @@ ShardPlan plan_shard(const uint64_t* len, uint64_t D_global, uint32_t groups, ui
     if (doc_begin > D_global || D_local > D_global - doc_begin) throw ArgError("shard outside the corpus");
     ShardPlan p;
     std::vector<uint64_t> gorder(D_global);
-    std::iota(gorder.begin(), gorder.end(), (uint64_t)0);
-    std::stable_sort(gorder.begin(), gorder.end(), [&](uint64_t a, uint64_t b) { return len[a] > len[b]; });
+    uint64_t longest = 0;
+    for (uint64_t d = 0; d < D_global; ++d) longest = std::max(longest, len[d]);
+    if (longest <= 4 * D_global + 65536) {
+        // stable counting sort on (longest - len): the order std::stable_sort
+        // by descending length gives, in O(D + longest)
+        std::vector<uint64_t> start(longest + 2, 0);
+        for (uint64_t d = 0; d < D_global; ++d) ++start[longest - len[d] + 1];
+        for (uint64_t b = 1; b <= longest + 1; ++b) start[b] += start[b - 1];
+        for (uint64_t d = 0; d < D_global; ++d) gorder[start[longest - len[d]]++] = d;
+    } else {
+        std::iota(gorder.begin(), gorder.end(), (uint64_t)0);
+        std::stable_sort(gorder.begin(), gorder.end(), [&](uint64_t a, uint64_t b) { return len[a] > len[b]; });
+    }
     uint64_t total = 0;
     for (uint64_t d = 0; d < D_global; ++d) {
         total += len[d];
@@ -1610,14 +1709,19 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         h->N_all = n_all;
         h->global_step = 0;
         h->cur = 0;
-        // host-side facts: valid-token count per doc, doc order (longest first)
-        std::vector<int32_t> len(D);
+        // valid-token count per document: counted on the host for weighted
+        // counts (the planner's facts are uploaded), else N is read back from
+        // the device's n_k after the counts kernel
+        std::vector<int32_t> len;
         uint64_t N = 0;
-        for (uint64_t d = 0; d < D; ++d) {
-            int32_t c = 0;
-            for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) c += wid[i] < V;
-            len[d] = c;
-            N += c;
+        if (weights) {
+            len.resize(D);
+            for (uint64_t d = 0; d < D; ++d) {
+                int32_t c = 0;
+                for (uint64_t i = doc_off[d]; i < doc_off[d + 1]; ++i) c += wid[i] < V;
+                len[d] = c;
+                N += c;
+            }
         }
         h->N = N;
         ShardPlan plan;
@@ -1786,9 +1890,16 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             CK(cudaMemcpyAsync(h->d_doc_len, len.data(), D * sizeof(int32_t), cudaMemcpyHostToDevice, st));
         } else if (D) {
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D * 32 + 255) / 256);
-            k_counts<<<grid, 256, 0, st>>>(h->d_doc_off, h->d_words, h->d_z, D, K, V, h->d_ndk, h->d_nkw[0],
-                                           h->d_nk[0], h->d_doc_len);
+            const bool nk_smem = K <= 8192;     // at most 32 KB of shared memory
+            k_counts<<<grid, 256, nk_smem ? K * sizeof(int32_t) : 0, st>>>(
+                h->d_doc_off, h->d_words, h->d_z, D, K, V, h->d_ndk, h->d_nkw[0], h->d_nk[0], h->d_doc_len, nk_smem);
             launch_check(h);
+            // this rank's valid tokens: the sum of its n_k, before any exchange
+            std::vector<int32_t> nk_local(K);
+            CK(cudaMemcpyAsync(nk_local.data(), h->d_nk[0], K * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (uint32_t k = 0; k < K; ++k) N += (uint64_t)(uint32_t)nk_local[k];
+            h->N = N;
         }
         if (h->world > 1) {
             if (h->d_delta) CK(cudaMemsetAsync(h->d_delta, 0, ((uint64_t)K * V + K) * sizeof(int32_t), st));
@@ -2027,8 +2138,8 @@ tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t
         if (h->weighted && (n_kw || n_k))
             throw StateError("the counts are weighted (float): read them with tmt_download_counts_f32");
         const uint32_t K = h->cfg.K, V = h->cfg.V;
-        if (z && h->N_all) CK(cudaMemcpyAsync(z, h->d_z, h->N_all * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream));
-        if (n_kw) CK(cudaMemcpyAsync(n_kw, h->d_nkw[h->cur], (uint64_t)K * V * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        if (z) d2h(h, z, h->d_z, h->N_all * sizeof(uint16_t));
+        if (n_kw) d2h(h, n_kw, h->d_nkw[h->cur], (uint64_t)K * V * sizeof(int32_t));
         if (n_k) CK(cudaMemcpyAsync(n_k, h->d_nk[h->cur], K * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaMemcpyAsync(h->alpha.data(), h->d_alpha, K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -2043,8 +2154,8 @@ tmt_status tmt_download_counts_f32(tmt_handle* h, float* n_dk, float* n_kw, floa
         if (!h->uploaded) throw StateError("no corpus uploaded");
         if (!h->weighted) throw StateError("the counts are integers: read them with tmt_download_state");
         const uint64_t K = h->cfg.K, V = h->cfg.V;
-        if (n_dk && h->D) CK(cudaMemcpyAsync(n_dk, h->d_ndk, h->D * K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-        if (n_kw) CK(cudaMemcpyAsync(n_kw, h->d_nkw[0], K * V * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        if (n_dk) d2h(h, n_dk, h->d_ndk, h->D * K * sizeof(float));
+        if (n_kw) d2h(h, n_kw, h->d_nkw[0], K * V * sizeof(float));
         if (n_k) CK(cudaMemcpyAsync(n_k, h->d_nk[0], K * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
         if (doc_wlen && h->D)
             CK(cudaMemcpyAsync(doc_wlen, h->d_doc_wlen, h->D * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -2059,10 +2170,7 @@ tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk)
         if (!h->uploaded) throw StateError("no corpus uploaded");
         if (!n_dk) throw ArgError("n_dk is NULL");
         if (h->weighted) throw StateError("the counts are weighted (float): read them with tmt_download_counts_f32");
-        if (h->D)
-            CK(cudaMemcpyAsync(n_dk, h->d_ndk, h->D * (uint64_t)h->cfg.K * sizeof(int32_t),
-                               cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        d2h(h, n_dk, h->d_ndk, h->D * (uint64_t)h->cfg.K * sizeof(int32_t));
     });
 }
 
