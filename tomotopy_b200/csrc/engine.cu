@@ -31,6 +31,7 @@
 #include <stdexcept>
 #include <mutex>
 #include <thread>
+#include <sys/mman.h>
 #include "philox.cuh"
 #include "special.cuh"
 #include "common.cuh"
@@ -1157,27 +1158,22 @@ void host_copy_parallel(char* dst, const char* src, uint64_t bytes)
     for (auto& x : th) x.join();
 }
 
-// Device -> host copy on the handle's stream, synchronous on return.  A
-// pinned destination (or a small copy) takes one cudaMemcpyAsync; a large
-// pageable one goes through two pinned staging buffers, the device copy of a
-// chunk overlapping the threaded host copy of the one before (the driver's
-// own path to pageable memory copies and takes its page faults on a single
-// host thread).
-void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
+constexpr uint64_t kStageChunk = 16ull << 20;
+
+bool host_pinned(const void* p)
 {
-    if (!bytes) return;
-    constexpr uint64_t kChunk = 16ull << 20;
     cudaPointerAttributes at{};
-    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    const bool pinned = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    if (pinned || bytes < 2 * kChunk) {
-        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        return;
-    }
+    return pinned;
+}
+
+// the handle's two pinned staging buffers, allocated on first use
+void ensure_stage(tmt_handle* h)
+{
     for (int i = 0; i < 2; ++i) {
         if (!h->stage[i]) {
-            if (cudaHostAlloc(&h->stage[i], kChunk, cudaHostAllocDefault) != cudaSuccess) {
+            if (cudaHostAlloc(&h->stage[i], kStageChunk, cudaHostAllocDefault) != cudaSuccess) {
                 cudaGetLastError();
                 h->stage[i] = nullptr;
                 throw OomError("pinned staging buffer allocation failed");
@@ -1185,10 +1181,55 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         }
         if (!h->stage_ev[i]) CK(cudaEventCreateWithFlags(&h->stage_ev[i], cudaEventDisableTiming));
     }
-    const uint64_t n = (bytes + kChunk - 1) / kChunk;
-    auto len = [&](uint64_t c) { return std::min(kChunk, bytes - c * kChunk); };
+}
+
+// Backs the pages of a pageable destination with memory ahead of the copies
+// (MADV_POPULATE_WRITE: allocates without changing contents, so it may run
+// beside the threads that fill the same pages).  A kernel without it refuses
+// the call and the copies take the page faults themselves.
+struct Populate {
+    std::vector<std::thread> th;
+    Populate(void* dst, uint64_t bytes)
+    {
+        const uintptr_t b = ((uintptr_t)dst + 4095) & ~(uintptr_t)4095;
+        const uintptr_t e = ((uintptr_t)dst + bytes) & ~(uintptr_t)4095;
+        if (e <= b) return;
+        const uint64_t T = 4;
+        const uint64_t sl = (((e - b) + T - 1) / T + 4095) & ~4095ull;
+        for (uint64_t t = 0; t < T; ++t) {
+            const uintptr_t sb = b + t * sl;
+            if (sb >= e) break;
+            const uint64_t n = std::min<uint64_t>(sl, e - sb);
+            th.emplace_back([=] { madvise(reinterpret_cast<void*>(sb), n, kMadvPopulateWrite); });
+        }
+    }
+    ~Populate()
+    {
+        for (auto& x : th) x.join();
+    }
+    static constexpr int kMadvPopulateWrite = 23;    // MADV_POPULATE_WRITE (Linux 5.14)
+};
+
+// Device -> host copy on the handle's stream, synchronous on return.  A
+// pinned destination (or a small copy) takes one cudaMemcpyAsync; a large
+// pageable one goes through two pinned staging buffers, the device copy of a
+// chunk overlapping the threaded host copy of the one before, while four
+// more threads populate the destination's pages (the driver's own path to
+// pageable memory copies and takes its page faults on one host thread).
+void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
+{
+    if (!bytes) return;
+    if (bytes < 2 * kStageChunk || host_pinned(dst)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return;
+    }
+    ensure_stage(h);
+    Populate pop(dst, bytes);
+    const uint64_t n = (bytes + kStageChunk - 1) / kStageChunk;
+    auto len = [&](uint64_t c) { return std::min(kStageChunk, bytes - c * kStageChunk); };
     auto issue = [&](uint64_t c) {
-        CK(cudaMemcpyAsync(h->stage[c & 1], static_cast<const char*>(src) + c * kChunk, len(c),
+        CK(cudaMemcpyAsync(h->stage[c & 1], static_cast<const char*>(src) + c * kStageChunk, len(c),
                            cudaMemcpyDeviceToHost, h->stream));
         CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
     };
@@ -1197,7 +1238,33 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         // buffer (c+1)&1 last held chunk c-1, whose host copy has finished
         if (c + 1 < n) issue(c + 1);
         CK(cudaEventSynchronize(h->stage_ev[c & 1]));
-        host_copy_parallel(static_cast<char*>(dst) + c * kChunk, static_cast<const char*>(h->stage[c & 1]), len(c));
+        host_copy_parallel(static_cast<char*>(dst) + c * kStageChunk, static_cast<const char*>(h->stage[c & 1]),
+                           len(c));
+    }
+}
+
+// Host -> device copy ordered on the handle's stream.  A pinned source (or a
+// small copy) takes one cudaMemcpyAsync; a large pageable one is copied by
+// host threads into the two pinned staging buffers, each chunk's device copy
+// overlapping the host copy of the next.  On return the source has been read
+// (the caller may free it); the last device copies may still be in flight.
+void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
+{
+    if (!bytes) return;
+    if (bytes < 2 * kStageChunk || host_pinned(src)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+        return;
+    }
+    ensure_stage(h);
+    const uint64_t n = (bytes + kStageChunk - 1) / kStageChunk;
+    for (uint64_t c = 0; c < n; ++c) {
+        const uint64_t len = std::min(kStageChunk, bytes - c * kStageChunk);
+        // the buffer's previous device copy (chunk c-2, or an earlier call's) has finished
+        CK(cudaEventSynchronize(h->stage_ev[c & 1]));
+        host_copy_parallel(static_cast<char*>(h->stage[c & 1]), static_cast<const char*>(src) + c * kStageChunk, len);
+        CK(cudaMemcpyAsync(static_cast<char*>(dst) + c * kStageChunk, h->stage[c & 1], len, cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
     }
 }
 
@@ -1851,7 +1918,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
 
         cudaStream_t st = h->stream;
         CK(cudaMemcpyAsync(h->d_doc_off, doc_off, (D + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        if (n_all) CK(cudaMemcpyAsync(h->d_words, wid, n_all * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        h2d(h, h->d_words, wid, n_all * sizeof(uint32_t));
         CK(cudaMemcpyAsync(h->d_doc_order, order.data(), D * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(h->d_alpha, h->alpha.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(h->d_dg_points, dg.data(), dg.size() * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -1859,7 +1926,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         CK(cudaMemsetAsync(h->d_nkw[0], 0, (uint64_t)K * V * sizeof(int32_t), st));
         CK(cudaMemsetAsync(h->d_nk[0], 0, K * sizeof(int32_t), st));
         if (z0) {
-            if (n_all) CK(cudaMemcpyAsync(h->d_z, z0, n_all * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+            h2d(h, h->d_z, z0, n_all * sizeof(uint16_t));
         } else if (n_all) {
             std::vector<float> acum(K);
             float s = 0.f;
@@ -1872,7 +1939,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             launch_check(h);
         }
         if (D && h->weighted) {
-            if (n_all) CK(cudaMemcpyAsync(h->d_wt, weights, n_all * sizeof(float), cudaMemcpyHostToDevice, st));
+            h2d(h, h->d_wt, weights, n_all * sizeof(float));
             CK(cudaMemsetAsync(h->d_dkw, 0, (uint64_t)K * V * sizeof(long long), st));
             CK(cudaMemsetAsync(h->d_dk, 0, K * sizeof(long long), st));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D + 127) / 128);
@@ -2182,7 +2249,7 @@ tmt_status tmt_set_counts(tmt_handle* h, const int32_t* n_kw, const int32_t* n_k
         if (!n_kw || !n_k) throw ArgError("n_kw / n_k is NULL");
         if (h->weighted) throw StateError("set_counts takes integer counts; this corpus has weighted counts");
         const uint64_t kv = (uint64_t)h->cfg.K * h->cfg.V;
-        if (kv) CK(cudaMemcpyAsync(h->d_nkw[h->cur], n_kw, kv * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        h2d(h, h->d_nkw[h->cur], n_kw, kv * sizeof(int32_t));
         CK(cudaMemcpyAsync(h->d_nk[h->cur], n_k, h->cfg.K * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     });
@@ -2268,7 +2335,7 @@ tmt_status tmt_set_counts_f32(tmt_handle* h, const float* n_kw, const float* n_k
             if (!(n_kw[i] >= 0.f) || !std::isfinite(n_kw[i])) throw ArgError("n_kw holds a negative or non-finite value");
         for (uint32_t k = 0; k < h->cfg.K; ++k)
             if (!(n_k[k] >= 0.f) || !std::isfinite(n_k[k])) throw ArgError("n_k holds a negative or non-finite value");
-        if (kv) CK(cudaMemcpyAsync(h->d_nkw[0], n_kw, kv * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        h2d(h, h->d_nkw[0], n_kw, kv * sizeof(float));
         CK(cudaMemcpyAsync(h->d_nk[0], n_k, h->cfg.K * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     });
