@@ -1887,7 +1887,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         h->d_partials = h->dalloc<double>(2 * (size_t)h->n_partials);
         h->ll_cap = 0;
         h->d_ll = nullptr;
-        std::vector<float> dg = tmt::build_digamma_points();
+        const std::vector<float>& dg = tmt::digamma_points();
         h->d_dg_points = h->dalloc<float>(dg.size());
         h->n_apart = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 4, (D + 63) / 64));
         h->d_part_nom = h->dalloc<double>((size_t)h->n_apart * K);

@@ -13,6 +13,8 @@
 #include <cstdint>
 #include <cstddef>
 #include <vector>
+#include <thread>
+#include <algorithm>
 #include "philox.cuh"   // TMT_HD
 
 namespace tmt {
@@ -95,16 +97,45 @@ inline float digamma_series_f(float x)
     return acc;
 }
 
+// point i of the table (each point is independent of the others)
+inline float digamma_point(size_t i)
+{
+    using T_ = DigammaTable;
+    const float P = (float)(1. / T_::S), Q = (float)(1. / T_::T), R = (float)(1. / T_::U);
+    if (i < (size_t)T_::N) return digamma_series_f(i ? i * P : (float)0.0001);
+    i -= T_::N;
+    if (i < (size_t)T_::M) return digamma_series_f(i * Q + T_::N * P);
+    i -= T_::M;
+    return digamma_series_f(i * R + T_::N * P + T_::M * Q);
+}
+
 inline std::vector<float> build_digamma_points()
 {
     using T_ = DigammaTable;
     std::vector<float> p(T_::N + T_::M + T_::L);
-    const float P = (float)(1. / T_::S), Q = (float)(1. / T_::T), R = (float)(1. / T_::U);
-    for (size_t i = 0; i < (size_t)T_::N; ++i) p[i] = digamma_series_f(i ? i * P : (float)0.0001);
-    for (size_t i = 0; i < (size_t)T_::M; ++i) p[i + T_::N] = digamma_series_f(i * Q + T_::N * P);
-    for (size_t i = 0; i < (size_t)T_::L; ++i)
-        p[i + T_::N + T_::M] = digamma_series_f(i * R + T_::N * P + T_::M * Q);
+    for (size_t i = 0; i < p.size(); ++i) p[i] = digamma_point(i);
     return p;
+}
+
+// The table's points, built once per process on up to 16 host threads: the
+// series recurses on halved arguments above 3, so the 11,424 points take tens
+// of milliseconds on one thread.  A pure function of the constants above.
+inline const std::vector<float>& digamma_points()
+{
+    static const std::vector<float> pts = [] {
+        using T_ = DigammaTable;
+        std::vector<float> p(T_::N + T_::M + T_::L);
+        const size_t n = p.size();
+        const size_t T = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < T; ++t)
+            th.emplace_back([&p, t, T, n] {
+                for (size_t i = t; i < n; i += T) p[i] = digamma_point(i);
+            });
+        for (auto& x : th) x.join();
+        return p;
+    }();
+    return pts;
 }
 
 TMT_HD float digamma_approx_f(float z)
