@@ -1153,7 +1153,11 @@ void host_copy_parallel(char* dst, const char* src, uint64_t bytes, uint32_t max
         const uint64_t b = (uint64_t)t * slice;
         if (b >= bytes) break;
         const uint64_t n = std::min(slice, bytes - b);
-        th.emplace_back([=] { std::memcpy(dst + b, src + b, n); });
+        try {
+            th.emplace_back([=] { std::memcpy(dst + b, src + b, n); });
+        } catch (...) {
+            std::memcpy(dst + b, src + b, n);     // no thread to be had: this one copies the slice
+        }
     }
     for (auto& x : th) x.join();
 }

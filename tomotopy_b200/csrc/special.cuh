@@ -127,11 +127,17 @@ inline const std::vector<float>& digamma_points()
         std::vector<float> p(T_::N + T_::M + T_::L);
         const size_t n = p.size();
         const size_t T = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+        auto part = [&p, T, n](size_t t) {
+            for (size_t i = t; i < n; i += T) p[i] = digamma_point(i);
+        };
         std::vector<std::thread> th;
-        for (size_t t = 0; t < T; ++t)
-            th.emplace_back([&p, t, T, n] {
-                for (size_t i = t; i < n; i += T) p[i] = digamma_point(i);
-            });
+        for (size_t t = 0; t < T; ++t) {
+            try {
+                th.emplace_back(part, t);
+            } catch (...) {
+                part(t);      // no thread to be had: this one computes the share
+            }
+        }
         for (auto& x : th) x.join();
         return p;
     }();
