@@ -9,6 +9,8 @@ Gates:
   (d) ll_per_word within 1% of the reference's sequential sampler at the same
       iteration count, averaged over seeds.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 from scipy import stats
@@ -87,6 +89,10 @@ def test_large_downloads_through_staging():
     check(lib.tmt_download_state(eng.h, _p(pz), _p(pkw), _p(nk2), _p(a2)), eng.h)
     np.testing.assert_array_equal(pz, z)
     np.testing.assert_array_equal(pkw.reshape(V, K), nkw)
+    # a destination in device memory takes one direct copy as well
+    dkw = torch.zeros(V * K, dtype=torch.int32, device="cuda")
+    check(lib.tmt_download_state(eng.h, None, C.c_void_p(dkw.data_ptr()), None, None), eng.h)
+    np.testing.assert_array_equal(dkw.cpu().numpy().reshape(V, K), nkw)
     eng.close()
 
 

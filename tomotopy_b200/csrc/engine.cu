@@ -1164,12 +1164,14 @@ void host_copy_parallel(char* dst, const char* src, uint64_t bytes, uint32_t max
 
 constexpr uint64_t kStageChunk = 16ull << 20;
 
-bool host_pinned(const void* p)
+// true for memory CUDA knows (pinned host, device or managed memory): one
+// direct copy serves it; false for plain pageable host memory
+bool cuda_visible(const void* p)
 {
     cudaPointerAttributes at{};
-    const bool pinned = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    const bool known = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type != cudaMemoryTypeUnregistered;
     cudaGetLastError();
-    return pinned;
+    return known;
 }
 
 // the handle's two pinned staging buffers, allocated on first use
@@ -1188,7 +1190,8 @@ void ensure_stage(tmt_handle* h)
 }
 
 // Device -> host copy on the handle's stream, synchronous on return.  A
-// pinned destination (or a small copy) takes one cudaMemcpyAsync; a large
+// destination CUDA knows (pinned, or device memory), or a small copy, takes
+// one cudaMemcpyAsync; a large
 // pageable one goes through two pinned staging buffers, the device copy of a
 // chunk overlapping the copy of the one before by 16 host threads.  Measured
 // on B200's host, 808 MB into freshly mapped memory: 48-63 ms, against
@@ -1198,8 +1201,8 @@ void ensure_stage(tmt_handle* h)
 void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
-    if (bytes < 2 * kStageChunk || host_pinned(dst)) {
-        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (bytes < 2 * kStageChunk || cuda_visible(dst)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         return;
     }
@@ -1221,8 +1224,8 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
     }
 }
 
-// Host -> device copy ordered on the handle's stream.  A pinned source (or a
-// small copy) takes one cudaMemcpyAsync; a large pageable one is copied by 8
+// Host -> device copy ordered on the handle's stream.  A source CUDA knows
+// (pinned, or device memory), or a small copy, takes one cudaMemcpyAsync; a large pageable one is copied by 8
 // host threads into the two pinned staging buffers, each chunk's device copy
 // overlapping the host copy of the next (808 MB: 27-32 ms against 77 ms for
 // the driver's pageable path, measured on B200's host).  On return the source
@@ -1231,8 +1234,8 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
-    if (bytes < 2 * kStageChunk || host_pinned(src)) {
-        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    if (bytes < 2 * kStageChunk || cuda_visible(src)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream));
         return;
     }
     ensure_stage(h);
