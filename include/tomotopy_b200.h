@@ -173,9 +173,10 @@ tmt_status tmt_ll(tmt_handle* h, double* ll_docs, double* ll_rest);
 /* Downloads the model state (any pointer may be NULL): z doc-major
  * (N_all uint16, 0xFFFF for skipped words; DocumentLDA::Zs), n_kw (K x V
  * column-major), n_k (K), alpha (K, after optimisation).  Synchronous.  This
- * and the other downloads copy into pinned (cudaHostAlloc'd or registered)
- * destinations directly; a pageable destination above 32 MB is filled through
- * the handle's two 16 MB pinned staging buffers by up to 16 host threads. */
+ * and the other downloads copy directly into memory CUDA knows (pinned host
+ * memory, or device or managed memory); a plain pageable destination above
+ * 32 MB is filled through the handle's two 16 MB pinned staging buffers by up
+ * to 16 host threads. */
 tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t* n_k, float* alpha);
 
 /* Replaces the topic-word state with host arrays n_kw (K x V column-major)
