@@ -89,6 +89,23 @@ def test_large_downloads_through_staging():
     check(lib.tmt_download_state(eng.h, _p(pz), _p(pkw), _p(nk2), _p(a2)), eng.h)
     np.testing.assert_array_equal(pz, z)
     np.testing.assert_array_equal(pkw.reshape(V, K), nkw)
+    # two handles staging at once from two threads (the process's staging
+    # buffers serve one transfer at a time)
+    import threading
+    other = T.Engine(K, V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
+    other.upload(off, w)
+    other.train(2)
+    got = {}
+    ths = [threading.Thread(target=lambda k, e: got.__setitem__(k, e.state()), args=(k, e))
+           for k, e in (("a", eng), ("b", other))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    for k in ("a", "b"):
+        np.testing.assert_array_equal(got[k][0], z)
+        np.testing.assert_array_equal(got[k][1], nkw)
+    other.close()
     # a destination in device memory takes one direct copy as well
     dkw = torch.zeros(V * K, dtype=torch.int32, device="cuda")
     check(lib.tmt_download_state(eng.h, None, C.c_void_p(dkw.data_ptr()), None, None), eng.h)

@@ -940,8 +940,7 @@ struct tmt_handle {
     uint32_t sweeps_timed = 0;
     int num_sms = 0;
     std::string err;
-    void* stage[2] = {nullptr, nullptr};          // pinned staging of downloads to pageable memory
-    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};   // the staged transfers' chunk events
 
     uint64_t D = 0, N_all = 0, N = 0, global_step = 0, bytes = 0, launches = 0;
     int sampler_used = 0;
@@ -1079,10 +1078,8 @@ struct tmt_handle {
     ~tmt_handle()
     {
         release();
-        for (int i = 0; i < 2; ++i) {
-            if (stage[i]) cudaFreeHost(stage[i]);
+        for (int i = 0; i < 2; ++i)
             if (stage_ev[i]) cudaEventDestroy(stage_ev[i]);
-        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (kev0) cudaEventDestroy(kev0);
@@ -1174,30 +1171,46 @@ bool cuda_visible(const void* p)
     return known;
 }
 
-// the handle's two pinned staging buffers, allocated on first use
-void ensure_stage(tmt_handle* h)
+// Two 16 MB pinned staging buffers shared by every handle of the process:
+// allocated on the first staged transfer and kept until the process exits
+// (32 MB of pinned host memory).  Pinning took 16-56 ms and unpinning up to
+// 1.2 s per pair on B200's host, too much to pay per handle.  One staged
+// transfer at a time holds them (handles on other threads wait).
+struct StagePool {
+    std::mutex m;
+    void* buf[2] = {nullptr, nullptr};
+};
+
+StagePool& stage_pool()
+{
+    static StagePool* p = new StagePool();   // never destroyed: outlives every handle
+    return *p;
+}
+
+// with the pool's lock held: the buffers, and the handle's two events
+void** ensure_stage(tmt_handle* h, StagePool& pool)
 {
     for (int i = 0; i < 2; ++i) {
-        if (!h->stage[i]) {
-            if (cudaHostAlloc(&h->stage[i], kStageChunk, cudaHostAllocDefault) != cudaSuccess) {
+        if (!pool.buf[i]) {
+            if (cudaHostAlloc(&pool.buf[i], kStageChunk, cudaHostAllocPortable) != cudaSuccess) {
                 cudaGetLastError();
-                h->stage[i] = nullptr;
+                pool.buf[i] = nullptr;
                 throw OomError("pinned staging buffer allocation failed");
             }
         }
         if (!h->stage_ev[i]) CK(cudaEventCreateWithFlags(&h->stage_ev[i], cudaEventDisableTiming));
     }
+    return pool.buf;
 }
 
 // Device -> host copy on the handle's stream, synchronous on return.  A
 // destination CUDA knows (pinned, or device memory), or a small copy, takes
-// one cudaMemcpyAsync; a large
-// pageable one goes through two pinned staging buffers, the device copy of a
-// chunk overlapping the copy of the one before by 16 host threads.  Measured
-// on B200's host, 808 MB into freshly mapped memory: 48-63 ms, against
-// 370-380 ms for the driver's pageable path, which copies and takes the page
-// faults on one thread (populating the pages with more threads beside the
-// copies measured slower: 72-128 ms).
+// one cudaMemcpyAsync; a large pageable one goes through the two pinned
+// staging buffers, the device copy of a chunk overlapping the copy of the one
+// before by 16 host threads.  Measured on B200's host, 808 MB into freshly
+// mapped memory: 48-63 ms, against 370-380 ms for the driver's pageable path,
+// which copies and takes the page faults on one thread (populating the pages
+// with more threads beside the copies measured slower: 72-128 ms).
 void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
@@ -1206,11 +1219,13 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         CK(cudaStreamSynchronize(h->stream));
         return;
     }
-    ensure_stage(h);
+    StagePool& pool = stage_pool();
+    std::lock_guard<std::mutex> lock(pool.m);
+    void** stage = ensure_stage(h, pool);
     const uint64_t n = (bytes + kStageChunk - 1) / kStageChunk;
     auto len = [&](uint64_t c) { return std::min(kStageChunk, bytes - c * kStageChunk); };
     auto issue = [&](uint64_t c) {
-        CK(cudaMemcpyAsync(h->stage[c & 1], static_cast<const char*>(src) + c * kStageChunk, len(c),
+        CK(cudaMemcpyAsync(stage[c & 1], static_cast<const char*>(src) + c * kStageChunk, len(c),
                            cudaMemcpyDeviceToHost, h->stream));
         CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
     };
@@ -1219,18 +1234,17 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         // buffer (c+1)&1 last held chunk c-1, whose host copy has finished
         if (c + 1 < n) issue(c + 1);
         CK(cudaEventSynchronize(h->stage_ev[c & 1]));
-        host_copy_parallel(static_cast<char*>(dst) + c * kStageChunk, static_cast<const char*>(h->stage[c & 1]),
-                           len(c));
+        host_copy_parallel(static_cast<char*>(dst) + c * kStageChunk, static_cast<const char*>(stage[c & 1]), len(c));
     }
 }
 
 // Host -> device copy ordered on the handle's stream.  A source CUDA knows
-// (pinned, or device memory), or a small copy, takes one cudaMemcpyAsync; a large pageable one is copied by 8
-// host threads into the two pinned staging buffers, each chunk's device copy
-// overlapping the host copy of the next (808 MB: 27-32 ms against 77 ms for
-// the driver's pageable path, measured on B200's host).  On return the source
-// has been read (the caller may free it); the last device copies may still
-// be in flight.
+// (pinned, or device memory), or a small copy, takes one cudaMemcpyAsync; a
+// large pageable one is copied by 8 host threads into the two pinned staging
+// buffers, each chunk's device copy overlapping the host copy of the next
+// (808 MB: 27-32 ms against 77 ms for the driver's pageable path, measured on
+// B200's host).  On return the source has been read and, for a staged copy,
+// the device copies have finished (the buffers are free for the next user).
 void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
@@ -1238,18 +1252,20 @@ void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream));
         return;
     }
-    ensure_stage(h);
+    StagePool& pool = stage_pool();
+    std::lock_guard<std::mutex> lock(pool.m);
+    void** stage = ensure_stage(h, pool);
     const uint64_t n = (bytes + kStageChunk - 1) / kStageChunk;
     for (uint64_t c = 0; c < n; ++c) {
         const uint64_t len = std::min(kStageChunk, bytes - c * kStageChunk);
-        // the buffer's previous device copy (chunk c-2, or an earlier call's) has finished
-        CK(cudaEventSynchronize(h->stage_ev[c & 1]));
-        host_copy_parallel(static_cast<char*>(h->stage[c & 1]), static_cast<const char*>(src) + c * kStageChunk, len,
-                           8);
-        CK(cudaMemcpyAsync(static_cast<char*>(dst) + c * kStageChunk, h->stage[c & 1], len, cudaMemcpyHostToDevice,
+        // the buffer's previous device copy (chunk c-2) has finished
+        if (c >= 2) CK(cudaEventSynchronize(h->stage_ev[c & 1]));
+        host_copy_parallel(static_cast<char*>(stage[c & 1]), static_cast<const char*>(src) + c * kStageChunk, len, 8);
+        CK(cudaMemcpyAsync(static_cast<char*>(dst) + c * kStageChunk, stage[c & 1], len, cudaMemcpyHostToDevice,
                            h->stream));
         CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
     }
+    CK(cudaEventSynchronize(h->stage_ev[(n - 1) & 1]));   // stream order: every chunk has landed
 }
 
 struct SweepShape {
