@@ -137,6 +137,19 @@ def test_pageable_uploads_through_staging():
     np.testing.assert_array_equal(za, zb)
     np.testing.assert_array_equal(kwa, kwb)
     np.testing.assert_array_equal(ka, kb)
+    # weighted counts: 34 MB of token weights staged from pageable memory
+    wts = (1.0 + (np.arange(len(w)) % 7) * 0.25).astype(np.float32)
+    pwt = torch.from_numpy(wts).pin_memory().numpy()
+    wa = T.Engine(K, V, alpha=0.1, eta=0.01, seed=5, optim_interval=0)
+    wb = T.Engine(K, V, alpha=0.1, eta=0.01, seed=5, optim_interval=0)
+    wa.upload(off, w, weights=wts)
+    wb.upload(off, pw, weights=pwt)
+    wa.train(1)
+    wb.train(1)
+    for x, y in zip(wa.state(), wb.state()):
+        np.testing.assert_array_equal(x, y)
+    wa.close()
+    wb.close()
     # counts set from pageable memory (36 MB) come back unchanged
     kw2 = np.ascontiguousarray(kwa[::-1])
     check(lib.tmt_set_counts(b.h, _p(kw2), _p(ka)), b.h)
