@@ -106,6 +106,16 @@ def test_large_downloads_through_staging():
         np.testing.assert_array_equal(got[k][0], z)
         np.testing.assert_array_equal(got[k][1], nkw)
     other.close()
+    # batched inference whose theta (9,000 x 1,000 floats, 36 MB) is staged
+    # into pageable memory equals the same call into pinned memory
+    th1, ll1 = eng.infer(off, w, iters=3, seed=2)
+    pth = torch.empty((len(off) - 1) * K, dtype=torch.float32).pin_memory().numpy()
+    pll = np.zeros(len(off) - 1, np.float64)
+    check(lib.tmt_infer_batch(eng.h, _p(np.ascontiguousarray(w, dtype=np.uint32)),
+                              _p(np.ascontiguousarray(off, dtype=np.uint64)), len(off) - 1, 3, 2, None,
+                              _p(pth), _p(pll)), eng.h)
+    np.testing.assert_array_equal(th1, pth.reshape(-1, K))
+    np.testing.assert_array_equal(ll1, pll)
     # a destination in device memory takes one direct copy as well
     dkw = torch.zeros(V * K, dtype=torch.int32, device="cuda")
     check(lib.tmt_download_state(eng.h, None, C.c_void_p(dkw.data_ptr()), None, None), eng.h)

@@ -2498,9 +2498,8 @@ tmt_status infer_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_of
         for (uint32_t k = 0; k < K; ++k) { sf = sf + h->alpha[k]; acum[k] = sf; sd += (double)h->alpha[k]; }
         cudaStream_t st = h->stream;
         CK(cudaMemcpyAsync(B.doc_off, doc_off, (D + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        if (n_all) CK(cudaMemcpyAsync(B.words, sorted.data(), n_all * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        if (weights && n_all)
-            CK(cudaMemcpyAsync(B.wt, wsorted.data(), n_all * sizeof(float), cudaMemcpyHostToDevice, st));
+        h2d(h, B.words, sorted.data(), n_all * sizeof(uint32_t));
+        if (weights) h2d(h, B.wt, wsorted.data(), n_all * sizeof(float));
         if (doc_keys) CK(cudaMemcpyAsync(B.keys, doc_keys, D * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(B.acum, acum.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(B.counter, 0, sizeof(uint32_t), st));
@@ -2542,7 +2541,7 @@ tmt_status infer_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_of
         a.ecum = h->d_cum_eta;
         launch_infer(a, h->num_sms, h->stream);
         ++h->launches;
-        if (theta) CK(cudaMemcpyAsync(theta, B.theta, D * (uint64_t)K * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (theta) d2h(h, theta, B.theta, D * (uint64_t)K * sizeof(float));
         if (ll) CK(cudaMemcpyAsync(ll, B.ll, D * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
     });
