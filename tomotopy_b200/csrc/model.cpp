@@ -27,6 +27,9 @@
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
+#include <memory>
+#include <type_traits>
+#include <utility>
 #include "../../include/tomotopy_b200.h"
 
 namespace {
@@ -160,6 +163,33 @@ struct Doc {
 
 } // namespace
 
+// An allocator whose value-less construct leaves trivial elements
+// uninitialised: resize() then reserves the pages without writing them, and
+// the engine's threaded download is the first to touch them (a zero fill of
+// a 4 GB n_dk on one thread first took seconds).
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value)
+    {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a)
+    {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using HostBuf = std::vector<T, NoInit<T>>;
+
 struct tmt_model {
     // hyper-parameters (LDAArgs, LDAModel.hpp:962-983)
     uint32_t K = 1;
@@ -187,8 +217,8 @@ struct tmt_model {
     tmt_handle* eng = nullptr;
     // host copies, refreshed on demand
     bool host_fresh = false;
-    std::vector<int32_t> nkw, nk, ndk;
-    std::vector<float> nkw_f, nk_f, ndk_f;   // the same for weighted counts
+    HostBuf<int32_t> nkw, nk, ndk;
+    HostBuf<float> nkw_f, nk_f, ndk_f;   // the same for weighted counts
     std::string err;
 
     ~tmt_model()
@@ -214,19 +244,20 @@ struct tmt_model {
     void refresh()
     {
         if (host_fresh || !eng) return;
-        std::vector<uint16_t> z(realN_all());
+        // every element is written by the downloads: sized, not filled
+        HostBuf<uint16_t> z(realN_all());
         if (tw) {
-            nkw_f.assign((uint64_t)K * realV, 0.f);
-            nk_f.assign(K, 0.f);
-            ndk_f.assign((uint64_t)docs.size() * K, 0.f);
+            nkw_f.resize((uint64_t)K * realV);
+            nk_f.resize(K);
+            ndk_f.resize((uint64_t)docs.size() * K);
             check(tmt_download_state(eng, z.data(), nullptr, nullptr, alphas.data()));
             check(tmt_download_counts_f32(eng, docs.empty() ? nullptr : ndk_f.data(), nkw_f.data(), nk_f.data(),
                                           nullptr));
         } else {
-            nkw.assign((uint64_t)K * realV, 0);
-            nk.assign(K, 0);
+            nkw.resize((uint64_t)K * realV);
+            nk.resize(K);
             check(tmt_download_state(eng, z.data(), nkw.data(), nk.data(), alphas.data()));
-            ndk.assign((uint64_t)docs.size() * K, 0);
+            ndk.resize((uint64_t)docs.size() * K);
             if (!docs.empty()) check(tmt_download_doc_topic(eng, ndk.data()));
         }
         uint64_t at = 0;
