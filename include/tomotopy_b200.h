@@ -175,7 +175,7 @@ tmt_status tmt_ll(tmt_handle* h, double* ll_docs, double* ll_rest);
  * column-major), n_k (K), alpha (K, after optimisation).  Synchronous.  This
  * and the other downloads copy directly into memory CUDA knows (pinned host
  * memory, or device or managed memory); a plain pageable destination above
- * 32 MB is filled through two 16 MB pinned staging buffers by up to 16 host
+ * 32 MB is filled through two 32 MB pinned staging buffers by up to 16 host
  * threads.  The staging buffers are shared by all handles of the process
  * (one staged transfer at a time) and kept until the process exits. */
 tmt_status tmt_download_state(tmt_handle* h, uint16_t* z, int32_t* n_kw, int32_t* n_k, float* alpha);

@@ -1159,7 +1159,7 @@ void host_copy_parallel(char* dst, const char* src, uint64_t bytes, uint32_t max
     for (auto& x : th) x.join();
 }
 
-constexpr uint64_t kStageChunk = 16ull << 20;
+constexpr uint64_t kStageChunk = 32ull << 20;   // a staging buffer; staged transfers are >= 32 MB
 
 // true for memory CUDA knows (pinned host, device or managed memory): one
 // direct copy serves it; false for plain pageable host memory
@@ -1171,9 +1171,9 @@ bool cuda_visible(const void* p)
     return known;
 }
 
-// Two 16 MB pinned staging buffers shared by every handle of the process:
+// Two 32 MB pinned staging buffers shared by every handle of the process:
 // allocated on the first staged transfer and kept until the process exits
-// (32 MB of pinned host memory).  Pinning took 16-56 ms and unpinning up to
+// (64 MB of pinned host memory).  Pinning took 16-56 ms and unpinning up to
 // 1.2 s per pair on B200's host, too much to pay per handle.  One staged
 // transfer at a time holds them (handles on other threads wait).
 struct StagePool {
@@ -1208,13 +1208,14 @@ void** ensure_stage(tmt_handle* h, StagePool& pool)
 // one cudaMemcpyAsync; a large pageable one goes through the two pinned
 // staging buffers, the device copy of a chunk overlapping the copy of the one
 // before by 16 host threads.  Measured on B200's host, 808 MB into freshly
-// mapped memory: 48-63 ms, against 370-380 ms for the driver's pageable path,
-// which copies and takes the page faults on one thread (populating the pages
-// with more threads beside the copies measured slower: 72-128 ms).
+// mapped memory: 40-41 ms with 32 MB chunks (47-53 ms with 16 MB, 71-96 ms
+// with 8 MB), against 370-380 ms for the driver's pageable path, which copies
+// and takes the page faults on one thread (populating the pages with more
+// threads beside the copies measured slower).
 void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
-    if (bytes < 2 * kStageChunk || cuda_visible(dst)) {
+    if (bytes < kStageChunk || cuda_visible(dst)) {
         CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         return;
@@ -1240,15 +1241,15 @@ void d2h(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 
 // Host -> device copy ordered on the handle's stream.  A source CUDA knows
 // (pinned, or device memory), or a small copy, takes one cudaMemcpyAsync; a
-// large pageable one is copied by 8 host threads into the two pinned staging
-// buffers, each chunk's device copy overlapping the host copy of the next
-// (808 MB: 27-32 ms against 77 ms for the driver's pageable path, measured on
-// B200's host).  On return the source has been read and, for a staged copy,
+// large pageable one is copied by 16 host threads into the two pinned
+// staging buffers, each chunk's device copy overlapping the host copy of the
+// next (808 MB: 24 ms against 77 ms for the driver's pageable path, measured
+// on B200's host).  On return the source has been read and, for a staged copy,
 // the device copies have finished (the buffers are free for the next user).
 void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
 {
     if (!bytes) return;
-    if (bytes < 2 * kStageChunk || cuda_visible(src)) {
+    if (bytes < kStageChunk || cuda_visible(src)) {
         CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream));
         return;
     }
@@ -1260,7 +1261,7 @@ void h2d(tmt_handle* h, void* dst, const void* src, uint64_t bytes)
         const uint64_t len = std::min(kStageChunk, bytes - c * kStageChunk);
         // the buffer's previous device copy (chunk c-2) has finished
         if (c >= 2) CK(cudaEventSynchronize(h->stage_ev[c & 1]));
-        host_copy_parallel(static_cast<char*>(stage[c & 1]), static_cast<const char*>(src) + c * kStageChunk, len, 8);
+        host_copy_parallel(static_cast<char*>(stage[c & 1]), static_cast<const char*>(src) + c * kStageChunk, len);
         CK(cudaMemcpyAsync(static_cast<char*>(dst) + c * kStageChunk, stage[c & 1], len, cudaMemcpyHostToDevice,
                            h->stream));
         CK(cudaEventRecord(h->stage_ev[c & 1], h->stream));
