@@ -123,6 +123,21 @@ def make_corpus(w, threads=0):
     return off, words, realV
 
 
+def idf_weights(off, words, V):
+    """TermWeight IDF per token (LDAModel.hpp:1093-1122): (float)log(D / df(w)),
+    df counted over documents; the prepared corpus holds each document's
+    words sorted, so a document's distinct words start its runs."""
+    D = len(off) - 1
+    o = off.astype(np.int64)
+    first = np.ones(len(words), bool)
+    first[1:] = words[1:] != words[:-1]
+    first[o[:-1][np.diff(o) > 0]] = True
+    ok = words < V
+    df = np.bincount(words[first & ok], minlength=V)[:V]
+    idf = np.log(D / np.maximum(df, 1).astype(np.float64)).astype(np.float32)
+    return np.where(ok, idf[np.minimum(words, V - 1)], np.float32(0)).astype(np.float32)
+
+
 def make_shard(w, rank, world):
     """Rank r's part of one corpus split across ranks: the documents
     [r*D, (r+1)*D) of the seeded generator, prepared with the vocabulary order
@@ -506,6 +521,8 @@ def main():
     ap.add_argument("--docs", type=int, default=0, help="override the document count (smaller case)")
     ap.add_argument("--groups", type=int, default=0, help="document groups per sweep (0: engine default)")
     ap.add_argument("--mode", default="train", choices=["train", "infer", "prepare"])
+    ap.add_argument("--tw", default="one", choices=["one", "idf"],
+                    help="train mode: term weighting of the corpus (idf: weighted counts, one GPU)")
     ap.add_argument("--requests", type=int, default=20000, help="infer mode: documents per run")
     ap.add_argument("--slots", type=int, default=8192, help="infer mode: server slots per model")
     ap.add_argument("--step-tokens", type=int, default=4096, help="infer mode: token-sweeps per document per step")
@@ -550,13 +567,19 @@ def main():
             e.upload_shard(o, ws, lens_global, rank * w["D"], rank, world)
     else:
         off, words, V = make_corpus(w)
+    wts = None
+    if args.tw != "one":
+        if world > 1:
+            raise SystemExit("--tw idf runs on one GPU (weighted counts are not sharded)")
+        wts = idf_weights(off, words, V)
+    if world == 1:
 
         def new_engine():
             return T.Engine(K, V, alpha=ALPHA, eta=ETA, seed=1, optim_interval=0, device=local,
                             sweep_groups=args.groups)
 
-        def upload(e, o, ws):
-            e.upload(o, ws)
+        def upload(e, o, ws, wt=None):
+            e.upload(o, ws, weights=wt)
 
     def total(x, op="sum"):
         t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
@@ -566,7 +589,10 @@ def main():
         return float(t.item())
 
     eng = new_engine()
-    upload(eng, off, words)
+    if wts is not None:
+        upload(eng, off, words, wts)
+    else:
+        upload(eng, off, words)
     info0 = eng.info()
     N = info0.N
     N_all_ranks = int(total(N))
@@ -599,17 +625,21 @@ def main():
         eng.close()
         pin_words = torch.from_numpy(words).pin_memory().numpy()
         pin_off = torch.from_numpy(off).pin_memory().numpy()
+        pin_wts = torch.from_numpy(wts).pin_memory().numpy() if wts is not None else None
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         te0 = time.perf_counter()
         e2e = new_engine()
-        upload(e2e, pin_off, pin_words)
+        if pin_wts is not None:
+            upload(e2e, pin_off, pin_words, pin_wts)
+        else:
+            upload(e2e, pin_off, pin_words)
         e2e.train(args.steps)
         ll = e2e.ll()
         z, nkw, nk, _ = e2e.state()
         te = total(time.perf_counter() - te0, "max")
-        h2d = pin_words.nbytes + pin_off.nbytes
+        h2d = pin_words.nbytes + pin_off.nbytes + (pin_wts.nbytes if pin_wts is not None else 0)
         d2h = z.nbytes + nkw.nbytes + nk.nbytes + 16
         e2e_obj = {"value": N_all_ranks * args.steps / te, "unit": "tokens/s",
                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
@@ -628,6 +658,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
             "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1) * world,
                        "tokens": N_all_ranks, "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups),
+                       "term_weight": args.tw,
                        "sweep_variants": variants,
                        "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
                                        if world > 1 else "dp1"),
@@ -635,7 +666,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": (MEASURED_TRAFFIC.get((args.config, int(len(off) - 1), int(info.sweep_groups)))
-                                     if world == 1 else None),
+                                     if world == 1 and args.tw == "one" else None),
                          "kernel": "k_sweep_doc", "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg,
                          "per": "one sweep = all k_sweep_doc + k_phi_copy launches of the document groups",
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
@@ -646,7 +677,7 @@ def main():
             "clocks": clk,
             "ll_per_word": (ll[0] + ll[1]) / N_all_ranks if N_all_ranks else 0.0,
         }
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and args.tw == "one":
             line["cpu_baseline"] = cpu_baseline_sample(w, off, words, V)
         print(json.dumps(line), flush=True)
     eng.close()
