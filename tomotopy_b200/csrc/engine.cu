@@ -293,8 +293,15 @@ __global__ void k_phi_fold_w(float* __restrict__ nkw, long long* __restrict__ dk
 __global__ void k_counts_w(const uint64_t* __restrict__ doc_off, const uint32_t* __restrict__ words,
                            const uint16_t* __restrict__ z, const float* __restrict__ wt, uint64_t D, uint32_t K,
                            uint32_t V, float* __restrict__ ndk, long long* __restrict__ dkw,
-                           long long* __restrict__ dk, float* __restrict__ doc_wlen)
+                           long long* __restrict__ dk, float* __restrict__ doc_wlen, bool dk_smem)
 {
+    // with dk_smem the block sums n_k's fixed-point deltas in shared memory
+    // (integers: any order gives the same sums) and adds them once at the end
+    extern __shared__ unsigned long long s_dk[];
+    if (dk_smem) {
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) s_dk[k] = 0;
+        __syncthreads();
+    }
     for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < D; d += (uint64_t)gridDim.x * blockDim.x) {
         float* row = ndk + d * K;
         float len = 0.f;
@@ -307,9 +314,15 @@ __global__ void k_counts_w(const uint64_t* __restrict__ doc_off, const uint32_t*
             len = __fadd_rn(len, w);
             const unsigned long long q = (unsigned long long)wq_of(w);
             atomicAdd(reinterpret_cast<unsigned long long*>(dkw) + (uint64_t)v * K + k, q);
-            atomicAdd(reinterpret_cast<unsigned long long*>(dk) + k, q);
+            if (dk_smem) atomicAdd(s_dk + k, q);
+            else atomicAdd(reinterpret_cast<unsigned long long*>(dk) + k, q);
         }
         doc_wlen[d] = len;
+    }
+    if (dk_smem) {
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+            if (s_dk[k]) atomicAdd(reinterpret_cast<unsigned long long*>(dk) + k, s_dk[k]);
     }
 }
 
@@ -1944,8 +1957,10 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             CK(cudaMemsetAsync(h->d_dkw, 0, (uint64_t)K * V * sizeof(long long), st));
             CK(cudaMemsetAsync(h->d_dk, 0, K * sizeof(long long), st));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D + 127) / 128);
-            k_counts_w<<<grid, 128, 0, st>>>(h->d_doc_off, h->d_words, h->d_z, h->d_wt, D, K, V,
-                                             reinterpret_cast<float*>(h->d_ndk), h->d_dkw, h->d_dk, h->d_doc_wlen);
+            const bool dk_smem = K <= 4096;     // at most 32 KB of shared memory
+            k_counts_w<<<grid, 128, dk_smem ? K * sizeof(long long) : 0, st>>>(
+                h->d_doc_off, h->d_words, h->d_z, h->d_wt, D, K, V, reinterpret_cast<float*>(h->d_ndk), h->d_dkw,
+                h->d_dk, h->d_doc_wlen, dk_smem);
             launch_check(h);
             k_nk_fold_w<<<1, 1024, 0, st>>>(reinterpret_cast<float*>(h->d_nk[0]), h->d_dk, K);
             launch_check(h);
