@@ -243,6 +243,22 @@ __device__ __forceinline__ float fold_w(float n, long long q)
     return s > 0.f ? s : 0.f;
 }
 
+// n_k's fixed-point deltas of a group: the column sums of the word deltas
+// (every token adds the same q to dkw[v][k] as to n_k's delta of k), summed
+// as integers, so any order gives the same value.  Block (x, y): topics
+// [256x, 256x + 256), word rows [y * rows, (y + 1) * rows).
+__global__ void k_dk_sum(const long long* __restrict__ dkw, uint32_t V, uint32_t K, uint32_t rows,
+                         long long* __restrict__ dk)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const uint64_t v0 = (uint64_t)blockIdx.y * rows;
+    const uint64_t v1 = v0 + rows < (uint64_t)V ? v0 + rows : (uint64_t)V;
+    unsigned long long sum = 0;
+    for (uint64_t v = v0; v < v1; ++v) sum += (unsigned long long)__ldg(dkw + v * K + k);
+    if (sum) atomicAdd(reinterpret_cast<unsigned long long*>(dk) + k, sum);
+}
+
 __global__ void k_nk_fold_w(float* __restrict__ nk, long long* __restrict__ dk, uint32_t K)
 {
     for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
@@ -394,16 +410,15 @@ k_sweep_doc(SweepArgs a)
     const int K = (int)a.K;
     const int KP = (int)round4(a.K);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // n_k deltas in shared memory: integer counts only (weighted counts take
+    // theirs from the word deltas after the sweep, k_dk_sum)
+    const bool dnk_smem = !WT && a.dnk_smem;
     int* s_dnk = smem;
-    long long* s_dnk64 = reinterpret_cast<long long*>(smem);
-    float* s_rowf = reinterpret_cast<float*>(smem + (a.dnk_smem ? (WT ? 2 * KP : KP) : 0));
+    float* s_rowf = reinterpret_cast<float*>(smem + (dnk_smem ? KP : 0));
     float* rowf = s_rowf + warp * KP;
     int* s_rowi = reinterpret_cast<int*>(s_rowf + nwarps * KP);
-    if (a.dnk_smem) {
-        for (int k = threadIdx.x; k < K; k += blockDim.x) {
-            if (WT) s_dnk64[k] = 0;
-            else s_dnk[k] = 0;
-        }
+    if (dnk_smem) {
+        for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
         __syncthreads();
     }
     // blocks of four owned by this lane
@@ -644,10 +659,7 @@ k_sweep_doc(SweepArgs a)
                                 unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
                                 atomicAdd(dw + zo, 0ull - q);
                                 atomicAdd(dw + znew, q);
-                                unsigned long long* dn = a.dnk_smem ? reinterpret_cast<unsigned long long*>(s_dnk64)
-                                                                    : reinterpret_cast<unsigned long long*>(a.dk);
-                                atomicAdd(dn + zo, 0ull - q);
-                                atomicAdd(dn + znew, q);
+                                // n_k's deltas are the column sums of these (k_dk_sum)
                             }
                         } else {
                             const int n = rowi[znew] + 1;
@@ -694,16 +706,10 @@ k_sweep_doc(SweepArgs a)
             for (int k = lane; k < K; k += 32) grow[k] = rowi[k];
         __syncwarp();
     }
-    if (a.dnk_smem) {
+    if (dnk_smem) {
         __syncthreads();
-        for (int k = threadIdx.x; k < K; k += blockDim.x) {
-            if constexpr (WT) {
-                if (s_dnk64[k])
-                    atomicAdd(reinterpret_cast<unsigned long long*>(a.dk) + k, (unsigned long long)s_dnk64[k]);
-            } else {
-                if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
-            }
-        }
+        for (int k = threadIdx.x; k < K; k += blockDim.x)
+            if (s_dnk[k]) atomicAdd(&a.nk_next[k], s_dnk[k]);
     }
 }
 
@@ -1295,10 +1301,12 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false)
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
     SweepShape s{};
-    s.dnk_smem = K <= (weighted ? 8192u : 16384u);
+    // weighted counts take n_k's deltas from the word deltas after the sweep
+    // (k_dk_sum): 64-bit shared-memory atomics per token cost ~17 ms a sweep
+    s.dnk_smem = !weighted && K <= 16384u;
     s.rowi_smem = K <= 8192 && !rowi_global;
     const uint32_t per_warp = 4 * KP + (s.rowi_smem ? 4 * KP : 0);
-    const uint32_t fixed = s.dnk_smem ? (weighted ? 8 : 4) * KP : 0;
+    const uint32_t fixed = s.dnk_smem ? 4 * KP : 0;
     uint32_t w = (budget - fixed) / per_warp;
     s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
     s.smem = fixed + s.warps * per_warp;
@@ -1490,13 +1498,21 @@ void do_sweep_w(tmt_handle* h, bool capture)
     const uint32_t smem_k = K <= 12288 ? K : 0;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->num_sms * 16, V));
     bool pending = false, recorded = false;
+    // n_k's deltas of the group just sampled, then its fold
+    const uint32_t gx = (K + 255) / 256;
+    const uint32_t gy = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((V + 63) / 64,
+                                                                          (uint64_t)h->num_sms * 8 / gx + 1));
+    const uint32_t rows = (V + gy - 1) / gy;
+    auto fold_nk = [&] {
+        k_dk_sum<<<dim3(gx, gy), 256, 0, h->stream>>>(h->d_dkw, V, K, rows, h->d_dk);
+        launch_check(h);
+        k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
+        launch_check(h);
+    };
     const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
     for (uint32_t g = 0; g < G; ++g) {
         if (h->group_bounds[g] == h->group_bounds[g + 1]) continue;
-        if (pending) {
-            k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
-            launch_check(h);
-        }
+        if (pending) fold_nk();
         k_phi_fold_w<<<grid, 256, smem_k * 4, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta,
                                                          h->d_phi, smem_k, pending ? 1 : 0, h->prior_args());
         launch_check(h);
@@ -1516,8 +1532,7 @@ void do_sweep_w(tmt_handle* h, bool capture)
         pending = true;
     }
     if (pending) {
-        k_nk_fold_w<<<1, 1024, 0, h->stream>>>(nk, h->d_dk, K);
-        launch_check(h);
+        fold_nk();
         k_phi_fold_w<<<grid, 256, 0, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta, nullptr, 0, 1,
                                                  h->prior_args());
         launch_check(h);
