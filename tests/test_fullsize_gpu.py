@@ -9,7 +9,10 @@ since the oracle's sequential sweep cannot finish there:
 - n_k sums to the number of valid tokens N;
 - the FP64 log-likelihood (getLLDocs + getLLRest, LDAModel.hpp:616-668) is
   finite and rises from the first sweep to the third, as collapsed Gibbs
-  sampling from a random start does on data drawn from the model.
+  sampling from a random start does on data drawn from the model;
+- the same seed gives the same z, another seed another z;
+- with TermWeight IDF token weights (LDAModel.hpp:1093-1122), n_k and n_kw
+  each sum to the total weight of the corpus.
 
 The recount runs on the device with torch bincount: it is the checker, not
 the path under test."""
@@ -25,12 +28,18 @@ LENGTH = ("lognormal", float(np.log(100)), 1.2, 5, 5000)
 SEED = 20261206
 
 
-@pytest.mark.gpu
-def test_full_size_counts_match_z_and_ll_rises():
-    import torch
-
+@pytest.fixture(scope="module")
+def corpus():
     off, words = T.synth_corpus(V_GEN, TOPICS, D, LENGTH, seed=SEED)
     off, words, V, _ = T.prepare_ids(off, words)
+    return off, words, V
+
+
+@pytest.mark.gpu
+def test_full_size_counts_match_z_and_ll_rises(corpus):
+    import torch
+
+    off, words, V = corpus
     eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=1, optim_interval=0)
     eng.upload(off, words)
     N = eng.info().N
@@ -64,3 +73,45 @@ def test_full_size_counts_match_z_and_ll_rises():
     assert torch.equal(nkw_d.long().sum(dim=1), cf)
     assert torch.equal(torch.from_numpy(nk).to(dev).long(), rec_nk)
     assert torch.equal(nkw_d.long(), rec_nkw)
+
+
+@pytest.mark.gpu
+def test_full_size_same_seed_same_z(corpus):
+    off, words, V = corpus
+    zs = []
+    for seed in (7, 7, 8):
+        eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
+        eng.upload(off, words)
+        eng.train(2)
+        zs.append(eng.state()[0])
+        eng.close()
+    assert np.array_equal(zs[0], zs[1])
+    assert not np.array_equal(zs[0], zs[2])
+
+
+def _idf(off, words, V):
+    """(float)log(D / df(w)) per token, df over documents (LDAModel.hpp:1093-1122);
+    each prepared document holds its words sorted, so a run start is a new word."""
+    o = off.astype(np.int64)
+    first = np.ones(len(words), bool)
+    first[1:] = words[1:] != words[:-1]
+    first[o[:-1][np.diff(o) > 0]] = True
+    ok = words < V
+    df = np.bincount(words[first & ok], minlength=V)[:V]
+    idf = np.log((len(off) - 1) / np.maximum(df, 1).astype(np.float64)).astype(np.float32)
+    return np.where(ok, idf[np.minimum(words, V - 1)], np.float32(0)).astype(np.float32)
+
+
+@pytest.mark.gpu
+def test_full_size_idf_counts_sum_to_total_weight(corpus):
+    off, words, V = corpus
+    wts = _idf(off, words, V)
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
+    eng.upload(off, words, weights=wts)
+    eng.train(2)
+    _, nkw, nk, _ = eng.state()
+    eng.close()
+    total = float(wts.astype(np.float64).sum())
+    assert float(nk.astype(np.float64).sum()) == pytest.approx(total, rel=1e-3)
+    assert float(nkw.astype(np.float64).sum()) == pytest.approx(total, rel=1e-3)
+    assert (nk >= 0).all() and (nkw >= 0).all()
