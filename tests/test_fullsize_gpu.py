@@ -12,7 +12,10 @@ since the oracle's sequential sweep cannot finish there:
   sampling from a random start does on data drawn from the model;
 - the same seed gives the same z, another seed another z;
 - with TermWeight IDF token weights (LDAModel.hpp:1093-1122), n_k and n_kw
-  each sum to the total weight of the corpus.
+  each sum to the total weight of the corpus;
+- inference of unseen documents (LDAModel::_infer, LDAModel.hpp:920-953)
+  against the full model gives a document the same theta and ll whatever
+  batch it comes in, and theta rows sum to 1.
 
 The recount runs on the device with torch bincount: it is the checker, not
 the path under test."""
@@ -31,15 +34,14 @@ SEED = 20261206
 @pytest.fixture(scope="module")
 def corpus():
     off, words = T.synth_corpus(V_GEN, TOPICS, D, LENGTH, seed=SEED)
-    off, words, V, _ = T.prepare_ids(off, words)
-    return off, words, V
+    return T.prepare_ids(off, words)      # (doc_off, words, V, vocabulary order)
 
 
 @pytest.mark.gpu
 def test_full_size_counts_match_z_and_ll_rises(corpus):
     import torch
 
-    off, words, V = corpus
+    off, words, V, _ = corpus
     eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=1, optim_interval=0)
     eng.upload(off, words)
     N = eng.info().N
@@ -77,7 +79,7 @@ def test_full_size_counts_match_z_and_ll_rises(corpus):
 
 @pytest.mark.gpu
 def test_full_size_same_seed_same_z(corpus):
-    off, words, V = corpus
+    off, words, V, _ = corpus
     zs = []
     for seed in (7, 7, 8):
         eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=seed, optim_interval=0)
@@ -104,7 +106,7 @@ def _idf(off, words, V):
 
 @pytest.mark.gpu
 def test_full_size_idf_counts_sum_to_total_weight(corpus):
-    off, words, V = corpus
+    off, words, V, _ = corpus
     wts = _idf(off, words, V)
     eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
     eng.upload(off, words, weights=wts)
@@ -115,3 +117,26 @@ def test_full_size_idf_counts_sum_to_total_weight(corpus):
     assert float(nk.astype(np.float64).sum()) == pytest.approx(total, rel=1e-3)
     assert float(nkw.astype(np.float64).sum()) == pytest.approx(total, rel=1e-3)
     assert (nk >= 0).all() and (nkw >= 0).all()
+
+
+@pytest.mark.gpu
+def test_full_size_infer_is_batch_independent(corpus):
+    off, words, V, order = corpus
+    eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=5, optim_interval=0)
+    eng.upload(off, words)
+    eng.train(2)
+    noff, nw = T.synth_corpus(V_GEN, TOPICS, 4000, LENGTH, seed=SEED + 1)
+    # generator ids -> the model's vocabulary; words it never saw become out-of-vocabulary
+    nw = np.where(nw < len(order), order[np.minimum(nw, len(order) - 1)], V + 5).astype(np.uint32)
+    theta, ll = eng.infer(noff, nw, iters=20, seed=9)
+    assert np.isfinite(ll).all()
+    np.testing.assert_allclose(theta.sum(axis=1), 1.0, atol=1e-4)
+    t2, l2 = eng.infer(noff[:1001], nw[:int(noff[1000])], iters=20, seed=9)
+    np.testing.assert_array_equal(t2, theta[:1000])
+    np.testing.assert_array_equal(l2, ll[:1000])
+    for d in (0, 1234, 3999):
+        a, b = int(noff[d]), int(noff[d + 1])
+        t1, l1 = eng.infer(np.array([0, b - a], np.uint64), nw[a:b], iters=20, seed=9)
+        np.testing.assert_array_equal(t1[0], theta[d])
+        assert l1[0] == ll[d]
+    eng.close()
