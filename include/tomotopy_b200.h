@@ -386,14 +386,20 @@ tmt_status tmt_prepare_corpus_counted(uint64_t D, const uint64_t* doc_off, const
  * must not pick up the implicit device synchronisation cudaMalloc/cudaFree
  * can cause.  Its scratch is one static device array of 281 KB, held by
  * every GPU that loads this library until the process exits; it supports
- * K <= 32767 and rejects larger K with TMT_ERR_INVALID_ARGUMENT.  The first
- * call on a device looks up that array's device address (with the device
- * current) and caches it; make that first call before any stream capture.
- * All calls on a device share the scratch: calls that overlap on the GPU
- * race and give wrong sums -- serialise them (one stream, or events).  Each
- * call overwrites every scratch slot it reads, so no clearing is needed.
- * The launches are asynchronous on `stream`.  A message for a non-OK status
- * is written to err (err_len bytes, may be NULL). */
+ * K <= 32767 and rejects larger K with TMT_ERR_INVALID_ARGUMENT.  Every
+ * array must be device or managed memory (anything else is rejected before
+ * a launch).  The first call on a device -- and the first after its context
+ * changes, e.g. after cudaDeviceReset, which also replaces the array --
+ * looks up that array's device address (with the device current) and
+ * caches it; make that first call before any stream capture.  All calls on
+ * a device share the scratch: calls that overlap on the GPU race and give
+ * wrong sums -- serialise them (one stream, or events).  Each call
+ * overwrites every scratch slot it reads, so no clearing is needed.  The
+ * grid is tmt_ll's, so the result equals tmt_ll's bit for bit on the same
+ * counts.  A CUDA error already pending on the calling thread is reported
+ * (TMT_ERR_CUDA) and left pending, and nothing is launched.  The launches
+ * are asynchronous on `stream`.  A message for a non-OK status is written
+ * to err (err_len bytes, may be NULL). */
 tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, const int32_t* doc_len,
                                  const float* alpha, const int32_t* n_kw, uint32_t V, const int32_t* n_k,
                                  float eta, double* ll_out, void* stream, char* err, size_t err_len);

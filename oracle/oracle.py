@@ -13,7 +13,10 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = os.path.join(HERE, "liboracle.so")
+# TMT_ORACLE_LIB selects another build of the same source (e.g. the -O3
+# -march=native build of `make -C oracle native`; results are bit-identical:
+# no fast-math, no FMA contraction)
+_LIB = os.environ.get("TMT_ORACLE_LIB") or os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libtmtref.so")
 
 _u8p = C.POINTER(C.c_uint8)

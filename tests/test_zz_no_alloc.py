@@ -51,7 +51,31 @@ def test_noalloc_ll_matches_tmt_ll_on_two_calls():
         assert st == 0, msg
         torch.cuda.synchronize(dev)
         got = out.cpu().numpy()
-        np.testing.assert_allclose(got, [ref_docs, ref_rest], rtol=1e-12, atol=1e-9)
+        # tmt_ll's grid and summation order: the same bits
+        np.testing.assert_array_equal(got, [ref_docs, ref_rest])
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_host_arrays():
+    """A host array would be read by the kernels as a device address: it is
+    refused before anything is launched."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    K, V, D = 8, 20, 3
+    ndk = torch.zeros((D, K), dtype=torch.int32, device=dev)
+    doc_len = torch.zeros(D, dtype=torch.int32, device=dev)
+    alpha = torch.full((K,), 0.1, dtype=torch.float32, device=dev)
+    nkw = torch.zeros((V, K), dtype=torch.int32, device=dev)
+    out = torch.zeros(2, dtype=torch.float64, device=dev)
+    nk_host = np.zeros(K, dtype=np.int32)
+    err = C.create_string_buffer(256)
+    st = lib.tmt_ll_counts_noalloc(
+        C.c_void_p(ndk.data_ptr()), D, K, C.c_void_p(doc_len.data_ptr()), C.c_void_p(alpha.data_ptr()),
+        C.c_void_p(nkw.data_ptr()), V, nk_host.ctypes.data_as(C.c_void_p), 0.01, C.c_void_p(out.data_ptr()),
+        None, err, len(err))
+    assert st == -1 and b"n_k" in err.value, err.value
+    torch.cuda.synchronize(dev)
 
 
 def test_noalloc_rejects_k_beyond_scratch():

@@ -830,6 +830,43 @@ constexpr uint32_t kNoAllocMaxBlocks = 1184;
 constexpr uint32_t kNoAllocMaxK = 32767;
 static __device__ __align__(256) double g_ll_scratch[2 * kNoAllocMaxBlocks + kNoAllocMaxK + 2];
 
+// Blocks of the log-likelihood's partial-sum kernel on a GPU with `sms` SMs:
+// tmt_ll and tmt_ll_counts_noalloc use the same grid, so they add the same
+// terms in the same order.
+inline uint32_t ll_blocks(int sms)
+{
+    return std::min<uint32_t>(kNoAllocMaxBlocks, (uint32_t)std::max(1, sms * 8));
+}
+
+// The unique id of the calling thread's current CUDA context (0: none, or
+// the driver does not say).  The driver's cuCtxGetCurrent / cuCtxGetId are
+// reached through the runtime, so the library does not link the driver
+// library; ids are never reused within a process, unlike context handles.
+unsigned long long current_context_id()
+{
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+        cudaGetLastError();
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
 // ---------------------------------------------------------------------------
 // alpha optimisation (optimizeParameters / calcDigammaSum, LDAModel.hpp:221-265)
 // ---------------------------------------------------------------------------
@@ -1935,7 +1972,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         h->d_lg_alpha = h->dalloc<double>(K);
         h->d_asum_ll = h->dalloc<double>(2);
         h->d_llv = h->dalloc<double>(2);
-        h->n_partials = (uint32_t)std::max(1, h->num_sms * 8);
+        h->n_partials = ll_blocks(h->num_sms);
         h->d_partials = h->dalloc<double>(2 * (size_t)h->n_partials);
         h->ll_cap = 0;
         h->d_ll = nullptr;
@@ -2601,8 +2638,8 @@ tmt_status tmt_infer_batch_weighted(tmt_handle* h, const uint32_t* wid, const ui
 
 /* Allocation-free FP64 log-likelihood over caller-owned device counts.
  * Host code may not pass g_ll_scratch itself (its host-side name is not a
- * device address): the device address is looked up once per device with
- * cudaGetSymbolAddress, with that device current, and reused. */
+ * device address): the device address is looked up with cudaGetSymbolAddress,
+ * with the device current, once per device context, and reused. */
 tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, const int32_t* doc_len,
                                  const float* alpha, const int32_t* n_kw, uint32_t V, const int32_t* n_k,
                                  float eta, double* ll_out, void* stream, char* err, size_t err_len)
@@ -2621,29 +2658,63 @@ tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, co
     if (!ll_out || !alpha || !n_k || (D && (!n_dk || !doc_len)) || (V && !n_kw))
         return say(TMT_ERR_INVALID_ARGUMENT, "a required device pointer is NULL");
     if (!(eta > 0)) return say(TMT_ERR_INVALID_ARGUMENT, "eta must be > 0");
+    // an error left by the caller's own earlier work is reported as such and
+    // left in place; nothing is launched
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return say(TMT_ERR_CUDA, std::string("an earlier CUDA error is pending on this thread: ") +
+                                     cudaGetErrorString(e));
+    // every array must be device (or managed) memory: a host pointer handed
+    // to the kernels would fault on the GPU instead of failing here
+    const struct { const void* p; const char* name; } arrays[] = {
+        { n_dk, "n_dk" }, { doc_len, "doc_len" }, { alpha, "alpha" }, { n_kw, "n_kw" }, { n_k, "n_k" },
+        { ll_out, "ll_out" } };
+    for (const auto& a : arrays) {
+        if (!a.p) continue;
+        cudaPointerAttributes at{};
+        const cudaError_t pe = cudaPointerGetAttributes(&at, a.p);
+        if (pe != cudaSuccess) {
+            cudaGetLastError();
+            return say(TMT_ERR_INVALID_ARGUMENT, std::string(a.name) + " is not memory CUDA knows: " +
+                                                     cudaGetErrorString(pe));
+        }
+        if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+            return say(TMT_ERR_INVALID_ARGUMENT, std::string(a.name) + " is not device or managed memory");
+    }
+    // set-up, once per device context: the array's device address and the
+    // SM count.  A new context (cudaDeviceReset, or another context made
+    // current) has its own copy of the array, so the cache is keyed by the
+    // context's unique id.
+    struct Slot { unsigned long long ctx; double* ptr; int sms; };
     static std::mutex mu;
-    static double* scratch[64] = {};
-    static int sms[64] = {};
+    static Slot slots[64] = {};
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= 64) return say(TMT_ERR_UNSUPPORTED, "device ordinal above 63");
+    double* base = nullptr;
+    int sms = 0;
     {
         std::lock_guard<std::mutex> lock(mu);
-        if (!scratch[dev]) {
+        Slot& sl = slots[dev];
+        const unsigned long long ctx = current_context_id();
+        if (!sl.ptr || ctx == 0 || sl.ctx != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_ll_scratch);
             if (e != cudaSuccess)
                 return say(TMT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+            int n = 0;
+            e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess)
                 return say(TMT_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
-            scratch[dev] = static_cast<double*>(p);
+            sl = Slot{ current_context_id(), static_cast<double*>(p), n };
         }
+        base = sl.ptr;
+        sms = sl.sms;
     }
-    // the same grid as tmt_ll on this device, so both give the same sums
-    const uint32_t blocks = std::min<uint32_t>(kNoAllocMaxBlocks, (uint32_t)std::max(1, sms[dev] * 8));
-    double* partials = scratch[dev];                     // 2 * blocks, every slot overwritten
+    // tmt_ll's grid on this device (ll_blocks), so both give the same sums
+    const uint32_t blocks = ll_blocks(sms);
+    double* partials = base;                             // 2 * blocks, every slot overwritten
     double* lg_alpha = partials + 2 * kNoAllocMaxBlocks; // K, every slot overwritten
     double* asum = lg_alpha + kNoAllocMaxK;              // 2, overwritten
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -2652,6 +2723,7 @@ tmt_status tmt_ll_counts_noalloc(const int32_t* n_dk, uint64_t D, uint32_t K, co
     k_ll_partials<<<blocks, 256, 0, st>>>(n_dk, D, K, lg_alpha, alpha, doc_len, asum, n_kw, V, etad,
                                           std::lgamma(etad), partials, PriorArgs{}, nullptr, nullptr, nullptr);
     k_ll_final<<<1, 256, 0, st>>>(partials, blocks, n_k, K, (double)V * etad, ll_out, nullptr);
+    // no error was pending before the launches: one now is theirs
     e = cudaGetLastError();
     if (e != cudaSuccess) return say(TMT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     return say(TMT_OK, "");
