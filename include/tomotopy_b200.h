@@ -46,9 +46,12 @@ typedef struct tmt_handle tmt_handle;
 typedef enum tmt_sampler {
     TMT_SAMPLER_AUTO = 0,   /* the engine's choice: the dense sampler */
     TMT_SAMPLER_DENSE = 1,  /* full K-vector conditional per token */
-    TMT_SAMPLER_SPARSE = 2  /* accepted; runs the dense sampler (documents of the benchmark corpora
-                               keep ~160 nonzero topics at K = 1000, where the bucket decomposition
-                               would gather more per token than the dense pass loads) */
+    TMT_SAMPLER_SPARSE = 2  /* not built: tmt_create returns TMT_ERR_UNSUPPORTED.  The exact bucket
+                               decomposition of the conditional pays when documents and words hold
+                               few nonzero topics; documents of the benchmark corpora keep ~160
+                               nonzero topics at K = 1000 and their frequent words' columns are
+                               dense, so the buckets would gather more per token than the dense
+                               pass loads */
 } tmt_sampler;
 
 /* Model hyper-parameters.  Mirrors LDAArgs (LDA.h:170-176) plus the

@@ -91,3 +91,20 @@ def test_synth_poisson_mean():
     lens = np.diff(off.astype(np.int64))
     assert abs(lens.mean() - 150) < 2.0
     assert abs(lens.var() - 150) < 25
+
+
+def test_sparse_sampler_is_refused():
+    """TMT_SAMPLER_SPARSE is not built: tmt_create says so (TMT_ERR_UNSUPPORTED)
+    before touching a GPU, instead of running the dense sampler under that name."""
+    lib = _lib.lib
+    alpha = np.full(8, 0.1, np.float32)
+    cfg = _lib.TmtConfig(K=8, V=100, alpha=alpha.ctypes.data_as(C.POINTER(C.c_float)), alpha_scalar=0.1, eta=0.01,
+                      seed=1, optim_interval=0, burn_in=0, device=0, sampler=_lib.SAMPLER_SPARSE, hbm_budget=0,
+                      sweep_groups=0)
+    h = _lib._H()
+    st = lib.tmt_create(C.byref(cfg), C.byref(h))
+    try:
+        assert st == -5
+        assert b"sparse" in lib.tmt_last_error(h)
+    finally:
+        lib.tmt_destroy(h)

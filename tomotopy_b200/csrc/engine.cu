@@ -2071,6 +2071,11 @@ tmt_status tmt_create(const tmt_config* cfg, tmt_handle** out)
         *out = h;
         return TMT_ERR_INVALID_ARGUMENT;
     }
+    if (cfg->sampler == TMT_SAMPLER_SPARSE) {
+        h->err = "the sparse-bucket sampler is not built (the dense sampler is TMT_SAMPLER_DENSE / AUTO)";
+        *out = h;
+        return TMT_ERR_UNSUPPORTED;
+    }
     tmt_status s = guarded(h, [&] {
         h->groups = cfg->sweep_groups ? cfg->sweep_groups : 8;
         h->alpha.assign(cfg->K, cfg->alpha_scalar);
