@@ -49,11 +49,89 @@ def bytes_per_sweep(N, K, V):
     return N * (4 * K + 16) + 8 * K * V + 4 * (V + 1) + 8 * K
 
 
-# DRAM bytes of one sweep (k_sweep_doc + k_phi_copy over all document groups),
-# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of the same
-# workload (profiles/k_sweep_doc_c3_traffic.md); keyed by (config, D, groups).
-# Captured with sweep variant 2 in every group, the tuner's usual choice there.
-MEASURED_TRAFFIC = {("c3", 1000000, 8): 169.61e9}
+# DRAM bytes of one sweep measured by ncu outside the bench (dram__bytes_read.sum +
+# dram__bytes_write.sum), keyed by config: shown beside the roofline as the
+# capture it came from; the bench itself measures no DRAM traffic, so its
+# roofline.traffic stays null.
+NCU_TRAFFIC = {"c3": {"bytes_per_sweep": 169.61e9, "source": "profiles/k_sweep_doc_c3_traffic.md"}}
+
+
+# ll-parity runs: the benchmark corpora at the configurations' iteration
+# counts (the k=1000 one on its first 100,000 documents), against tomotopy's
+# PARTITION train() restated in the oracle (tests/golden/ll_partition.json,
+# written by tests/golden/make_ll_parity.py)
+PARITY = {
+    "c1": dict(config="c1", docs=0, iters=200),
+    "c2": dict(config="c2", docs=0, iters=500),
+    "c3s": dict(config="c3", docs=100000, iters=50),
+}
+PARITY_SEEDS = (1, 2, 3, 4, 5)
+PARITY_FILE = os.path.join(ROOT, "tests", "golden", "ll_partition.json")
+
+
+def parity_corpus(run):
+    """The prepared corpus of a parity run: (doc_off, words, realV, K, sha1 of the ids)."""
+    import hashlib
+    r = PARITY[run]
+    w = dict(WORKLOADS[r["config"]])
+    if r["docs"]:
+        w["D"] = r["docs"]
+    off, words, V = make_corpus(w)
+    h = hashlib.sha1()
+    h.update(np.ascontiguousarray(off, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(words, np.uint32).tobytes())
+    return off, words, V, w["K"], h.hexdigest()
+
+
+def gpu_parity(run, optim, seeds=PARITY_SEEDS, corpus=None):
+    """ll_per_word every 10 sweeps of the device sampler on a parity run's
+    corpus, per seed (tomotopy's defaults: alpha 0.1, eta 0.01, burn_in 0)."""
+    import tomotopy_b200 as T
+    off, words, V, K, sha = corpus or parity_corpus(run)
+    iters = PARITY[run]["iters"]
+    curves, ms = {}, []
+    for seed in seeds:
+        eng = T.Engine(K, V, alpha=ALPHA, eta=ETA, seed=seed, optim_interval=optim)
+        eng.upload(off, words)
+        ll = eng.train(iters, ll_every=10)
+        info = eng.info()
+        curves[str(seed)] = (ll / info.N).tolist()
+        ms.append(info.train_ms / iters)
+        eng.close()
+    return {"corpus_sha1": sha, "ll_per_word": curves, "ms_per_sweep": ms}
+
+
+def parity_compare(ref, gpu):
+    """Mean over seeds of the final ll_per_word, and the relative gap."""
+    r = float(np.mean([c[-1] for c in ref["ll_per_word"].values()]))
+    g = float(np.mean([c[-1] for c in gpu["ll_per_word"].values()]))
+    return {"ref_mean": r, "gpu_mean": g, "rel_gap": abs(g - r) / abs(r),
+            "ref_final": [c[-1] for c in ref["ll_per_word"].values()],
+            "gpu_final": [c[-1] for c in gpu["ll_per_word"].values()]}
+
+
+def run_parity(args):
+    """One JSON line per parity run in the fixture: the device sampler's
+    ll_per_word against tomotopy's PARTITION train() (oracle restatement) at
+    the same iteration count, 5 seeds."""
+    import torch
+    torch.cuda.set_device(0)
+    with open(PARITY_FILE) as f:
+        ref = json.load(f)["runs"]
+    corpora = {}
+    for key, r in sorted(ref.items()):
+        run = key.split("/")[0]
+        if args.config in PARITY and run != args.config:
+            continue
+        if run not in corpora:
+            corpora[run] = parity_corpus(run)
+        g = gpu_parity(run, r["optim_interval"], corpus=corpora[run])
+        cmp = parity_compare(r, g)
+        print(json.dumps({"metric": "ll_per_word at the same iteration count (device vs PARTITION)", "run": key,
+                          "K": r["K"], "V": r["V"], "D": r["D"], "N": r["N"], "iters": r["iters"],
+                          "optim_interval": r["optim_interval"], "same_corpus": g["corpus_sha1"] == r["corpus_sha1"],
+                          "ref_threads": r["threads"], "gpu_ms_per_sweep": float(np.mean(g["ms_per_sweep"])),
+                          **cmp}), flush=True)
 
 
 def peaks():
@@ -117,6 +195,72 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def load_oracle(native=True):
+    """The oracle (test infrastructure: the CPU baseline's restatement of
+    tomotopy's PARTITION train()), built for this host at -O3 -march=native
+    (bit-identical to the -O2 build: no fast-math, no FMA contraction)."""
+    odir = os.path.join(ROOT, "oracle")
+    if native and "oracle" not in sys.modules:
+        # always rebuilt (-B): a -march=native build from another machine may
+        # use instructions this host lacks
+        r = subprocess.run(["make", "-s", "-B", "-C", odir, "native"], capture_output=True, text=True)
+        if r.returncode == 0:
+            os.environ["TMT_ORACLE_LIB"] = os.path.join(odir, "liboracle_native.so")
+    sys.path.insert(0, odir)
+    import oracle as O
+    return O
+
+
+def host_cpu():
+    """CPU model and hardware threads of this host."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "threads": os.cpu_count() or 1}
+
+
+def tomotopy_probe():
+    """tomotopy itself, when importable here (its version and tp.isa); it is
+    not installable offline, so the CPU leg falls back to the oracle port."""
+    try:
+        import tomotopy as tp
+        return {"importable": True, "version": tp.__version__, "isa": tp.isa}
+    except Exception as e:
+        return {"importable": False, "why": type(e).__name__ + ": " + str(e)[:80]}
+
+
+def l2_statement(n_tokens, K, V):
+    """Whether the inputs exceed the 126 MB L2 between timed sweeps."""
+    mb_c, mb_kw = 4 * n_tokens / 1e6, 4 * K * V / 1e6
+    big = mb_c + mb_kw > 126
+    return (f"inputs {'larger' if big else 'smaller'} than L2 (corpus {mb_c:.0f} MB per GPU, n_kw {mb_kw:.0f} MB)"
+            + ("" if big else ": the state stays in L2 across sweeps, as it does in training"))
+
+
+def workload_config(cfg, w, world):
+    """The workload definition both arms print as `config`: the
+    configuration, its sizes and the model's hyper-parameters."""
+    return {"workload": workload_name(cfg, w), "K": w["K"], "V": w["V"], "D": w["D"] * world,
+            "alpha": ALPHA, "eta": ETA, "true_topics": w["T"], "length": list(w["length"]),
+            "generator_seed": w["seed"],
+            "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
+                            if world > 1 else "dp1")}
+
+
+def oracle_corpus(w):
+    """The workload's prepared corpus built by the oracle (no engine code)."""
+    O = load_oracle()
+    off, words = O.synth_corpus(w["V"], w["T"], w["D"], w["length"], seed=w["seed"])
+    off, words, realV, _ = O.prepare_ids(off, words)
+    return off, words, realV
+
+
 def make_corpus(w, threads=0):
     import tomotopy_b200 as T
     off, words = T.synth_corpus(w["V"], w["T"], w["D"], w["length"], seed=w["seed"], threads=threads)
@@ -171,18 +315,28 @@ def dist_env():
     return rank, world, local
 
 
+# tokens of the CPU arm's sample per sweep, by K: about a second of PARTITION
+# work per sweep on a host of a few dozen cores
+REF_SAMPLE_TOKENS = {20: 1_500_000, 100: 8_000_000, 1000: 3_000_000}
+
+
 def run_reference(args, w):
-    """tomotopy's PARTITION scheme restated on the host (oracle), all threads,
-    on a bounded sample of the workload's documents."""
+    """The reference arm: tomotopy's train() -- ParallelScheme::PARTITION on
+    every host thread (TopicModel.hpp:684-755, LDAModel.hpp:356-489) -- on the
+    host cores.  tomotopy cannot be built offline (its CMake fetches Eigen and
+    EigenRand), so the oracle's C restatement of PARTITION stands in, compiled
+    here at -O3 -march=native.  The corpus is the workload's, generated and
+    prepared by the oracle (no engine code is loaded); each step is one
+    PARTITION sweep over a bounded sample -- the workload's first documents --
+    so the run ends within minutes.  Rank 0 only."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    off, words, V = make_corpus(w)
+    probe = tomotopy_probe()
+    O = load_oracle()
+    off, words, V = oracle_corpus(w)
     cores = os.cpu_count() or 1
-    # bounded sample: a prefix of the documents, ~tokens so one sweep is ~1 s of host work
-    target = {20: 6_000_000, 100: 2_000_000, 1000: 600_000}.get(w["K"], 1_000_000)
+    target = REF_SAMPLE_TOKENS.get(w["K"], 2_000_000)
     D = int(np.searchsorted(off.astype(np.int64), target))
     D = max(1, min(D, len(off) - 1))
     soff = off[:D + 1].copy()
@@ -201,16 +355,24 @@ def run_reference(args, w):
     part.close()
     t = float(np.sum(times))
     value = c.N * args.steps / t
+    native = os.environ.get("TMT_ORACLE_LIB", "").endswith("liboracle_native.so")
+    sample = (f"the workload's first {D} documents ({c.N} tokens of {len(words)}), one PARTITION sweep per "
+              f"step, {cores} host threads")
     line = {
         "metric": METRIC, "value": value, "unit": "tokens/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
         "impl": "reference",
-        "config": {"workload": workload_name(args.config, w), "K": w["K"], "docs_sampled": D,
-                   "tokens_sampled": c.N},
-        "cpu_baseline": {"value": value, "unit": "tokens/s", "cores": cores, "kind": "port",
-                         "sample": f"first {D} docs ({c.N} tokens) of the workload, PARTITION scheme, "
-                                   f"{cores} host threads, one sweep per step"},
+        "config": dict(workload_config(args.config, w, world), l2=l2_statement(len(words), w["K"], w["V"])),
+        "corpus": {"realV": int(V), "tokens_all_ids": int(len(words)), "built_by": "oracle (synth + prepare restated)"},
+        "sample": {"docs": D, "tokens": int(c.N)},
+        "ll_per_word": st.ll_per_word(),
+        "ll_after_sweeps": args.warmup + args.steps,
+        "cpu_baseline": {"value": value, "unit": "tokens/s", "cores": cores, "kind": "port", "sample": sample,
+                         "cpu": host_cpu(),
+                         "build": ("gcc -O3 -march=native -ffp-contract=off" if native
+                                   else "gcc -O2 -ffp-contract=off (native build failed)"),
+                         "tomotopy": probe},
         "e2e": {"value": value, "unit": "tokens/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -222,9 +384,8 @@ def workload_name(cfg, w):
 
 
 def cpu_baseline_sample(w, off, words, V, seconds=10.0):
-    """The oracle's PARTITION port on the host, bounded to ~`seconds`."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    """The oracle's PARTITION port on the host (-O3 -march=native), bounded to ~`seconds`."""
+    O = load_oracle()
     cores = os.cpu_count() or 1
     target = {20: 3_000_000, 100: 1_000_000, 1000: 300_000}.get(w["K"], 500_000)
     D = int(np.searchsorted(off.astype(np.int64), target))
@@ -244,7 +405,8 @@ def cpu_baseline_sample(w, off, words, V, seconds=10.0):
         n += 1
     part.close()
     return {"value": c.N * n / t, "unit": "tokens/s", "cores": cores, "kind": "port",
-            "sample": f"first {D} docs ({c.N} tokens), {n} PARTITION sweeps on {cores} host threads"}
+            "sample": f"first {D} docs ({c.N} tokens), {n} PARTITION sweeps on {cores} host threads",
+            "cpu": host_cpu(), "tomotopy": tomotopy_probe()}
 
 
 INFER = {
@@ -434,8 +596,7 @@ def cpu_infer_baseline(engines, which, docs, iters, seconds=10.0):
     """tomotopy's per-document infer (LDAModel.hpp:920-953) restated in the
     oracle, one document per host thread."""
     from concurrent.futures import ThreadPoolExecutor
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = load_oracle()
     models = []
     for e in engines:
         _, nkw, nk, alpha = e.state()
@@ -515,13 +676,16 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=sorted(set(WORKLOADS) | set(INFER)))
+    ap.add_argument("--config", default="c3", choices=sorted(set(WORKLOADS) | set(INFER) | set(PARITY)))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI pass")
     ap.add_argument("--docs", type=int, default=0, help="override the document count (smaller case)")
     ap.add_argument("--groups", type=int, default=0, help="document groups per sweep (0: engine default)")
-    ap.add_argument("--mode", default="train", choices=["train", "infer", "prepare"])
+    ap.add_argument("--split", type=int, default=0,
+                    help="train mode: split documents of at least this many tokens (0: the engine's rule)")
+    ap.add_argument("--split-step", type=int, default=0, help="train mode: positions per slice between merges")
+    ap.add_argument("--mode", default="train", choices=["train", "infer", "prepare", "parity"])
     ap.add_argument("--tw", default="one", choices=["one", "idf"],
                     help="train mode: term weighting of the corpus (idf: weighted counts, one GPU)")
     ap.add_argument("--requests", type=int, default=20000, help="infer mode: documents per run")
@@ -532,11 +696,9 @@ def main():
         if args.config not in INFER:
             args.config = "c4"
         return run_infer(args)
+    if args.mode == "parity":
+        return run_parity(args)
     args.warmup = max(args.warmup, 3)
-    if args.mode == "train":
-        # the engine's autotuner runs its first 6 sweeps eagerly, timing each
-        # sweep-kernel variant twice per document group; the warm-up covers them
-        args.warmup = max(args.warmup, 6)
     w = dict(WORKLOADS[args.config])
     if args.docs:
         w["D"] = args.docs
@@ -589,7 +751,12 @@ def main():
                                          else torch.distributed.ReduceOp.SUM)
         return float(t.item())
 
+    def configure(e):
+        if args.split or args.split_step:
+            e.set_doc_split(args.split, args.split_step)
+
     eng = new_engine()
+    configure(eng)
     if wts is not None:
         upload(eng, off, words, wts)
     else:
@@ -597,6 +764,13 @@ def main():
     info0 = eng.info()
     N = info0.N
     N_all_ranks = int(total(N))
+    # the engine's autotuner: the first sweeps after an upload time each
+    # sweep-kernel variant per document group (identical results); they run
+    # here, before the warm-up, and are reported as tuning_sweeps
+    tuning = 0
+    while -1 in eng.sweep_variants():
+        eng.train(1)
+        tuning += 1
     eng.train(args.warmup)
     if world > 1:
         torch.distributed.barrier()
@@ -608,7 +782,8 @@ def main():
     eng.train(args.steps)
     wall = time.perf_counter() - t0
     info = eng.info()
-    variants = eng.sweep_variants() if hasattr(eng, "sweep_variants") else None
+    variants = eng.sweep_variants()
+    split = eng.doc_split()
     launches = info.kernel_launches - launches0
     clk = clocks.stop()
     kernel_ms = info.sweep_kernel_ms / max(info.sweeps_timed, 1)
@@ -617,71 +792,78 @@ def main():
     step_ms = total(info.train_ms / args.steps, "max")
     wall_ms = total(wall * 1000 / args.steps, "max")
     value = N_all_ranks * 1000.0 / step_ms
+    ll = eng.ll()
+    ll_sweeps = tuning + args.warmup + args.steps
 
-    # e2e through the C ABI from host buffers: upload + steps + ll + download
+    # e2e through the C ABI from the caller's pageable numpy arrays (tomotopy's
+    # own buffers are pageable std::vectors): engine creation, corpus upload
+    # (staged through pinned buffers), z0 and counts, the autotuner's sweeps and
+    # the K sweeps of one train() call, the log-likelihood, and the z / n_kw /
+    # n_k download into fresh pageable arrays
     if args.no_e2e:
-        ll = eng.ll()
         e2e_obj = None
     else:
         eng.close()
-        pin_words = torch.from_numpy(words).pin_memory().numpy()
-        pin_off = torch.from_numpy(off).pin_memory().numpy()
-        pin_wts = torch.from_numpy(wts).pin_memory().numpy() if wts is not None else None
+        e_words = np.ascontiguousarray(words).copy()
+        e_off = np.ascontiguousarray(off).copy()
+        e_wts = np.ascontiguousarray(wts).copy() if wts is not None else None
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         te0 = time.perf_counter()
         e2e = new_engine()
-        if pin_wts is not None:
-            upload(e2e, pin_off, pin_words, pin_wts)
+        configure(e2e)
+        if e_wts is not None:
+            upload(e2e, e_off, e_words, e_wts)
         else:
-            upload(e2e, pin_off, pin_words)
+            upload(e2e, e_off, e_words)
         e2e.train(args.steps)
-        ll = e2e.ll()
+        e2e.ll()
         z, nkw, nk, _ = e2e.state()
         te = total(time.perf_counter() - te0, "max")
-        h2d = pin_words.nbytes + pin_off.nbytes + (pin_wts.nbytes if pin_wts is not None else 0)
+        h2d = e_words.nbytes + e_off.nbytes + (e_wts.nbytes if e_wts is not None else 0)
         d2h = z.nbytes + nkw.nbytes + nk.nbytes + 16
         e2e_obj = {"value": N_all_ranks * args.steps / te, "unit": "tokens/s",
                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                   "includes": "engine creation, corpus upload (pinned), z0 init + counts, the sweeps, ll, "
-                               "z/n_kw/n_k download (pageable)"}
+                   "includes": "engine creation, corpus upload from pageable arrays (staged), z0 init + counts, "
+                               "one train() call of K sweeps (its first sweeps tune the kernel variants), ll, "
+                               "z/n_kw/n_k download into fresh pageable arrays"}
         e2e.close()
+        eng = None
 
     peak, peak_kind = peaks()
     alg = bytes_per_sweep(N, K, V)
     achieved = alg / (kernel_ms / 1000.0) / 1e9
     if rank == 0:
+        cfgd = workload_config(args.config, w, world)
+        cfgd["l2"] = l2_statement(len(words), K, w["V"])
         line = {
             "metric": METRIC, "value": value, "unit": "tokens/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "wall_ms_per_step": wall_ms,
             "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded LDA generative process)",
-            "config": {"workload": workload_name(args.config, w), "K": K, "V": V, "D": int(len(off) - 1) * world,
-                       "tokens": N_all_ranks, "alpha": ALPHA, "eta": ETA, "sweep_groups": int(info.sweep_groups),
-                       "term_weight": args.tw,
-                       "sweep_variants": variants,
-                       "parallelism": (f"dp{world}: documents sharded, n_kw deltas summed over NCCL per group"
-                                       if world > 1 else "dp1"),
-                       "l2": "inputs larger than L2 (corpus %.0f MB, n_kw %.0f MB)" % (words.nbytes / 1e6, 4 * K * V / 1e6)},
+            "config": cfgd,
+            "corpus": {"realV": int(V), "tokens": N_all_ranks, "tokens_all_ids": int(len(words)) * world},
+            "engine": {"sweep_groups": int(info.sweep_groups), "sweep_variants": variants,
+                       "split_docs_per_group": split, "tuning_sweeps": tuning, "term_weight": args.tw,
+                       "optim_interval": 0},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": (MEASURED_TRAFFIC.get((args.config, int(len(off) - 1), int(info.sweep_groups)))
-                                     if world == 1 and args.tw == "one" else None),
+                         "frac": achieved / peak, "traffic": None,
                          "kernel": "k_sweep_doc", "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg,
                          "per": "one sweep = all k_sweep_doc + k_phi_copy launches of the document groups",
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                           "profiles/k_sweep_doc_c3_traffic.md",
+                         "traffic_ncu": NCU_TRAFFIC.get(args.config) if args.tw == "one" else None,
                          "peak_source": peak_kind},
             "e2e": e2e_obj,
             "gpu_launches": int(launches),
             "clocks": clk,
             "ll_per_word": (ll[0] + ll[1]) / N_all_ranks if N_all_ranks else 0.0,
+            "ll_after_sweeps": ll_sweeps,
         }
         if not args.no_cpu_baseline and world == 1 and args.tw == "one":
             line["cpu_baseline"] = cpu_baseline_sample(w, off, words, V)
         print(json.dumps(line), flush=True)
-    eng.close()
+    if eng is not None:
+        eng.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -224,6 +224,21 @@ tmt_status tmt_set_seed(tmt_handle* h, uint64_t seed);
 /* Sets the alpha-optimisation schedule between train() calls
  * (LDAModel::optimInterval / burnIn, python setters py_LDA.cpp). */
 tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_in);
+/* Long documents.  A document of at least split_len tokens (all ids counted)
+ * is sampled by one block as 8 slices of contiguous positions side by side,
+ * each with a private copy of the document's n_dk row that takes in the other
+ * slices' changes every `step` positions -- the within-document counterpart of
+ * tomotopy's PARTITION chunks (LDAModel.hpp:436-489: a document's tokens split
+ * by vocabulary range; its sorted tokens make each slice a vocabulary range).
+ * Without it one warp samples a document in order and the document's length
+ * bounds its group's time.  Default (min_tokens = 0): per document group,
+ * split_len = max(256, ceil(2 * group tokens / 4096)), for integer counts
+ * with K <= 2048; min_tokens >= 2^32 - 1: never; step 0: 16.  The split
+ * depends only on the corpus and these settings (never on timing or the
+ * device), so results stay bit-reproducible. */
+tmt_status tmt_set_doc_split(tmt_handle* h, uint64_t min_tokens, uint32_t step);
+/* Per document group, how many documents are split (*n = groups). */
+tmt_status tmt_get_doc_split(const tmt_handle* h, uint32_t* n_long, uint32_t cap, uint32_t* n);
 /* Single GPU: after the autotuner's first sweeps, each sweep is one launch of
  * a CUDA graph holding the sweep's kernels (default on).  0 launches every
  * kernel from the host instead; results are identical either way.  Replaces

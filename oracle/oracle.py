@@ -30,6 +30,44 @@ def build(ref_tree=None):
     subprocess.run(cmd, check=True)
 
 
+class SweepSpec(C.Structure):
+    """orc_sweep_spec (tmt_oracle.h)."""
+    _fields_ = [("K", C.c_uint32), ("V", C.c_uint32), ("alpha", C.c_void_p), ("eta", C.c_float),
+                ("pidx", C.c_void_p), ("prior", C.c_void_p), ("esum", C.c_void_p),
+                ("alpha_rows", C.c_void_p), ("arow", C.c_void_p), ("mask", C.c_void_p),
+                ("seed", C.c_uint64), ("iter", C.c_uint32),
+                ("doc_off", C.c_void_p), ("words", C.c_void_p),
+                ("ndk", C.c_void_p), ("nkw", C.c_void_p), ("nk", C.c_void_p),
+                ("nkw_next", C.c_void_p), ("nk_next", C.c_void_p), ("z", C.c_void_p),
+                ("split_len", C.c_uint64), ("slices", C.c_uint32), ("step", C.c_uint32)]
+
+
+# The long-document split of the device sweep (engine.cu, split_len_of): a
+# document of at least split_len tokens is sampled as SPLIT_SLICES slices side
+# by side, merging their n_dk changes every SPLIT_STEP positions.  split_len
+# per document group: max(SPLIT_MIN, ceil(2 * group tokens / 4096)), for
+# integer counts with K <= SPLIT_MAX_K.
+SPLIT_SLICES, SPLIT_STEP, SPLIT_MIN, SPLIT_MAX_K = 8, 16, 256, 512
+
+
+def split_len_of(group_tokens, K, min_len=0):
+    """The split threshold of a document group (0: no document is split).
+    min_len: the engine's override (0: the rule; >= 2^32 - 1: never)."""
+    if K > SPLIT_MAX_K or min_len >= 0xFFFFFFFF:
+        return 0
+    if min_len:
+        return int(min_len)
+    return max(SPLIT_MIN, (2 * int(group_tokens) + 4095) // 4096)
+
+
+class SynthSpec(C.Structure):
+    """orc_synth_spec (tmt_oracle.h)."""
+    _fields_ = [("V", C.c_uint32), ("T", C.c_uint32), ("D", C.c_uint64), ("len_kind", C.c_int32),
+                ("len_a", C.c_double), ("len_b", C.c_double), ("len_min", C.c_uint32), ("len_max", C.c_uint32),
+                ("doc_alpha", C.c_double), ("topic_beta", C.c_double), ("zipf_s", C.c_double),
+                ("seed", C.c_uint64), ("doc_offset", C.c_uint64)]
+
+
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
@@ -57,6 +95,13 @@ def _load():
         "orc_sweep_snapshot": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32,
                                       V, V, V, V, V, V, V]),
         "orc_conditional_f64": (None, [C.c_uint32, C.c_uint32, V, C.c_float, V, V, V, C.c_uint16, V]),
+        "orc_draw_intervals": (C.c_float, [V, V, C.c_uint32, C.c_uint32, C.c_float, V, V]),
+        "orc_sweep_docs": (None, [C.POINTER(SweepSpec), V, C.c_uint64]),
+        "orc_synth_corpus": (C.c_int, [C.POINTER(SynthSpec), V, V, C.c_uint64, V, C.c_uint32]),
+        "orc_prepare_corpus": (C.c_uint64, [C.c_uint64, V, V, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, V,
+                                            C.c_uint32]),
+        "orc_blocked_draw": (C.c_uint32, [V, V, C.c_uint32, C.c_uint32, C.c_float, C.c_float]),
+        "orc_ref_draw_intervals": (C.c_float, [V, V, V, C.c_uint32, V]),
         "orc_sweep_doc_live": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32,
                                       C.c_uint64, V, V, V, V, V, V, V, V]),
         "orc_sweep_doc_live_subset": (None, [C.c_uint32, C.c_uint32, V, C.c_float, C.c_uint64, C.c_uint32,
@@ -145,6 +190,72 @@ def philox(ctr, key):
     out = np.zeros(4, dtype=np.uint32)
     lib.orc_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
     return out
+
+
+def synth_corpus(V, T, D, length, seed, doc_alpha=0.1, topic_beta=0.01, zipf_s=1.07, threads=0, doc_offset=0):
+    """The benchmark's seeded synthetic corpus, generated without the engine
+    (orc_synth_corpus): length = ("poisson", mean, lo, hi) or ("lognormal",
+    mu, sigma, lo, hi).  Returns (doc_off uint64[D+1], words uint32[N])."""
+    if length[0] == "poisson":
+        kind, a, b, lo, hi = 0, float(length[1]), 0.0, int(length[2]), int(length[3])
+    else:
+        kind, a, b, lo, hi = 1, float(length[1]), float(length[2]), int(length[3]), int(length[4])
+    spec = SynthSpec(V=V, T=T, D=D, len_kind=kind, len_a=a, len_b=b, len_min=lo, len_max=hi, doc_alpha=doc_alpha,
+                     topic_beta=topic_beta, zipf_s=zipf_s, seed=seed, doc_offset=doc_offset)
+    th = threads or os.cpu_count() or 1
+    off = np.zeros(D + 1, dtype=np.uint64)
+    n = np.zeros(1, dtype=np.uint64)
+    if lib.orc_synth_corpus(C.byref(spec), _ptr(off), None, 0, _ptr(n), th) != 0:
+        raise ValueError("bad synthetic corpus spec")
+    words = np.zeros(max(int(n[0]), 1), dtype=np.uint32)
+    lib.orc_synth_corpus(C.byref(spec), _ptr(off), _ptr(words), int(n[0]), _ptr(n), th)
+    return off, words[:int(n[0])]
+
+
+def prepare_ids(doc_off, words, min_cf=0, min_df=0, rm_top=0, threads=0):
+    """removeStopwords + prepareDoc of a corpus (orc_prepare_corpus):
+    returns (doc_off, words renumbered and sorted per document, realV, order)."""
+    doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
+    out = np.ascontiguousarray(words, dtype=np.uint32).copy()
+    nv = int(out.max()) + 1 if len(out) else 0
+    order = np.zeros(max(nv, 1), dtype=np.uint32)
+    rv = lib.orc_prepare_corpus(len(doc_off) - 1, _ptr(doc_off), _ptr(out), nv, min_cf, min_df, rm_top,
+                                _ptr(order), threads or os.cpu_count() or 1)
+    return doc_off, out, int(rv), order[:nv]
+
+
+def token_factors(ndk_row, nkw_col, nk, alpha, eta, V, zo):
+    """The float operands of one token's draw with the token removed: the
+    device's (A, phi, phi_own) and tomotopy's (A, B, C) of getZLikelihoods
+    (LDAModel.hpp:273-285), each rounded as the code rounds it."""
+    K = len(nk)
+    veta = np.float32(eta) * np.float32(V)
+    own = (np.arange(K) == zo).astype(np.int32)
+    A = f32((np.asarray(ndk_row) - own).astype(np.float32) + f32(alpha))
+    R = f32(np.float32(1) / (np.asarray(nk).astype(np.float32) + veta))
+    phi = f32((np.asarray(nkw_col).astype(np.float32) + np.float32(eta)) * R)
+    phi_own = np.float32((np.float32(nkw_col[zo] - 1) + np.float32(eta)) *
+                         (np.float32(1) / (np.float32(nk[zo] - 1) + veta)))
+    B = f32((np.asarray(nkw_col) - own).astype(np.float32) + np.float32(eta))
+    Cc = f32((np.asarray(nk) - own).astype(np.float32) + veta)
+    return A, phi, phi_own, B, Cc
+
+
+def implied_conditionals(ndk_row, nkw_col, nk, alpha, eta, V, zo):
+    """(p_device, p_tomotopy, p_f64): the topic probabilities the device's
+    blocked draw and tomotopy's prefix-sum draw imply for one token (interval
+    widths over the total), and the FP64 conditional."""
+    K = len(nk)
+    A, phi, phi_own, B, Cc = token_factors(ndk_row, nkw_col, nk, alpha, eta, V, zo)
+    w = np.zeros(K)
+    t = lib.orc_draw_intervals(_ptr(A), _ptr(phi), K, int(zo), float(phi_own), _ptr(w), None)
+    wr = np.zeros(K)
+    tr = lib.orc_ref_draw_intervals(_ptr(A), _ptr(B), _ptr(Cc), K, _ptr(wr))
+    p64 = np.zeros(K)
+    lib.orc_conditional_f64(K, V, _ptr(f32(alpha)), float(eta), _ptr(np.ascontiguousarray(ndk_row, np.int32)),
+                            _ptr(np.ascontiguousarray(nkw_col, np.int32)), _ptr(np.ascontiguousarray(nk, np.int32)),
+                            int(zo), _ptr(p64))
+    return w / t, wr / tr, p64
 
 
 class Corpus:
@@ -249,23 +360,33 @@ class State:
         bounds.append(c.D)
         return order, bounds
 
-    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+    def _spec_extra(self):
+        """orc_sweep_spec fields of the conditional's options (priors, masks)."""
+        return {}
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1, split_min=0, split_step=SPLIT_STEP):
         """The device sweep: doc-major, live n_dk, snapshot n_kw / n_k,
         sampled group by group (see group_bounds), the snapshot refreshed
-        between groups."""
+        between groups; long documents split as the engine splits them
+        (split_min / split_step: the engine's tmt_set_doc_split)."""
         c = self.c
         order, b = self.group_bounds(groups)
+        lens = np.diff(c.doc_off.astype(np.int64))
         parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
+        splits = [split_len_of(lens[p.astype(np.int64)].sum(), self.K, split_min) for p in parts]
+        extra = self._spec_extra()
         for it in range(iters):
-            for part in parts:
+            for part, sl in zip(parts, splits):
                 if len(part) == 0:
                     continue
                 nkw2 = self.nkw.copy()
                 nk2 = self.nk.copy()
-                lib.orc_sweep_doc_live_subset(self.K, c.V, _ptr(self.alpha), self.eta, self.seed, start_step + it,
-                                              c.D, _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk), _ptr(self.nkw),
-                                              _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z), _ptr(part),
-                                              len(part))
+                sp = SweepSpec(K=self.K, V=c.V, alpha=self.alpha.ctypes.data, eta=self.eta, seed=self.seed,
+                               iter=start_step + it, doc_off=c.doc_off.ctypes.data, words=c.words.ctypes.data,
+                               ndk=self.ndk.ctypes.data, nkw=self.nkw.ctypes.data, nk=self.nk.ctypes.data,
+                               nkw_next=nkw2.ctypes.data, nk_next=nk2.ctypes.data, z=self.z.ctypes.data,
+                               split_len=sl, slices=SPLIT_SLICES, step=int(split_step), **extra)
+                lib.orc_sweep_docs(C.byref(sp), _ptr(part), len(part))
                 self.nkw = nkw2
                 self.nk = nk2
 
@@ -430,23 +551,8 @@ class StateP(State):
             self.z = np.ascontiguousarray(z0, dtype=np.uint16).copy()
         self.recount()
 
-    def doc_live_sweeps(self, iters, start_step=0, groups=1):
-        c = self.c
-        order, b = self.group_bounds(groups)
-        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
-        for it in range(iters):
-            for part in parts:
-                if len(part) == 0:
-                    continue
-                nkw2 = self.nkw.copy()
-                nk2 = self.nk.copy()
-                lib.orc_sweep_doc_live_p_subset(self.K, c.V, _ptr(self.alpha), self.eta, _ptr(self.pidx),
-                                                _ptr(self.prior), _ptr(self.esum), self.seed, start_step + it,
-                                                _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk), _ptr(self.nkw),
-                                                _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z), _ptr(part),
-                                                len(part))
-                self.nkw = nkw2
-                self.nk = nk2
+    def _spec_extra(self):
+        return dict(pidx=self.pidx.ctypes.data, prior=self.prior.ctypes.data, esum=self.esum.ctypes.data)
 
     def ll_f64(self):
         c = self.c
@@ -495,23 +601,14 @@ class StateM(State):
         self.alpha_rows = None if alpha_rows is None else np.ascontiguousarray(alpha_rows, np.float32)
         self.doc_row = None if doc_row is None else np.ascontiguousarray(doc_row, np.uint32)
 
-    def doc_live_sweeps(self, iters, start_step=0, groups=1):
-        c = self.c
-        order, b = self.group_bounds(groups)
-        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
-        for it in range(iters):
-            for part in parts:
-                if len(part) == 0:
-                    continue
-                nkw2 = self.nkw.copy()
-                nk2 = self.nk.copy()
-                lib.orc_sweep_doc_live_m_subset(self.K, c.V, _ptr(self.alpha), _ptr(self.alpha_rows),
-                                                _ptr(self.doc_row), _ptr(self.mask_bits), self.eta, self.seed,
-                                                start_step + it, _ptr(c.doc_off), _ptr(c.words), _ptr(self.ndk),
-                                                _ptr(self.nkw), _ptr(self.nk), _ptr(nkw2), _ptr(nk2), _ptr(self.z),
-                                                _ptr(part), len(part))
-                self.nkw = nkw2
-                self.nk = nk2
+    def _spec_extra(self):
+        e = {}
+        if self.mask_bits is not None:
+            e["mask"] = self.mask_bits.ctypes.data
+        if self.alpha_rows is not None:
+            e["alpha_rows"] = self.alpha_rows.ctypes.data
+            e["arow"] = self.doc_row.ctypes.data
+        return e
 
     def ll_f64(self):
         a, b = super().ll_f64()

@@ -954,8 +954,9 @@ double orc_infer_doc(uint32_t K, uint32_t V, const float* alpha, float eta,
  * Topics are dealt to 32 lanes in blocks of four: lane l owns the topics
  * k = 128*j + 4*l + i (j = 0, 1, ..., i = 0..3, k < K), in that order.
  * Pass 1: T_l = fma-chain of A_k * phi_k over lane l's topics (s = fma(A, phi,
- * s) from s = 0); the lane owning zo then sets T_l = max((T_l - A_zo*phi_zo)
- * + A_zo*phi_own, 0).  X = Hillis-Steele inclusive scan of T over 32 lanes,
+ * s) from s = 0), the own topic zo contributing fma(0, phi_zo, s) = s; the
+ * lane owning zo then adds T_l = T_l + A_zo*phi_own (no subtraction, so no
+ * cancellation when A_zo*phi_zo would dominate the lane).  X = Hillis-Steele inclusive scan of T over 32 lanes,
  * E_l = X_{l-1} (E_0 = 0), r = u * X_31, u = Philox(token index, step).
  * h = first lane owning a topic with r < E_h + T_h (none: K-1).
  * Pass 2: x_t = A_k * phi_k (phi_own at zo) over lane h's topics in order,
@@ -998,16 +999,13 @@ static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint3
     for (uint32_t l = 0; l < 32; ++l) {
         float s = 0.f;
         cl[l] = lane_count(l, K);
+        /* the own topic is left out of the chain (its document weight reads 0:
+         * fmaf(0, phi, s) == s) and added last by its lane: no subtraction */
         for (uint32_t t = 0; t < cl[l]; ++t) {
             int64_t k = lane_topic(l, t, K);
-            s = fmaf(A[k], phi[k], s);
+            s = fmaf((uint32_t)k == zo ? 0.f : A[k], phi[k], s);
         }
-        if (zo < K && ((zo >> 2) & 31) == l) {
-            float wu = A[zo] * phi[zo];
-            float wo = A[zo] * phi_own;
-            s = (s - wu) + wo;
-            if (!(s > 0.f)) s = 0.f;
-        }
+        if (zo < K && ((zo >> 2) & 31) == l) s = s + A[zo] * phi_own;
         T[l] = s;
         X[l] = s;
     }
@@ -1039,6 +1037,101 @@ static uint32_t blocked_draw(const float* A, const float* phi, uint32_t K, uint3
         carry = carry + x[31];
     }
     return (uint32_t)lane_topic((uint32_t)h, n - 1, K);
+}
+
+/* The conditional blocked_draw implies: width[k] = the length of the set of
+ * r = u * total in [0, total) that the draw maps to topic k, formed from the
+ * same float lane totals, lane scan and pass-2 prefix sums (a lane is hit for
+ * r below fl(E_h + T_h); inside it, topic t for r below fl(E_h + P_t), the
+ * lane's last topic taking the rest; r past every lane goes to K-1).
+ * start[k] (may be NULL): where topic k's interval begins (-1 if empty;
+ * every interval but K-1's is one contiguous range).
+ * Returns total; width sums to total.  Test infrastructure for the 1e-5
+ * gate on the kernel's own arithmetic. */
+float orc_draw_intervals(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own,
+                         double* width, double* start)
+{
+    float T[32], X[32];
+    uint32_t cl[32];
+    for (uint32_t k = 0; k < K; ++k) { width[k] = 0.0; if (start) start[k] = -1.0; }
+    for (uint32_t l = 0; l < 32; ++l) {
+        float s = 0.f;
+        cl[l] = lane_count(l, K);
+        for (uint32_t t = 0; t < cl[l]; ++t) {
+            int64_t k = lane_topic(l, t, K);
+            s = fmaf((uint32_t)k == zo ? 0.f : A[k], phi[k], s);
+        }
+        if (zo < K && ((zo >> 2) & 31) == l) s = s + A[zo] * phi_own;
+        T[l] = s;
+        X[l] = s;
+    }
+    hs32(X);
+    const float total = X[31];
+    double lo = 0.0;                         /* r below lo is taken by earlier lanes */
+    for (uint32_t l = 0; l < 32; ++l) {
+        if (!cl[l]) continue;
+        const float E = l ? X[l - 1] : 0.f;
+        const double b = (double)(E + T[l]);
+        const double lane_hi = b < (double)total ? b : (double)total;
+        if (lane_hi > lo) {
+            double tlo = lo;
+            float carry = 0.f;
+            const uint32_t n = cl[l];
+            for (uint32_t m = 0; m < n; m += 32) {
+                float x[32];
+                for (uint32_t t = 0; t < 32; ++t) {
+                    if (m + t < n) {
+                        int64_t k = lane_topic(l, m + t, K);
+                        x[t] = A[k] * ((uint32_t)k == zo ? phi_own : phi[k]);
+                    } else {
+                        x[t] = 0.f;
+                    }
+                }
+                hs32(x);
+                for (uint32_t t = 0; t < 32 && m + t < n; ++t) {
+                    const int64_t k = lane_topic(l, m + t, K);
+                    double hi = (m + t == n - 1) ? lane_hi : (double)(E + (carry + x[t]));
+                    if (hi > lane_hi) hi = lane_hi;
+                    if (hi > tlo) { if (start) start[k] = tlo; width[k] += hi - tlo; tlo = hi; }
+                }
+                carry = carry + x[31];
+            }
+        }
+        if (b > lo) lo = b;
+    }
+    if ((double)total > lo) {
+        if (start && width[K - 1] == 0.0) start[K - 1] = lo;
+        width[K - 1] += (double)total - lo;
+    }
+    return total;
+}
+
+/* blocked_draw itself, for tests: the topic drawn for u (and *total) */
+uint32_t orc_blocked_draw(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own, float u)
+{
+    return blocked_draw(A, phi, K, zo, phi_own, u);
+}
+
+/* The same for tomotopy's draw (getZLikelihoods + prefixSum + sampleFromDiscreteAcc,
+ * LDAModel.hpp:273-285, sample.hpp:69-86, 133-189): dist_k = (A_k * B_k) / C_k
+ * in float, the SSE-order prefix sum cum, r = u * cum[K-1], first k with
+ * r < cum[k]; width[k] from cum's running maximum.  A, B, C: the three
+ * factors with the token removed. */
+float orc_ref_draw_intervals(const float* A, const float* B, const float* C, uint32_t K, double* width)
+{
+    float* cum = (float*)aligned_alloc(64, ((K + 15) / 16) * 64);
+    for (uint32_t k = 0; k < K; ++k) cum[k] = (A[k] * B[k]) / C[k];
+    orc_prefix_sum_sse(cum, (int)K);
+    const float total = cum[K - 1];
+    double lo = 0.0;
+    for (uint32_t k = 0; k < K; ++k) {
+        double hi = (double)cum[k] < (double)total ? (double)cum[k] : (double)total;
+        width[k] = hi > lo ? hi - lo : 0.0;
+        if (hi > lo) lo = hi;
+    }
+    if ((double)total > lo) width[K - 1] += (double)total - lo;
+    free(cum);
+    return total;
 }
 
 void orc_sweep_doc_live_subset(uint32_t K, uint32_t V, const float* alpha, float eta,
@@ -1079,6 +1172,109 @@ void orc_sweep_doc_live_subset(uint32_t K, uint32_t V, const float* alpha, float
         }
     }
     free(R); free(A); free(phi);
+}
+
+/* One document group of the device sweep, generic over the conditional's
+ * options (word priors, per-document alphas and masks) and with the
+ * long-document split.  A document of at least split_len tokens (all ids
+ * counted) is cut into `slices` contiguous position ranges, slice w =
+ * [b + w*L/slices, b + (w+1)*L/slices) (integer division); they are sampled
+ * side by side in steps of `step` positions: in step s every slice samples its
+ * positions [s*step, (s+1)*step) in order with a private copy of the
+ * document's n_dk row -- the row as of the start of the step plus its own
+ * changes -- and after the step the row gains every slice's changes.  A
+ * shorter document is sampled in order with its row live (split_len = 0:
+ * every document).  Draws, n_kw / n_k snapshots and deltas as
+ * orc_sweep_doc_live_subset. */
+/* orc_sweep_spec: see tmt_oracle.h */
+static inline float mask_bit(const uint32_t* mask, uint32_t mw, uint64_t d, uint32_t k);
+
+typedef struct {
+    const orc_sweep_spec* sp;
+    const float* al; uint64_t d;
+    float* R; float* phi; float veta; uint32_t mw;
+} sweep_ctx;
+
+static inline float sweep_afold(const sweep_ctx* c, int32_t n, uint32_t k)
+{
+    const float x = (float)n + c->al[k];
+    return c->sp->mask ? x * mask_bit(c->sp->mask, c->mw, c->d, k) : x;
+}
+
+/* tokens [tb, te) of document c->d with the row `row` (and A) live; the
+ * row's changes are also added to dlt when dlt != NULL */
+static void sweep_tokens(const sweep_ctx* c, uint64_t tb, uint64_t te, int32_t* row, float* A, int32_t* dlt)
+{
+    const orc_sweep_spec* sp = c->sp;
+    const uint32_t K = sp->K;
+    for (uint64_t i = tb; i < te; ++i) {
+        uint32_t v = sp->words[i];
+        if (v >= sp->V) continue;
+        uint16_t zo = sp->z[i];
+        const int32_t* col = sp->nkw + (size_t)v * K;
+        const float* pe = (sp->pidx && sp->pidx[v] >= 0) ? sp->prior + (size_t)sp->pidx[v] * K : NULL;
+        row[zo]--;
+        A[zo] = sweep_afold(c, row[zo], zo);
+        for (uint32_t k = 0; k < K; ++k) c->phi[k] = ((float)col[k] + (pe ? pe[k] : sp->eta)) * c->R[k];
+        const float so = sp->esum ? sp->esum[zo] : c->veta;
+        float phi_own = ((float)(col[zo] - 1) + (pe ? pe[zo] : sp->eta)) * (1.0f / ((float)(sp->nk[zo] - 1) + so));
+        float u = orc_u01(philox_first((uint32_t)i, (uint32_t)(i >> 32), ORC_STREAM_SWEEP, sp->iter, sp->seed));
+        uint16_t zn = (uint16_t)blocked_draw(A, c->phi, K, zo, phi_own, u);
+        row[zn]++;
+        A[zn] = sweep_afold(c, row[zn], zn);
+        sp->z[i] = zn;
+        if (zn != zo) {
+            sp->nkw_next[(size_t)v * K + zo]--; sp->nkw_next[(size_t)v * K + zn]++;
+            sp->nk_next[zo]--; sp->nk_next[zn]++;
+            if (dlt) { dlt[zo]--; dlt[zn]++; }
+        }
+    }
+}
+
+void orc_sweep_docs(const orc_sweep_spec* sp, const uint64_t* docs, uint64_t n_docs)
+{
+    const uint32_t K = sp->K;
+    sweep_ctx c;
+    c.sp = sp;
+    c.veta = sp->eta * (float)sp->V;
+    c.mw = (K + 31) / 32;
+    c.R = (float*)malloc(K * sizeof(float));
+    c.phi = (float*)malloc(K * sizeof(float));
+    float* A = (float*)malloc(K * sizeof(float));
+    int32_t* P = (int32_t*)malloc(K * sizeof(int32_t));
+    int32_t* dlt = (int32_t*)malloc(K * sizeof(int32_t));
+    for (uint32_t k = 0; k < K; ++k) c.R[k] = 1.0f / ((float)sp->nk[k] + (sp->esum ? sp->esum[k] : c.veta));
+    for (uint64_t di = 0; di < n_docs; ++di) {
+        const uint64_t d = docs ? docs[di] : di;
+        c.d = d;
+        c.al = sp->arow ? sp->alpha_rows + (size_t)sp->arow[d] * K : sp->alpha;
+        int32_t* row = sp->ndk + d * K;
+        const uint64_t b = sp->doc_off[d], e = sp->doc_off[d + 1], L = e - b;
+        if (!sp->split_len || L < sp->split_len || sp->slices < 2) {
+            for (uint32_t k = 0; k < K; ++k) A[k] = sweep_afold(&c, row[k], k);
+            sweep_tokens(&c, b, e, row, A, NULL);
+            continue;
+        }
+        const uint32_t S = sp->slices, m = sp->step;
+        uint64_t longest = 0;
+        for (uint32_t w = 0; w < S; ++w) {
+            const uint64_t n = (uint64_t)(w + 1) * L / S - (uint64_t)w * L / S;
+            if (n > longest) longest = n;
+        }
+        for (uint64_t s = 0; s * m < longest; ++s) {
+            for (uint32_t k = 0; k < K; ++k) dlt[k] = 0;
+            for (uint32_t w = 0; w < S; ++w) {
+                const uint64_t sb = b + (uint64_t)w * L / S, se = b + (uint64_t)(w + 1) * L / S;
+                uint64_t tb = sb + s * m, te = tb + m;
+                if (tb >= se) continue;
+                if (te > se) te = se;
+                for (uint32_t k = 0; k < K; ++k) { P[k] = row[k]; A[k] = sweep_afold(&c, P[k], k); }
+                sweep_tokens(&c, tb, te, P, A, dlt);
+            }
+            for (uint32_t k = 0; k < K; ++k) row[k] += dlt[k];
+        }
+    }
+    free(c.R); free(c.phi); free(A); free(P); free(dlt);
 }
 
 void orc_sweep_doc_live(uint32_t K, uint32_t V, const float* alpha, float eta,
@@ -1677,4 +1873,285 @@ void orc_gibbs_none_p(uint64_t D, const uint64_t* doc_off, const uint32_t* words
         }
     }
     free(dist); free(order);
+}
+
+
+/* ------------------------------------------------------------------------ */
+/* The benchmark workload, without the engine: the seeded synthetic corpus  */
+/* and its preparation, for the timed CPU baseline                          */
+/* ------------------------------------------------------------------------ */
+/* The generator of tomotopy_b200/csrc/synth.cpp restated (the workload of
+ * both bench arms, so the CPU arm needs no engine code): Philox4x32-10
+ * streams keyed by seed ^ 0x5EEDC0DE5EEDC0DE with counters (owner a, owner b,
+ * 'SYNT', draw index); lengths Poisson (a sum of pieces of mean <= 50, Knuth)
+ * or round(lognormal) clipped; topic-word distributions Dirichlet(beta V
+ * Zipf(s)) drawn as log-Gamma (Marsaglia-Tsang, the a < 1 boost in log
+ * space), words 40 nats below a topic's top word dropped, Vose alias tables;
+ * tokens by the Polya urn of Dirichlet(doc_alpha * 1_T).  Identical output
+ * for any thread count. */
+typedef struct { uint64_t key; uint32_t a, b, n, buf[4]; int left; } syn_rng;
+
+static void syn_init(syn_rng* r, uint64_t seed, uint32_t a, uint32_t b)
+{
+    r->key = seed ^ 0x5EEDC0DE5EEDC0DEull; r->a = a; r->b = b; r->n = 0; r->left = 0;
+}
+static uint32_t syn_next(syn_rng* r)
+{
+    if (!r->left) {
+        uint32_t ctr[4] = { r->a, r->b, 0x53594E54u, r->n++ }, key[2] = { (uint32_t)r->key, (uint32_t)(r->key >> 32) };
+        orc_philox4x32_10(ctr, key, r->buf);
+        r->left = 4;
+    }
+    return r->buf[--r->left];
+}
+static double syn_uniform(syn_rng* r)      /* (0, 1], 53 bits */
+{
+    uint64_t hi = syn_next(r), lo = syn_next(r);
+    uint64_t m = ((hi << 32) | lo) >> 11;
+    return ((double)m + 1.0) * (1.0 / 9007199254740992.0);
+}
+static double syn_normal(syn_rng* r)
+{
+    double u1 = syn_uniform(r), u2 = syn_uniform(r);
+    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+static double syn_log_gamma(syn_rng* r, double a)
+{
+    double boost = 0.0;
+    if (a < 1.0) { boost = log(syn_uniform(r)) / a; a += 1.0; }
+    const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
+    for (;;) {
+        double x = syn_normal(r), v = 1.0 + c * x;
+        if (v <= 0) continue;
+        v = v * v * v;
+        double u = syn_uniform(r);
+        if (log(u) < 0.5 * x * x + d - d * v + d * log(v)) return log(d * v) + boost;
+    }
+}
+static uint32_t syn_poisson_small(syn_rng* r, double lam)
+{
+    double L = exp(-lam), p = 1.0;
+    uint32_t k = 0;
+    do { ++k; p *= syn_uniform(r); } while (p > L);
+    return k - 1;
+}
+
+typedef struct { uint32_t n; uint32_t* word; float* prob; uint32_t* alias; } syn_alias;
+
+/* Vose's alias method with the generator's stack order */
+static void syn_build_alias(const double* p, const uint32_t* ids, uint32_t n, syn_alias* out)
+{
+    out->n = n;
+    out->word = (uint32_t*)malloc((n + 1) * sizeof(uint32_t));
+    out->prob = (float*)calloc(n + 1, sizeof(float));
+    out->alias = (uint32_t*)calloc(n + 1, sizeof(uint32_t));
+    memcpy(out->word, ids, n * sizeof(uint32_t));
+    double s = 0;
+    for (uint32_t i = 0; i < n; ++i) s += p[i];
+    double* q = (double*)malloc((n + 1) * sizeof(double));
+    uint32_t* small = (uint32_t*)malloc((n + 1) * sizeof(uint32_t));
+    uint32_t* large = (uint32_t*)malloc((n + 1) * sizeof(uint32_t));
+    uint32_t ns = 0, nl = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        q[i] = p[i] / s * (double)n;
+        if (q[i] < 1.0) small[ns++] = i; else large[nl++] = i;
+    }
+    while (ns && nl) {
+        uint32_t l = small[--ns], g = large[--nl];
+        out->prob[l] = (float)q[l];
+        out->alias[l] = g;
+        q[g] = (q[g] + q[l]) - 1.0;
+        if (q[g] < 1.0) small[ns++] = g; else large[nl++] = g;
+    }
+    for (uint32_t i = 0; i < nl; ++i) { out->prob[large[i]] = 1.f; out->alias[large[i]] = large[i]; }
+    for (uint32_t i = 0; i < ns; ++i) { out->prob[small[i]] = 1.f; out->alias[small[i]] = small[i]; }
+    free(q); free(small); free(large);
+}
+
+typedef struct {
+    const orc_synth_spec* s; uint64_t b, e; int phase;
+    uint32_t* len; const uint64_t* doc_off; uint32_t* words;
+    const double* zipf; double zs; syn_alias* topics;
+} syn_job;
+
+static uint32_t syn_doc_length(const orc_synth_spec* s, syn_rng* r)
+{
+    double L;
+    if (s->len_kind == 0) {
+        double lam = s->len_a, acc = 0;
+        uint32_t m = (uint32_t)ceil(lam / 50.0);
+        if (m < 1) m = 1;
+        for (uint32_t i = 0; i < m; ++i) acc += syn_poisson_small(r, lam / m);
+        L = acc;
+    } else {
+        L = floor(exp(s->len_a + s->len_b * syn_normal(r)) + 0.5);
+    }
+    if (L < s->len_min) L = s->len_min;
+    if (L > s->len_max) L = s->len_max;
+    return (uint32_t)L;
+}
+
+static void* syn_work(void* arg)
+{
+    syn_job* j = (syn_job*)arg;
+    const orc_synth_spec* s = j->s;
+    if (j->phase == 0) {
+        for (uint64_t d = j->b; d < j->e; ++d) {
+            const uint64_t dd = d + s->doc_offset;
+            syn_rng r;
+            syn_init(&r, s->seed, (uint32_t)dd, 0x4C454E00u | (uint32_t)(dd >> 32));
+            j->len[d] = syn_doc_length(s, &r);
+        }
+    } else if (j->phase == 1) {
+        double* lg = (double*)malloc(s->V * sizeof(double));
+        double* p = (double*)malloc(s->V * sizeof(double));
+        uint32_t* ids = (uint32_t*)malloc(s->V * sizeof(uint32_t));
+        for (uint64_t t = j->b; t < j->e; ++t) {
+            syn_rng r;
+            syn_init(&r, s->seed, (uint32_t)t, 0x50484900u);
+            double mx = -INFINITY;
+            for (uint32_t v = 0; v < s->V; ++v) {
+                double a = s->topic_beta * (double)s->V * j->zipf[v] / j->zs;
+                lg[v] = syn_log_gamma(&r, a);
+                if (lg[v] > mx) mx = lg[v];
+            }
+            uint32_t n = 0;
+            for (uint32_t v = 0; v < s->V; ++v) {
+                double x = lg[v] - mx;
+                if (x < -40.0) continue;
+                p[n] = exp(x);
+                ids[n++] = v;
+            }
+            syn_build_alias(p, ids, n, &j->topics[t]);
+        }
+        free(lg); free(p); free(ids);
+    } else {
+        const double conc = s->doc_alpha * (double)s->T;
+        uint32_t cap = 0;
+        uint32_t* zt = NULL;
+        for (uint64_t d = j->b; d < j->e; ++d) {
+            const uint64_t dd = d + s->doc_offset;
+            syn_rng r;
+            syn_init(&r, s->seed, (uint32_t)dd, 0x544F4B00u | (uint32_t)(dd >> 32));
+            const uint32_t L = (uint32_t)(j->doc_off[d + 1] - j->doc_off[d]);
+            if (L > cap) { free(zt); cap = L; zt = (uint32_t*)malloc(cap * sizeof(uint32_t)); }
+            uint32_t* out = j->words + j->doc_off[d];
+            for (uint32_t i = 0; i < L; ++i) {
+                double u = syn_uniform(&r) * ((double)i + conc);
+                uint32_t z;
+                if (u < conc || i == 0) z = syn_next(&r) % s->T;
+                else { uint32_t q = (uint32_t)(u - conc); z = zt[q < i - 1 ? q : i - 1]; }
+                zt[i] = z;
+                const syn_alias* A = &j->topics[z];
+                uint32_t jj = (uint32_t)(((uint64_t)syn_next(&r) * A->n) >> 32);
+                float f = (float)(syn_next(&r) >> 8) * (1.0f / 16777216.0f);
+                out[i] = A->word[f < A->prob[jj] ? jj : A->alias[jj]];
+            }
+        }
+        free(zt);
+    }
+    return NULL;
+}
+
+static void syn_parallel(syn_job* proto, uint64_t n, uint32_t threads)
+{
+    if (threads < 1) threads = 1;
+    if (n < 64) threads = 1;
+    pthread_t* th = (pthread_t*)malloc(threads * sizeof(pthread_t));
+    syn_job* jobs = (syn_job*)malloc(threads * sizeof(syn_job));
+    for (uint32_t i = 0; i < threads; ++i) {
+        jobs[i] = *proto;
+        jobs[i].b = n * i / threads;
+        jobs[i].e = n * (i + 1) / threads;
+        if (threads > 1) pthread_create(&th[i], NULL, syn_work, &jobs[i]);
+        else syn_work(&jobs[i]);
+    }
+    if (threads > 1) for (uint32_t i = 0; i < threads; ++i) pthread_join(th[i], NULL);
+    free(th); free(jobs);
+}
+
+int orc_synth_corpus(const orc_synth_spec* s, uint64_t* doc_off, uint32_t* words, uint64_t capacity,
+                     uint64_t* n_tokens, uint32_t threads)
+{
+    if (!s || !doc_off || !n_tokens || !s->V || !s->T || !s->D || s->len_min > s->len_max || !s->len_max) return -1;
+    uint32_t* len = (uint32_t*)malloc(s->D * sizeof(uint32_t));
+    syn_job job = { s, 0, 0, 0, len, doc_off, words, NULL, 0, NULL };
+    syn_parallel(&job, s->D, threads);
+    doc_off[0] = 0;
+    for (uint64_t d = 0; d < s->D; ++d) doc_off[d + 1] = doc_off[d] + len[d];
+    free(len);
+    *n_tokens = doc_off[s->D];
+    if (!words) return 0;
+    if (capacity < *n_tokens) return -1;
+    double* zipf = (double*)malloc(s->V * sizeof(double));
+    double zs = 0;
+    for (uint32_t v = 0; v < s->V; ++v) { zipf[v] = pow((double)(v + 1), -s->zipf_s); zs += zipf[v]; }
+    syn_alias* topics = (syn_alias*)calloc(s->T, sizeof(syn_alias));
+    job.phase = 1; job.zipf = zipf; job.zs = zs; job.topics = topics;
+    syn_parallel(&job, s->T, threads);
+    job.phase = 2;
+    syn_parallel(&job, s->D, threads);
+    for (uint32_t t = 0; t < s->T; ++t) { free(topics[t].word); free(topics[t].prob); free(topics[t].alias); }
+    free(topics); free(zipf);
+    return 0;
+}
+
+/* removeStopwords + prepareDoc over a whole corpus (the restated functions
+ * above), threaded over documents: words are renumbered in place and sorted
+ * within each document; order[old id] = new id; returns realV. */
+typedef struct { const uint64_t* doc_off; uint32_t* words; uint64_t b, e; uint64_t nv; uint64_t* df;
+                 const uint32_t* order; int phase; } prep_job;
+
+static void* prep_work(void* arg)
+{
+    prep_job* j = (prep_job*)arg;
+    uint32_t* tmp = NULL; uint32_t* wo = NULL; size_t cap = 0;
+    for (uint64_t d = j->b; d < j->e; ++d) {
+        const uint64_t b = j->doc_off[d], n = j->doc_off[d + 1] - b;
+        if (n > cap) { free(tmp); free(wo); cap = n; tmp = (uint32_t*)malloc(cap * 4); wo = (uint32_t*)malloc(cap * 4); }
+        if (j->phase == 0) {          /* df: distinct words of the document */
+            memcpy(tmp, j->words + b, n * 4);
+            orc_sort_doc(tmp, n, wo);
+            for (uint64_t i = 0; i < n; ++i)
+                if (i == 0 || tmp[i] != tmp[i - 1]) j->df[tmp[i]]++;
+        } else {                      /* renumber, then sort by the new ids */
+            uint32_t* w = j->words + b;
+            for (uint64_t i = 0; i < n; ++i) w[i] = j->order[w[i]];
+            orc_sort_doc(w, n, wo);
+        }
+    }
+    free(tmp); free(wo);
+    return NULL;
+}
+
+uint64_t orc_prepare_corpus(uint64_t D, const uint64_t* doc_off, uint32_t* words, uint64_t nv,
+                            uint64_t min_cf, uint64_t min_df, uint64_t rm_top, uint32_t* order, uint32_t threads)
+{
+    if (threads < 1) threads = 1;
+    uint64_t* cf = (uint64_t*)calloc(nv + 1, sizeof(uint64_t));
+    uint64_t* df = (uint64_t*)calloc(nv + 1, sizeof(uint64_t));
+    for (uint64_t i = 0; i < doc_off[D]; ++i) cf[words[i]]++;
+    uint64_t** dfs = (uint64_t**)malloc(threads * sizeof(uint64_t*));
+    pthread_t* th = (pthread_t*)malloc(threads * sizeof(pthread_t));
+    prep_job* jobs = (prep_job*)malloc(threads * sizeof(prep_job));
+    for (int phase = 0; phase < 2; ++phase) {
+        for (uint32_t i = 0; i < threads; ++i) {
+            dfs[i] = phase == 0 ? (uint64_t*)calloc(nv + 1, sizeof(uint64_t)) : NULL;
+            prep_job pj = { doc_off, words, D * i / threads, D * (i + 1) / threads, nv, dfs[i], order, phase };
+            jobs[i] = pj;
+            pthread_create(&th[i], NULL, prep_work, &jobs[i]);
+        }
+        for (uint32_t i = 0; i < threads; ++i) pthread_join(th[i], NULL);
+        if (phase == 0) {
+            for (uint32_t i = 0; i < threads; ++i) {
+                for (uint64_t v = 0; v < nv; ++v) df[v] += dfs[i][v];
+                free(dfs[i]);
+            }
+            uint64_t rv = orc_remove_stopwords(nv, cf, df, min_cf, min_df, rm_top, order);
+            cf[nv] = rv;        /* kept for the return */
+        }
+    }
+    const uint64_t rv = cf[nv];
+    free(cf); free(df); free(dfs); free(th); free(jobs);
+    return rv;
 }

@@ -236,6 +236,32 @@ void orc_sweep_doc_live_m_subset(uint32_t K, uint32_t V, const float* alpha, con
 double orc_ll_docs_m_f64(uint64_t D, uint32_t K, const int32_t* ndk, const int32_t* doc_len,
                          const float* alpha_rows, const uint32_t* arow);
 
+/* ---- the device sweep with every option and the long-document split ----- */
+typedef struct {
+    uint32_t K, V;
+    const float* alpha; float eta;
+    const int32_t* pidx; const float* prior; const float* esum;   /* word priors or NULL */
+    const float* alpha_rows; const uint32_t* arow;                /* per-document alphas or NULL */
+    const uint32_t* mask;                                         /* D x ceil(K/32) or NULL */
+    uint64_t seed; uint32_t iter;
+    const uint64_t* doc_off; const uint32_t* words;
+    int32_t* ndk; const int32_t* nkw; const int32_t* nk;
+    int32_t* nkw_next; int32_t* nk_next; uint16_t* z;
+    uint64_t split_len; uint32_t slices, step;   /* split_len 0: no document is split */
+} orc_sweep_spec;
+/* the documents docs[0 .. n_docs) of one group (see tmt_oracle.c) */
+void orc_sweep_docs(const orc_sweep_spec* sp, const uint64_t* docs, uint64_t n_docs);
+
+/* ---- the conditional a draw implies (gate: 1e-5 of FP64) ---------------- */
+/* width[k]: the length of the r-interval (r = u * total) mapped to topic k by
+ * the device's blocked draw (A with the token removed, phi the word's table
+ * column, phi_own the own topic's weight); returns total. */
+float orc_draw_intervals(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own,
+                         double* width, double* start);
+uint32_t orc_blocked_draw(const float* A, const float* phi, uint32_t K, uint32_t zo, float phi_own, float u);
+/* the same for tomotopy's draw over dist_k = (A_k * B_k) / C_k (SSE prefix sum) */
+float orc_ref_draw_intervals(const float* A, const float* B, const float* C, uint32_t K, double* width);
+
 /* ---- the reference's sequential sampler with weights / word priors ------- */
 void orc_gibbs_none_w(uint64_t D, const uint64_t* doc_off, const uint32_t* words, const float* wt,
                       uint32_t V, uint32_t K, const float* alpha, float eta,
@@ -244,6 +270,24 @@ void orc_gibbs_none_p(uint64_t D, const uint64_t* doc_off, const uint32_t* words
                       uint32_t V, uint32_t K, const float* alpha, float eta,
                       const int32_t* pidx, const float* prior, const float* esum,
                       uint16_t* z, int32_t* ndk, int32_t* nkw, int32_t* nk, uint64_t* rng_state);
+
+/* ---- the benchmark workload without the engine (CPU baseline) ------------ */
+typedef struct {
+    uint32_t V, T;           /* vocabulary, true topics */
+    uint64_t D;              /* documents */
+    int32_t len_kind;        /* 0 Poisson, 1 lognormal */
+    double len_a, len_b;     /* Poisson mean | lognormal mu, sigma */
+    uint32_t len_min, len_max;
+    double doc_alpha, topic_beta, zipf_s;
+    uint64_t seed, doc_offset;
+} orc_synth_spec;
+/* the seeded synthetic corpus (tomotopy_b200/csrc/synth.cpp restated): words
+ * NULL fills doc_off[D+1] and *n_tokens only; 0 on success */
+int orc_synth_corpus(const orc_synth_spec* s, uint64_t* doc_off, uint32_t* words, uint64_t capacity,
+                     uint64_t* n_tokens, uint32_t threads);
+/* removeStopwords + prepareDoc of a whole corpus in place; returns realV */
+uint64_t orc_prepare_corpus(uint64_t D, const uint64_t* doc_off, uint32_t* words, uint64_t nv,
+                            uint64_t min_cf, uint64_t min_df, uint64_t rm_top, uint32_t* order, uint32_t threads);
 
 #ifdef __cplusplus
 }

@@ -108,3 +108,19 @@ def test_sparse_sampler_is_refused():
         assert b"sparse" in lib.tmt_last_error(h)
     finally:
         lib.tmt_destroy(h)
+
+
+@pytest.mark.parametrize("length", [("poisson", 150, 1, 10000), ("lognormal", float(np.log(100)), 1.2, 5, 5000)])
+def test_oracle_workload_equals_product_workload(length):
+    """The CPU baseline builds the benchmark corpus without the engine
+    (oracle.synth_corpus / oracle.prepare_ids); it must be the corpus the GPU
+    arm samples, id for id."""
+    a_off, a_w = T.synth_corpus(5000, 40, 700, length, seed=20261206, threads=3)
+    b_off, b_w = O.synth_corpus(5000, 40, 700, length, seed=20261206, threads=5)
+    np.testing.assert_array_equal(a_off, b_off)
+    np.testing.assert_array_equal(a_w, b_w)
+    pa = T.prepare_ids(a_off, a_w)
+    pb = O.prepare_ids(b_off, b_w, threads=4)
+    assert pa[2] == pb[2]
+    np.testing.assert_array_equal(pa[1], pb[1])
+    np.testing.assert_array_equal(pa[3], pb[3])

@@ -352,6 +352,74 @@ def test_chi_square_on_draws():
     assert p > 1e-4, (chi2, p)
 
 
+def test_chi_square_mid_document_k1000():
+    """K = 1000, a token deep inside a long document: each test document is
+    3,000 tokens of an anchor word whose word prior allows only topic zo
+    (so every anchor draw is zo again, exactly) followed by one token of its
+    own word, whose other occurrences (in background documents) give every
+    test word the same column.  With one document group every test token
+    draws from the same start-of-sweep conditional, with n_dk[zo] = 3,000
+    live counts before it and n_kw[zo, v] = 1 (the own-topic case); the
+    draws across 20,000 documents must fit the FP64 conditional."""
+    rng = np.random.default_rng(11)
+    K, zo, La, Dt, eta, alpha = 1000, 517, 3000, 20000, 0.01, 0.1
+    V = 1 + Dt
+    pattern = np.repeat(np.sort(rng.choice(np.delete(np.arange(K), zo), 30, replace=False)), 8)   # 240 tokens
+    docs_w, docs_z = [], []
+    for d in range(Dt):                     # test documents: anchors, then the document's word
+        docs_w.append(np.concatenate([np.zeros(La, np.uint32), [1 + d]]).astype(np.uint32))
+        docs_z.append(np.full(La + 1, zo, np.uint16))
+    for d in range(Dt):                     # background: the word with the shared topic pattern
+        docs_w.append(np.full(len(pattern), 1 + d, np.uint32))
+        docs_z.append(pattern.astype(np.uint16))
+    lens = np.array([len(x) for x in docs_w])
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    words = np.concatenate(docs_w)
+    z0 = np.concatenate(docs_z)
+    prior = np.zeros(K, np.float32)
+    prior[zo] = 1.0
+    eng = T.Engine(K, V, alpha=alpha, eta=eta, seed=123, optim_interval=0, sweep_groups=1)
+    eng.set_word_priors([0], prior[None, :])
+    eng.upload(off, words, z0=z0)
+    # FP64 conditional of a test token from the start-of-sweep counts
+    nk = np.bincount(z0.astype(np.int64), minlength=K).astype(np.float64)
+    col = np.bincount(pattern, minlength=K).astype(np.float64)
+    col[zo] += 1
+    own = (np.arange(K) == zo).astype(np.float64)
+    esum = (V - 1) * eta + prior.astype(np.float64)
+    A = np.full(K, alpha)
+    A[zo] += La
+    w64 = A * (col - own + eta) / (nk - own + esum)
+    p64 = w64 / w64.sum()
+    eng.train(1)
+    z = eng.state()[0]
+    anchors_ok = np.all(z[np.concatenate([np.arange(off[d], off[d] + La) for d in range(0, Dt, 997)]).astype(np.int64)] == zo)
+    assert anchors_ok, "an anchor token left its only allowed topic"
+    draws = z[(off[1:Dt + 1] - 1).astype(np.int64)].astype(np.int64)
+    obs = np.bincount(draws, minlength=K).astype(np.float64)
+    exp = p64 * Dt
+    keep = exp >= 5
+    obs_m = np.append(obs[keep], obs[~keep].sum())
+    exp_m = np.append(exp[keep], exp[~keep].sum())
+    chi2, p = stats.chisquare(obs_m, exp_m)
+    assert p > 1e-4, (chi2, p, int(keep.sum()))
+
+
+def test_full_config1_two_sweeps_bitexact():
+    """The k=20 benchmark corpus in full (V=10k, D=1,000 Poisson(1500)
+    documents, 1.5M tokens): z and every count after two sweeps equal the
+    oracle's restatement bit for bit."""
+    import bench
+    off, w, V = bench.make_corpus(bench.WORKLOADS["c1"])
+    eng = T.Engine(20, V, alpha=0.1, eta=0.01, seed=7, optim_interval=0)
+    eng.upload(off, w)
+    st = oracle_state(off, w, V, 20, 0.1, 0.01, 7)
+    assert_same_state(eng, st)
+    eng.train(2)
+    st.doc_live_sweeps(2, groups=G)
+    assert_same_state(eng, st)
+
+
 @pytest.mark.parametrize("K,V,Tt,D,mean,iters", [(20, 5000, 20, 400, 500, 200), (100, 8000, 50, 1500, 200, 150)])
 def test_ll_per_word_matches_reference_train(K, V, Tt, D, mean, iters):
     """(d) At the same iteration count, the device's ll_per_word is within 1%

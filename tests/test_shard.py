@@ -93,6 +93,9 @@ def test_plan_rejects_bad_shards():
         shard.plan(lens, 2, 2, 5)
 
 
+SPLIT_MIN = 60    # split threshold override: documents of 60+ tokens are split
+
+
 def _rank(rank, world, port, G, iters, out_q):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -108,6 +111,11 @@ def _rank(rank, world, port, G, iters, out_q):
         c = O.Corpus(off, w, V)
         st = O.State(c, K, 0.1, 0.01, seed=5)          # z0 keyed by the global token index
         ar = shard.make_allreduce(memory="host")
+        # long documents are split by the rule of the GLOBAL group (its tokens
+        # over all ranks), so every rank splits the same documents; a low
+        # threshold here makes this small corpus split some
+        order_all, _ = single_groups(lens, G)
+        gtok = [int(lens[order_all[gb[g]:gb[g + 1]].astype(np.int64)].sum()) for g in range(G)]
         for it in range(iters):
             for g in range(G):
                 if gb[g] == gb[g + 1]:
@@ -117,15 +125,18 @@ def _rank(rank, world, port, G, iters, out_q):
                 dk = delta[:V * K].reshape(V, K)
                 dn = delta[V * K:]
                 if len(mine):
-                    O.lib.orc_sweep_doc_live_subset(K, V, O._ptr(st.alpha), st.eta, st.seed, it, D,
-                                                    O._ptr(c.doc_off), O._ptr(c.words), O._ptr(st.ndk),
-                                                    O._ptr(st.nkw), O._ptr(st.nk), O._ptr(dk), O._ptr(dn),
-                                                    O._ptr(st.z), O._ptr(mine), len(mine))
+                    sp = O.SweepSpec(K=K, V=V, alpha=st.alpha.ctypes.data, eta=st.eta, seed=st.seed, iter=it,
+                                     doc_off=c.doc_off.ctypes.data, words=c.words.ctypes.data,
+                                     ndk=st.ndk.ctypes.data, nkw=st.nkw.ctypes.data, nk=st.nk.ctypes.data,
+                                     nkw_next=dk.ctypes.data, nk_next=dn.ctypes.data, z=st.z.ctypes.data,
+                                     split_len=O.split_len_of(gtok[g], K, SPLIT_MIN), slices=O.SPLIT_SLICES,
+                                     step=O.SPLIT_STEP)
+                    O.lib.orc_sweep_docs(C.byref(sp), O._ptr(mine), len(mine))
                 assert ar(None, delta.ctypes.data_as(C.c_void_p), len(delta), 0, None) == 0
                 st.nkw = st.nkw + dk
                 st.nk = st.nk + dn
         ref = O.State(c, K, 0.1, 0.01, seed=5)
-        ref.doc_live_sweeps(iters, groups=G)
+        ref.doc_live_sweeps(iters, groups=G, split_min=SPLIT_MIN)
         own = np.zeros(len(w), bool)
         own[int(off[b]):int(off[e])] = True
         ok = (np.array_equal(st.z[own], ref.z[own]) and np.array_equal(st.ndk[b:e], ref.ndk[b:e])

@@ -56,7 +56,7 @@ class HostAllreduce:
         return ALLREDUCE_FN(cb)
 
 
-def run_sharded(off, w, V, K, cuts, iters, groups, optim, ll=True):
+def run_sharded(off, w, V, K, cuts, iters, groups, optim, ll=True, split=None):
     world = len(cuts) - 1
     lens = np.diff(off.astype(np.int64)).astype(np.uint64)
     har = HostAllreduce(world)
@@ -70,6 +70,8 @@ def run_sharded(off, w, V, K, cuts, iters, groups, optim, ll=True):
             eng = shard.ShardedEngine(K, V, alpha=0.1, eta=0.01, seed=9, optim_interval=optim,
                                       sweep_groups=groups)
             engines.append(eng)
+            if split:
+                eng.set_doc_split(*split)
             eng.upload_shard(loff, lw, lens, b, r, world, allreduce=har.fn(r))
             eng.train(iters)
             z, nkw, nk, alpha = eng.state()
@@ -91,8 +93,10 @@ def run_sharded(off, w, V, K, cuts, iters, groups, optim, ll=True):
     return out, har.calls
 
 
-def run_single(off, w, V, K, iters, groups, optim):
+def run_single(off, w, V, K, iters, groups, optim, split=None):
     eng = T.Engine(K, V, alpha=0.1, eta=0.01, seed=9, optim_interval=optim, sweep_groups=groups)
+    if split:
+        eng.set_doc_split(*split)
     eng.upload(off, w)
     eng.train(iters)
     z, nkw, nk, alpha = eng.state()
@@ -101,13 +105,16 @@ def run_single(off, w, V, K, iters, groups, optim):
     return res
 
 
-@pytest.mark.parametrize("K,groups,cuts", [(24, 4, [0, 150, 400]), (130, 1, [0, 250, 400]),
-                                           (40, 8, [0, 90, 260, 400])])
-def test_sharded_equals_one_gpu(K, groups, cuts):
+@pytest.mark.parametrize("K,groups,cuts,split", [(24, 4, [0, 150, 400], None), (130, 1, [0, 250, 400], None),
+                                                 (40, 8, [0, 90, 260, 400], None),
+                                                 (24, 3, [0, 150, 400], (50, 8))])
+def test_sharded_equals_one_gpu(K, groups, cuts, split):
+    """split: a low threshold, so many documents are split; the split of
+    each group follows the global group, so every rank splits alike."""
     off, w, V = corpus()
     iters = 4
-    ref = run_single(off, w, V, K, iters, groups, 0)
-    out, calls = run_sharded(off, w, V, K, cuts, iters, groups, 0)
+    ref = run_single(off, w, V, K, iters, groups, 0, split)
+    out, calls = run_sharded(off, w, V, K, cuts, iters, groups, 0, split=split)
     z = np.concatenate([o[0] for o in out])
     np.testing.assert_array_equal(z, ref[0])
     for o in out:

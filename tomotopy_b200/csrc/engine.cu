@@ -12,12 +12,16 @@
 // start-of-sweep state: results are bit-identical for any scheduling.
 //
 // Conditional per topic k (getZLikelihoods, LDAModel.hpp:273-285):
-//   w_k = ((float)n_dk[k] + alpha_k) * ((float)(n_kw[k,v] - own) + eta) * R_k
-//   R_k = 1 / ((float)n_k[k] + V*eta), own topic: 1 / ((float)(n_k[k]-1) + V*eta)
-// each operation rounded to nearest (no contraction).  The inclusive scan is
-// segmented: lane l owns topics [l*c, l*c+c), c = ceil(K/32), sums them in
-// order, then a Hillis-Steele scan over the 32 lane totals.  The draw is the
-// first k with u*total < cum[k], else K-1 (sampleFromDiscreteAcc,
+//   w_k = A_k * phi_k,  A_k = (float)n_dk[k] + alpha_k,  phi_k = ((float)n_kw[k,v] + eta) * R_k,
+//   R_k = 1 / ((float)n_k[k] + V*eta)  (phi: the group's per-word table);
+//   the token's own topic zo: phi_own = ((float)(n_kw[zo,v] - 1) + eta) * (1 / ((float)(n_k[zo] - 1) + V*eta))
+// each operation rounded to nearest (no contraction).  Topics are dealt to
+// the 32 lanes in blocks of four (lane l owns k = 128 j + 4 l + i).  Pass 1:
+// each lane's fma chain over its topics with the own topic left out, the
+// owning lane then adding A_zo * phi_own; a Hillis-Steele scan over the lane
+// totals.  Pass 2: the prefix sums of the hit lane's topics.  The draw is
+// the first k (in that order) with u*total < cum[k], else the hit lane's
+// last topic, or K-1 when no lane is hit (sampleFromDiscreteAcc,
 // sample.hpp:133-189).
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -42,6 +46,25 @@ namespace {
 
 using namespace tmtk;
 constexpr int kSweepWarps = 8;           // warps per sweep block
+
+// Long documents: a document of at least split_len tokens (all ids counted)
+// is sampled by a whole block as kSweepWarps slices side by side, merging
+// their n_dk changes every split_step positions (k_sweep_doc, phase 1).  The
+// threshold of a document group is max(kSplitMin, ceil(2 * tokens / 4096)) --
+// documents longer than twice the group's work per warp of a 4096-warp
+// machine -- so it depends on the corpus only, never on the device or on
+// timing; integer counts with K <= kSplitMaxK (the kernels with phase 1 are
+// built for up to 4 blocks of four topics per lane).  tmt_set_doc_split overrides the threshold and the step.
+constexpr uint32_t kSplitStep = 16;
+constexpr uint64_t kSplitMin = 256;
+constexpr uint32_t kSplitMaxK = 512;
+
+uint64_t split_len_of(uint64_t group_tokens, uint32_t K, uint64_t min_len)
+{
+    if (K > kSplitMaxK || min_len >= 0xFFFFFFFFull) return 0;
+    if (min_len) return min_len;
+    return std::max<uint64_t>(kSplitMin, (2 * group_tokens + 4095) / 4096);
+}
 
 
 // ---------------------------------------------------------------------------
@@ -381,6 +404,11 @@ struct SweepArgs {
     uint32_t scan_steps;     // Hillis-Steele steps over the lanes holding topics: ceil(log2(min(32, ceil(K/4))))
     uint32_t rowi_smem;      // 1: the int n_dk row lives in shared memory
     uint32_t dnk_smem;       // 1: n_k deltas aggregate in shared memory
+    // split documents: positions [pos_begin, pos_begin + n_long) are sampled
+    // one per block in slices (phase 1 of k_sweep_doc); 0: none
+    uint32_t n_long;
+    uint32_t split_step;     // positions per slice between merges
+    uint32_t* long_counter;  // phase 1's document counter
 };
 
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
@@ -400,7 +428,9 @@ struct SweepArgs {
 //   WT: weighted counts (TermWeight IDF / PMI): n_dk, n_kw, n_k are floats,
 //       every token carries a weight w, a removal clamps at 0 (updateCnt<true>,
 //       Utils.hpp:132-155) and the count deltas are integers in units of 2^-24.
-template <int CH, int MINB, bool PF, bool WT>
+//   SPLIT: the launch's first n_long documents are split (phase 1); the
+//       kernels without it carry no phase-1 code.
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
 __global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
@@ -417,6 +447,12 @@ k_sweep_doc(SweepArgs a)
     float* s_rowf = reinterpret_cast<float*>(smem + (dnk_smem ? KP : 0));
     float* rowf = s_rowf + warp * KP;
     int* s_rowi = reinterpret_cast<int*>(s_rowf + nwarps * KP);
+    // split documents (integer counts): the document's row C and the slices'
+    // merged changes of the current step, after the per-warp rows
+    constexpr bool split = SPLIT && !WT;
+    int* s_C = s_rowi + nwarps * KP;
+    int* s_dlt = s_C + KP;
+    __shared__ uint32_t s_q;
     if (dnk_smem) {
         for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
         __syncthreads();
@@ -426,9 +462,8 @@ k_sweep_doc(SweepArgs a)
     const float eta = a.eta, veta = a.veta;
     const uint32_t iter = a.iter_ptr ? *a.iter_ptr : a.iter;
 
-    // a token's word weights, the table's own-topic entry phu and the own
-    // topic's weight with the token removed, phio (w: the token's weight)
-    // A word's weights: this lane's blocks of four of its table column.  A
+    // the own topic's word weight with the token removed from n_kw and n_k,
+    // phio (w: the token's weight).  A word's weights: this lane's blocks of four of its table column.  A
     // document's tokens are sorted by word, so about 40% of the tokens of the
     // benchmark corpora repeat the previous token's word: the column stays in
     // registers (the table is the group's snapshot, so it cannot change).
@@ -440,10 +475,8 @@ k_sweep_doc(SweepArgs a)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
     };
-    auto load_word = [&](uint32_t v, int zo, float w, float& phu, float& phio) {
-        const float* ph = a.phi + (uint64_t)v * KP;
+    auto load_word = [&](uint32_t v, int zo, float w, float& phio) {
         const CT nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
-        phu = __ldg(ph + zo);
         float eo = eta;
         if (a.pr.idx) {
             const float* pe = prior_col(a.pr, v, K);
@@ -470,22 +503,292 @@ k_sweep_doc(SweepArgs a)
 
     float4 pv[CHR];                      // the column of word v_have (see load_col)
     uint32_t v_have = 0xFFFFFFFFu;
+    // the current document's alphas and topic mask (the derived models' conditionals)
+    const float* alpha = a.alpha;
+    const uint32_t* dmask = nullptr;
+    auto set_doc = [&](uint64_t d) {
+        alpha = a.arow ? a.alpha_rows + (uint64_t)a.arow[d] * K : a.alpha;
+        dmask = a.mask ? a.mask + d * (uint64_t)a.mw : nullptr;
+    };
+    auto afold = [&](float n, int k) -> float {
+        const float x = __fadd_rn(n, __ldg(alpha + k));
+        return dmask ? __fmul_rn(x, (float)((__ldg(dmask + (k >> 5)) >> (k & 31)) & 1u)) : x;
+    };
+    // Samples the tokens [b, e) of the current document in order with the
+    // document row rowi (counts) / rowf (A_k) live; with dlt != NULL every
+    // change of the row is added to dlt as well.
+    auto run_tokens = [&](uint64_t b, uint64_t e, CT* rowi, float* rowf, int* dlt) {
+            for (uint64_t base = b; base < e; base += 32) {
+                const uint64_t my_i = base + lane;
+                uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
+                float my_u = 0.f, my_wt = 0.f;
+                if (my_i < e) {
+                    my_w = a.words[my_i];
+                    my_z = a.z[my_i];
+                    if (WT) my_wt = a.wt[my_i];
+                    const uint64_t gi = my_i + a.tok_offset;
+                    my_u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamSweep,
+                                                    iter, a.seed));
+                }
+                uint32_t my_new = my_z;
+                unsigned vm = __ballot_sync(FULL, my_i < e && my_w < a.V);
+                if (vm) {
+                    int j = __ffs(vm) - 1;
+                    vm &= vm - 1;
+                    uint32_t v = __shfl_sync(FULL, my_w, j);
+                    int zo = (int)__shfl_sync(FULL, my_z, j);
+                    if (v != v_have) {
+                        load_col(v, pv);
+                        v_have = v;
+                    }
+                    float phi_own;
+                    load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phi_own);
+                    for (;;) {
+                        const int jn = vm ? __ffs(vm) - 1 : -1;
+                        uint32_t vn = 0;
+                        int zon = 0;
+                        float4 pvn[CHR];
+                        float phion = 0.f;
+                        bool new_col = false;
+                        if (PF && jn >= 0) {
+                            vn = __shfl_sync(FULL, my_w, jn);
+                            zon = (int)__shfl_sync(FULL, my_z, jn);
+                            new_col = vn != v;
+                            if (new_col) load_col(vn, pvn);
+                            load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, phion);
+                        }
+                        const float u = __shfl_sync(FULL, my_u, j);
+                        const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
+                        const float* ph = a.phi + (uint64_t)v * KP;
+                        // remove the token from its document.  The own topic's document
+                        // weight Ao is held in a register and its slot of the row is 0
+                        // until the draw is made, so pass 1's chain leaves the own topic
+                        // out exactly and its owner adds Ao * phi_own last: no
+                        // subtract-and-add that could cancel when the own topic dominates its lane
+                        float Ao = 0.f;
+                        if (lane == 0) {
+                            if constexpr (WT) {
+                                float n = __fsub_rn(rowi[zo], wt);
+                                n = n > 0.f ? n : 0.f;
+                                rowi[zo] = n;
+                                Ao = afold(n, zo);
+                            } else {
+                                const int n = rowi[zo] - 1;
+                                rowi[zo] = n;
+                                Ao = afold((float)n, zo);
+                            }
+                            rowf[zo] = 0.f;
+                        }
+                        Ao = __shfl_sync(FULL, Ao, 0);
+                        __syncwarp();
+                        // pass 1: fma chain over this lane's topics
+                        float s = 0.f;
+                        if (CH > 0) {
+    #pragma unroll
+                            for (int jj = 0; jj < CHR; ++jj) {
+                                if (jj < nch) {
+                                    const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
+                                    s = __fmaf_rn(A4.x, pv[jj].x, s);
+                                    s = __fmaf_rn(A4.y, pv[jj].y, s);
+                                    s = __fmaf_rn(A4.z, pv[jj].z, s);
+                                    s = __fmaf_rn(A4.w, pv[jj].w, s);
+                                }
+                            }
+                        } else {
+                            for (int jj = 0; jj < nch; ++jj) {
+                                const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
+                                const float4 P4 = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
+                                s = __fmaf_rn(A4.x, P4.x, s);
+                                s = __fmaf_rn(A4.y, P4.y, s);
+                                s = __fmaf_rn(A4.z, P4.z, s);
+                                s = __fmaf_rn(A4.w, P4.w, s);
+                            }
+                        }
+                        // the own topic, with the token excluded from n_kw and n_k
+                        if (lane == ((zo >> 2) & 31)) s = __fadd_rn(s, __fmul_rn(Ao, phi_own));
+                        // lanes at or above min(32, ceil(K/4)) hold no topics: a Hillis-Steele
+                        // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
+                        // the values of the full scan, and the total sits in lane
+                        // 2^scan_steps - 1
+                        const float x = hs_scan_n(s, lane, a.scan_steps);
+                        float E = __shfl_up_sync(FULL, x, 1);
+                        if (lane == 0) E = 0.f;
+                        const float total = __shfl_sync(FULL, x, (1 << a.scan_steps) - 1);
+                        const float r = __fmul_rn(u, total);
+                        const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
+                        int znew = K - 1;
+                        if (m) {
+                            // pass 2: position among lane h's topics
+                            const int h = __ffs(m) - 1;
+                            const float Eh = __shfl_sync(FULL, E, h);
+                            const int mh = K - 4 * h;
+                            const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
+                            int found = nh - 1;
+                            if (CH > 0 && CH <= 2) {
+                                // at most 8 topics: lane h forms their Hillis-Steele prefix sums
+                                // (the warp-wide scan's order) from the weights in its registers
+                                if (lane == h) {
+                                    float c[4 * CHR];
+    #pragma unroll
+                                    for (int jj = 0; jj < CHR; ++jj) {
+                                        const float4 A4 = jj < nch ? *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * h)
+                                                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+                                        const float av[4] = { A4.x, A4.y, A4.z, A4.w };
+                                        const float pw[4] = { pv[jj].x, pv[jj].y, pv[jj].z, pv[jj].w };
+    #pragma unroll
+                                        for (int i = 0; i < 4; ++i) {
+                                            const int t = 4 * jj + i;
+                                            const int k = 128 * jj + 4 * h + i;
+                                            c[t] = t < nh ? (k == zo ? __fmul_rn(Ao, phi_own) : __fmul_rn(av[i], pw[i])) : 0.f;
+                                        }
+                                    }
+    #pragma unroll
+                                    for (int off = 1; off < 4 * CHR; off <<= 1) {
+    #pragma unroll
+                                        for (int t = 4 * CHR - 1; t >= off; --t) c[t] = __fadd_rn(c[t], c[t - off]);
+                                    }
+                                    bool hit = false;
+    #pragma unroll
+                                    for (int t = 0; t < 4 * CHR; ++t) {
+                                        if (!hit && t < nh && r < __fadd_rn(Eh, c[t])) {
+                                            found = t;
+                                            hit = true;
+                                        }
+                                    }
+                                }
+                                found = __shfl_sync(FULL, found, h);
+                            } else {
+                                // 32 at a time; up to 16 topics (CH == 4) a 4-step scan gives the
+                                // same prefix values
+                                constexpr int kSteps2 = CH == 4 ? 4 : 5;
+                                float carry = 0.f;
+                                for (int mm = 0; mm < nh; mm += 32) {
+                                    const int t = mm + lane;
+                                    const int k = 128 * (t >> 2) + 4 * h + (t & 3);
+                                    float x2 = 0.f;
+                                    if (t < nh) x2 = k == zo ? __fmul_rn(Ao, phi_own) : __fmul_rn(rowf[k], __ldg(ph + k));
+                                    x2 = hs_scan_n(x2, lane, kSteps2);
+                                    const unsigned mb =
+                                        __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
+                                    if (mb) { found = mm + __ffs(mb) - 1; break; }
+                                    carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
+                                }
+                            }
+                            znew = 128 * (found >> 2) + 4 * h + (found & 3);
+                        }
+                        if (lane == 0) {
+                            rowf[zo] = Ao;            // the own topic's slot back (znew's update follows)
+                            if constexpr (WT) {
+                                const float n = __fadd_rn(rowi[znew], wt);
+                                rowi[znew] = n;
+                                rowf[znew] = afold(n, znew);
+                                if (znew != zo) {
+                                    const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(wt, 16777216.f));
+                                    unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
+                                    atomicAdd(dw + zo, 0ull - q);
+                                    atomicAdd(dw + znew, q);
+                                    // n_k's deltas are the column sums of these (k_dk_sum)
+                                }
+                            } else {
+                                const int n = rowi[znew] + 1;
+                                rowi[znew] = n;
+                                rowf[znew] = afold((float)n, znew);
+                                if (znew != zo) {
+                                    atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
+                                    atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
+                                    if (a.dnk_smem) { atomicSub(&s_dnk[zo], 1); atomicAdd(&s_dnk[znew], 1); }
+                                    else { atomicSub(&a.nk_next[zo], 1); atomicAdd(&a.nk_next[znew], 1); }
+                                    if (dlt) { atomicSub(&dlt[zo], 1); atomicAdd(&dlt[znew], 1); }
+                                }
+                            }
+                        }
+                        __syncwarp();
+                        if (lane == j) my_new = (uint32_t)znew;
+                        if (jn < 0) break;
+                        j = jn;
+                        vm &= vm - 1;
+                        if (PF) {
+                            if (new_col) {
+    #pragma unroll
+                                for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
+                                v_have = vn;
+                            }
+                            v = vn;
+                            zo = zon;
+                            phi_own = phion;
+                        } else {
+                            v = __shfl_sync(FULL, my_w, j);
+                            zo = (int)__shfl_sync(FULL, my_z, j);
+                            if (v != v_have) {
+                                load_col(v, pv);
+                                v_have = v;
+                            }
+                            load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phi_own);
+                        }
+                    }
+                }
+                if (my_i < e && my_w < a.V) a.z[my_i] = (uint16_t)my_new;
+            }
+    };
+
+    // Phase 1: split documents, one per block.  The first n_long documents of
+    // this launch hold at least split_len tokens; a block cuts one into
+    // nwarps slices (slice w = [b + w*L/nwarps, b + (w+1)*L/nwarps)) and its
+    // warps sample them side by side in steps of split_step positions, each
+    // with a private copy of the row as of the step's start plus its own
+    // changes; after each step the row C gains all slices' changes.  Only
+    // integer sums are merged, so the result does not depend on timing.
+    if constexpr (split) {
+        CT* prow = reinterpret_cast<CT*>(s_rowi + warp * KP);
+        for (;;) {
+            __syncthreads();                  // the previous document is written back; s_q is free
+            if (threadIdx.x == 0) s_q = atomicAdd(a.long_counter, 1u);
+            __syncthreads();
+            const uint32_t q = s_q;
+            if (q >= a.n_long) break;
+            const uint64_t d = a.doc_order[a.pos_begin + q];
+            set_doc(d);
+            int* grow = reinterpret_cast<int*>(a.ndk) + d * (uint64_t)K;
+            for (int k = threadIdx.x; k < K; k += blockDim.x) {
+                s_C[k] = grow[k];
+                s_dlt[k] = 0;
+            }
+            __syncthreads();
+            const uint64_t b = a.doc_off[d], L = a.doc_off[d + 1] - b;
+            const uint64_t sb = b + (uint64_t)warp * L / nwarps, se = b + (uint64_t)(warp + 1) * L / nwarps;
+            const uint64_t m = a.split_step;
+            const uint64_t steps = ((L + nwarps - 1) / nwarps + m - 1) / m;   // the longest slice's steps
+            for (uint64_t st = 0; st < steps; ++st) {
+                for (int k = lane; k < KP; k += 32) {
+                    const int n = k < K ? s_C[k] : 0;
+                    prow[k] = (CT)n;
+                    rowf[k] = k < K ? afold((float)n, k) : 0.f;
+                }
+                __syncwarp();
+                const uint64_t tb = sb + st * m, te = min(tb + m, se);
+                if (tb < te) run_tokens(tb, te, prow, rowf, s_dlt);
+                __syncthreads();              // every slice's changes of this step are in s_dlt
+                for (int k = threadIdx.x; k < K; k += blockDim.x) {
+                    s_C[k] += s_dlt[k];
+                    s_dlt[k] = 0;
+                }
+                __syncthreads();
+            }
+            for (int k = threadIdx.x; k < K; k += blockDim.x) grow[k] = s_C[k];
+        }
+    }
+
+    // Phase 2: the other documents, one per warp, in order with the row live.
     for (;;) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
         q = __shfl_sync(FULL, q, 0);
-        const uint64_t pos = a.pos_begin + q;
+        const uint64_t pos = a.pos_begin + (split ? a.n_long : 0) + q;
         if (pos >= a.pos_end) break;
         const uint64_t d = a.doc_order[pos];
+        set_doc(d);
         CT* grow = reinterpret_cast<CT*>(a.ndk) + d * (uint64_t)K;
         CT* rowi = a.rowi_smem ? reinterpret_cast<CT*>(s_rowi + warp * KP) : grow;
-        // the document's alphas and topic mask (the derived models' conditionals)
-        const float* alpha = a.arow ? a.alpha_rows + (uint64_t)a.arow[d] * K : a.alpha;
-        const uint32_t* dmask = a.mask ? a.mask + d * (uint64_t)a.mw : nullptr;
-        auto afold = [&](float n, int k) -> float {
-            const float x = __fadd_rn(n, __ldg(alpha + k));
-            return dmask ? __fmul_rn(x, (float)((__ldg(dmask + (k >> 5)) >> (k & 31)) & 1u)) : x;
-        };
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f;
             if (k < K) {
@@ -496,211 +799,7 @@ k_sweep_doc(SweepArgs a)
             rowf[k] = f;
         }
         __syncwarp();
-        const uint64_t b = a.doc_off[d], e = a.doc_off[d + 1];
-        for (uint64_t base = b; base < e; base += 32) {
-            const uint64_t my_i = base + lane;
-            uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
-            float my_u = 0.f, my_wt = 0.f;
-            if (my_i < e) {
-                my_w = a.words[my_i];
-                my_z = a.z[my_i];
-                if (WT) my_wt = a.wt[my_i];
-                const uint64_t gi = my_i + a.tok_offset;
-                my_u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamSweep,
-                                                iter, a.seed));
-            }
-            uint32_t my_new = my_z;
-            unsigned vm = __ballot_sync(FULL, my_i < e && my_w < a.V);
-            if (vm) {
-                int j = __ffs(vm) - 1;
-                vm &= vm - 1;
-                uint32_t v = __shfl_sync(FULL, my_w, j);
-                int zo = (int)__shfl_sync(FULL, my_z, j);
-                if (v != v_have) {
-                    load_col(v, pv);
-                    v_have = v;
-                }
-                float phu, phi_own;
-                load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phu, phi_own);
-                for (;;) {
-                    const int jn = vm ? __ffs(vm) - 1 : -1;
-                    uint32_t vn = 0;
-                    int zon = 0;
-                    float4 pvn[CHR];
-                    float phun = 0.f, phion = 0.f;
-                    bool new_col = false;
-                    if (PF && jn >= 0) {
-                        vn = __shfl_sync(FULL, my_w, jn);
-                        zon = (int)__shfl_sync(FULL, my_z, jn);
-                        new_col = vn != v;
-                        if (new_col) load_col(vn, pvn);
-                        load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, phun, phion);
-                    }
-                    const float u = __shfl_sync(FULL, my_u, j);
-                    const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
-                    const float* ph = a.phi + (uint64_t)v * KP;
-                    if (lane == 0) {          // remove the token from its document
-                        if constexpr (WT) {
-                            float n = __fsub_rn(rowi[zo], wt);
-                            n = n > 0.f ? n : 0.f;
-                            rowi[zo] = n;
-                            rowf[zo] = afold(n, zo);
-                        } else {
-                            const int n = rowi[zo] - 1;
-                            rowi[zo] = n;
-                            rowf[zo] = afold((float)n, zo);
-                        }
-                    }
-                    __syncwarp();
-                    // pass 1: fma chain over this lane's topics
-                    float s = 0.f;
-                    if (CH > 0) {
-#pragma unroll
-                        for (int jj = 0; jj < CHR; ++jj) {
-                            if (jj < nch) {
-                                const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
-                                s = __fmaf_rn(A4.x, pv[jj].x, s);
-                                s = __fmaf_rn(A4.y, pv[jj].y, s);
-                                s = __fmaf_rn(A4.z, pv[jj].z, s);
-                                s = __fmaf_rn(A4.w, pv[jj].w, s);
-                            }
-                        }
-                    } else {
-                        for (int jj = 0; jj < nch; ++jj) {
-                            const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
-                            const float4 P4 = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
-                            s = __fmaf_rn(A4.x, P4.x, s);
-                            s = __fmaf_rn(A4.y, P4.y, s);
-                            s = __fmaf_rn(A4.z, P4.z, s);
-                            s = __fmaf_rn(A4.w, P4.w, s);
-                        }
-                    }
-                    if (lane == ((zo >> 2) & 31)) {   // the own topic: exclude the token from n_kw, n_k
-                        const float Ao = rowf[zo];
-                        s = fmaxf(__fadd_rn(__fsub_rn(s, __fmul_rn(Ao, phu)), __fmul_rn(Ao, phi_own)), 0.f);
-                    }
-                    // lanes at or above min(32, ceil(K/4)) hold no topics: a Hillis-Steele
-                    // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
-                    // the values of the full scan, and the total sits in lane
-                    // 2^scan_steps - 1
-                    const float x = hs_scan_n(s, lane, a.scan_steps);
-                    float E = __shfl_up_sync(FULL, x, 1);
-                    if (lane == 0) E = 0.f;
-                    const float total = __shfl_sync(FULL, x, (1 << a.scan_steps) - 1);
-                    const float r = __fmul_rn(u, total);
-                    const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
-                    int znew = K - 1;
-                    if (m) {
-                        // pass 2: position among lane h's topics
-                        const int h = __ffs(m) - 1;
-                        const float Eh = __shfl_sync(FULL, E, h);
-                        const int mh = K - 4 * h;
-                        const int nh = 4 * (mh >> 7) + min(mh & 127, 4);
-                        int found = nh - 1;
-                        if (CH > 0 && CH <= 2) {
-                            // at most 8 topics: lane h forms their Hillis-Steele prefix sums
-                            // (the warp-wide scan's order) from the weights in its registers
-                            if (lane == h) {
-                                float c[4 * CHR];
-#pragma unroll
-                                for (int jj = 0; jj < CHR; ++jj) {
-                                    const float4 A4 = jj < nch ? *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * h)
-                                                               : make_float4(0.f, 0.f, 0.f, 0.f);
-                                    const float av[4] = { A4.x, A4.y, A4.z, A4.w };
-                                    const float pw[4] = { pv[jj].x, pv[jj].y, pv[jj].z, pv[jj].w };
-#pragma unroll
-                                    for (int i = 0; i < 4; ++i) {
-                                        const int t = 4 * jj + i;
-                                        const int k = 128 * jj + 4 * h + i;
-                                        c[t] = t < nh ? __fmul_rn(av[i], k == zo ? phi_own : pw[i]) : 0.f;
-                                    }
-                                }
-#pragma unroll
-                                for (int off = 1; off < 4 * CHR; off <<= 1) {
-#pragma unroll
-                                    for (int t = 4 * CHR - 1; t >= off; --t) c[t] = __fadd_rn(c[t], c[t - off]);
-                                }
-                                bool hit = false;
-#pragma unroll
-                                for (int t = 0; t < 4 * CHR; ++t) {
-                                    if (!hit && t < nh && r < __fadd_rn(Eh, c[t])) {
-                                        found = t;
-                                        hit = true;
-                                    }
-                                }
-                            }
-                            found = __shfl_sync(FULL, found, h);
-                        } else {
-                            // 32 at a time; up to 16 topics (CH == 4) a 4-step scan gives the
-                            // same prefix values
-                            constexpr int kSteps2 = CH == 4 ? 4 : 5;
-                            float carry = 0.f;
-                            for (int mm = 0; mm < nh; mm += 32) {
-                                const int t = mm + lane;
-                                const int k = 128 * (t >> 2) + 4 * h + (t & 3);
-                                float x2 = 0.f;
-                                if (t < nh) x2 = __fmul_rn(rowf[k], k == zo ? phi_own : __ldg(ph + k));
-                                x2 = hs_scan_n(x2, lane, kSteps2);
-                                const unsigned mb =
-                                    __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
-                                if (mb) { found = mm + __ffs(mb) - 1; break; }
-                                carry = __fadd_rn(carry, __shfl_sync(FULL, x2, 31));
-                            }
-                        }
-                        znew = 128 * (found >> 2) + 4 * h + (found & 3);
-                    }
-                    if (lane == 0) {
-                        if constexpr (WT) {
-                            const float n = __fadd_rn(rowi[znew], wt);
-                            rowi[znew] = n;
-                            rowf[znew] = afold(n, znew);
-                            if (znew != zo) {
-                                const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(wt, 16777216.f));
-                                unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
-                                atomicAdd(dw + zo, 0ull - q);
-                                atomicAdd(dw + znew, q);
-                                // n_k's deltas are the column sums of these (k_dk_sum)
-                            }
-                        } else {
-                            const int n = rowi[znew] + 1;
-                            rowi[znew] = n;
-                            rowf[znew] = afold((float)n, znew);
-                            if (znew != zo) {
-                                atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
-                                atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
-                                if (a.dnk_smem) { atomicSub(&s_dnk[zo], 1); atomicAdd(&s_dnk[znew], 1); }
-                                else { atomicSub(&a.nk_next[zo], 1); atomicAdd(&a.nk_next[znew], 1); }
-                            }
-                        }
-                    }
-                    __syncwarp();
-                    if (lane == j) my_new = (uint32_t)znew;
-                    if (jn < 0) break;
-                    j = jn;
-                    vm &= vm - 1;
-                    if (PF) {
-                        if (new_col) {
-#pragma unroll
-                            for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
-                            v_have = vn;
-                        }
-                        v = vn;
-                        zo = zon;
-                        phu = phun;
-                        phi_own = phion;
-                    } else {
-                        v = __shfl_sync(FULL, my_w, j);
-                        zo = (int)__shfl_sync(FULL, my_z, j);
-                        if (v != v_have) {
-                            load_col(v, pv);
-                            v_have = v;
-                        }
-                        load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phu, phi_own);
-                    }
-                }
-            }
-            if (my_i < e && my_w < a.V) a.z[my_i] = (uint16_t)my_new;
-        }
+        run_tokens(a.doc_off[d], a.doc_off[d + 1], rowi, rowf, nullptr);
         __syncwarp();
         if (a.rowi_smem)
             for (int k = lane; k < K; k += 32) grow[k] = rowi[k];
@@ -1015,6 +1114,14 @@ struct tmt_handle {
     float* d_rm1 = nullptr;          // K: the own topic's reciprocal of the snapshot
     uint32_t groups = 1;             // document groups per sweep
     std::vector<uint64_t> group_bounds;   // doc_order positions: group g = [b[g], b[g+1])
+    // long documents (k_sweep_doc phase 1): per group, the tokens of the
+    // global group, and the number of its first (longest) local documents
+    // that are split; the lengths of the local documents in doc_order
+    std::vector<uint64_t> group_tokens;
+    std::vector<uint32_t> group_nlong;
+    std::vector<uint64_t> order_len;
+    uint64_t split_min = 0;          // 0: the rule (split_len_of); >= 2^32 - 1: never
+    uint32_t split_step = kSplitStep;
     // a corpus sharded across GPUs (tmt_upload_shard); world == 1: this GPU holds all of it
     uint32_t rank = 0, world = 1;
     uint64_t D_global = 0, tok_offset = 0;
@@ -1056,7 +1163,8 @@ struct tmt_handle {
     std::vector<int> group_variant;  // per document group, the fastest variant
     std::vector<std::vector<float>> group_ms;   // tuning: per group, per variant
     std::vector<cudaEvent_t> gev;    // tuning: start/end of each group's sweep kernel
-    std::vector<std::pair<const void*, int>> occ;   // blocks per SM of each sweep kernel launched
+    struct Occ { const void* kern; uint32_t smem; int per_sm; };
+    std::vector<Occ> occ;            // blocks per SM of each sweep kernel and shared-memory size launched
     // captured sweeps (single GPU, after tuning): one graph per starting buffer parity
     bool graphs = true;
     uint32_t* d_step = nullptr;
@@ -1333,7 +1441,11 @@ struct SweepShape {
 
 // rowi_global: the document's count row stays in global memory (L1-cached),
 // halving the shared memory of a warp (the occupancy variant)
-SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false)
+// split: the launch samples split documents (phase 1): every warp gets a
+// private row in shared memory whatever the variant, and the block the
+// document's row and the step's merged changes (K <= kSplitMaxK keeps the
+// block at kSweepWarps warps)
+SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool split = false)
 {
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
@@ -1342,31 +1454,37 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false)
     // (k_dk_sum): 64-bit shared-memory atomics per token cost ~17 ms a sweep
     s.dnk_smem = !weighted && K <= 16384u;
     s.rowi_smem = K <= 8192 && !rowi_global;
-    const uint32_t per_warp = 4 * KP + (s.rowi_smem ? 4 * KP : 0);
-    const uint32_t fixed = s.dnk_smem ? 4 * KP : 0;
+    const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0);
+    const uint32_t fixed = (s.dnk_smem ? 4 * KP : 0) + (split ? 8 * KP : 0);
     uint32_t w = (budget - fixed) / per_warp;
     s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
     s.smem = fixed + s.warps * per_warp;
     return s;
 }
 
-template <int CH, int MINB, bool PF, bool WT>
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF, WT>;
-    // attribute and occupancy once per kernel (the shape depends on K only),
-    // so a captured sweep makes no such call
+    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT>;
+    // attribute and occupancy once per kernel and shared-memory size (the
+    // shapes depend on K and on whether the launch splits documents), so a
+    // captured sweep makes no such call; the attribute allows the largest shape
     int per_sm = 0;
     for (const auto& e : h->occ)
-        if (e.first == (const void*)kern) per_sm = e.second;
+        if (e.kern == (const void*)kern && e.smem == sh.smem) per_sm = e.per_sm;
     if (per_sm == 0) {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+        const uint32_t KP = round4(a.K);
+        const uint32_t most = std::max(sh.smem, sweep_shape(a.K, WT, false, !WT && a.K <= kSplitMaxK).smem);
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(most, 4 * KP)));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sh.warps * 32, sh.smem));
         if (per_sm < 1) throw CudaError("sweep kernel does not fit on an SM");
-        h->occ.emplace_back((const void*)kern, per_sm);
+        h->occ.push_back({ (const void*)kern, sh.smem, per_sm });
     }
-    const uint64_t docs = a.pos_end - a.pos_begin;
-    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms, (docs + sh.warps - 1) / sh.warps);
+    // a split document takes a block; the others a warp each
+    const uint64_t n_long = SPLIT ? a.n_long : 0;
+    const uint64_t docs = a.pos_end - a.pos_begin - n_long;
+    uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)per_sm * h->num_sms,
+                                                 n_long + (docs + sh.warps - 1) / sh.warps);
     if (grid == 0) grid = 1;
     kern<<<grid, sh.warps * 32, sh.smem, h->stream>>>(a);
     launch_check(h);
@@ -1379,6 +1497,14 @@ template <int CH, bool WT>
 void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, int variant)
 {
     constexpr bool kPrefetch = CH <= 8;   // above, the prefetch registers spill
+    // split documents: integer counts, up to 4 blocks of four topics per lane
+    constexpr bool kSplit = !WT && CH >= 1 && CH <= 4;
+    if (kSplit && a.n_long > 0) {
+        if (variant == 2) launch_sweep_t<CH, 4, false, WT, kSplit>(h, a, sh);
+        else if (variant == 1) launch_sweep_t<CH, 3, false, WT, kSplit>(h, a, sh);
+        else launch_sweep_t<CH, 2, kPrefetch, WT, kSplit>(h, a, sh);
+        return;
+    }
     if (variant == 2) launch_sweep_t<CH, 4, false, WT>(h, a, sh);
     else if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
     else launch_sweep_t<CH, 2, kPrefetch, WT>(h, a, sh);
@@ -1401,7 +1527,9 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const uint32_t KP = round4(a.K);
     const uint32_t ch = (KP + 127) / 128;
     const bool wt = a.wt != nullptr;
-    const SweepShape sh = sweep_shape(a.K, wt, variant == 2);
+    const SweepShape sh = sweep_shape(a.K, wt, variant == 2, !wt && a.n_long > 0);
+    if (!wt && a.n_long > 0 && sh.warps != (uint32_t)kSweepWarps)
+        throw CudaError("split documents need a block of " + std::to_string(kSweepWarps) + " warps");
     SweepArgs b = a;
     b.rowi_smem = sh.rowi_smem;
     b.dnk_smem = sh.dnk_smem;
@@ -1429,9 +1557,11 @@ void exchange(tmt_handle* h, void* buf, uint64_t count, int32_t dtype)
     if (rc != 0) throw CudaError("allreduce across ranks failed (" + std::to_string(rc) + ")");
 }
 
+// The launch arguments of document group g.
 SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32_t* nkw_next, int32_t* nk_next,
-                     uint64_t pos_begin, uint64_t pos_end)
+                     uint32_t g)
 {
+    const uint64_t pos_begin = h->group_bounds[g], pos_end = h->group_bounds[g + 1];
     SweepArgs a{};
     a.doc_off = h->d_doc_off;
     a.words = h->d_words;
@@ -1468,6 +1598,9 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.arow = h->d_arow;
     a.mask = h->d_mask;
     a.mw = (h->cfg.K + 31) / 32;
+    a.n_long = h->weighted ? 0 : h->group_nlong[g];
+    a.split_step = h->split_step;
+    a.long_counter = h->d_counter + 1;
     return a;
 }
 
@@ -1500,10 +1633,9 @@ void do_sweep_sharded(tmt_handle* h)
                                                         h->d_rm1);
         launch_check(h);
         if (h->group_bounds[g] < h->group_bounds[g + 1]) {
-            CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
+            CK(cudaMemsetAsync(h->d_counter, 0, 2 * sizeof(uint32_t), h->stream));
             tune_mark(h, g, 0);
-            launch_sweep(h, sweep_args(h, h->d_nkw[0], h->d_nk[0], dnkw, dnk, h->group_bounds[g],
-                                       h->group_bounds[g + 1]), variant_of(h, g));
+            launch_sweep(h, sweep_args(h, h->d_nkw[0], h->d_nk[0], dnkw, dnk, g), variant_of(h, g));
             tune_mark(h, g, 1);
         }
         exchange(h, h->d_delta, KV + K, TMT_I32);
@@ -1553,9 +1685,8 @@ void do_sweep_w(tmt_handle* h, bool capture)
         k_phi_fold_w<<<grid, 256, smem_k * 4, h->stream>>>(nkw, h->d_dkw, nk, V, K, round4(K), h->cfg.eta, veta,
                                                          h->d_phi, smem_k, pending ? 1 : 0, h->prior_args());
         launch_check(h);
-        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
-        SweepArgs a = sweep_args(h, h->d_nkw[0], h->d_nk[0], nullptr, nullptr, h->group_bounds[g],
-                                 h->group_bounds[g + 1]);
+        CK(cudaMemsetAsync(h->d_counter, 0, 2 * sizeof(uint32_t), h->stream));
+        SweepArgs a = sweep_args(h, h->d_nkw[0], h->d_nk[0], nullptr, nullptr, g);
         a.wt = h->d_wt;
         a.dkw = h->d_dkw;
         a.dk = h->d_dk;
@@ -1603,9 +1734,8 @@ void do_sweep(tmt_handle* h, bool capture = false)
                                                         veta, h->d_phi, h->d_nkw[nxt], h->d_nk[nxt], smem_k,
                                                         h->prior_args(), h->d_rm1);
         launch_check(h);
-        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(uint32_t), h->stream));
-        SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt],
-                                 h->group_bounds[g], h->group_bounds[g + 1]);
+        CK(cudaMemsetAsync(h->d_counter, 0, 2 * sizeof(uint32_t), h->stream));
+        SweepArgs a = sweep_args(h, h->d_nkw[cur], h->d_nk[cur], h->d_nkw[nxt], h->d_nk[nxt], g);
         if (capture) a.iter_ptr = h->d_step;
         if (!capture) {
             if (!recorded) { CK(cudaEventRecord(h->kev0, h->stream)); recorded = true; }
@@ -1736,6 +1866,7 @@ struct ShardPlan {
     std::vector<uint32_t> order;        // local document indices, global order
     std::vector<uint64_t> bounds;       // group g = order[bounds[g] .. bounds[g+1])
     std::vector<uint64_t> gbounds;      // group g holds global positions [gbounds[g], gbounds[g+1])
+    std::vector<uint64_t> gtokens;      // group g's tokens over all ranks
     uint64_t tok_offset = 0;
 };
 
@@ -1767,6 +1898,7 @@ ShardPlan plan_shard(const uint64_t* len, uint64_t D_global, uint32_t groups, ui
     p.gbounds[G] = D_global;
     p.bounds.assign(G + 1, 0);
     p.order.reserve(D_local);
+    p.gtokens.assign(G, 0);
     uint64_t prefix = 0, g = 1;
     for (uint64_t q = 0; q < D_global; ++q) {
         while (g < G && prefix * G >= g * total) {
@@ -1777,6 +1909,7 @@ ShardPlan plan_shard(const uint64_t* len, uint64_t D_global, uint32_t groups, ui
         const uint64_t d = gorder[q];
         if (d >= doc_begin && d - doc_begin < D_local) p.order.push_back((uint32_t)(d - doc_begin));
         prefix += len[d];
+        p.gtokens[g - 1] += len[d];
     }
     for (; g < G; ++g) {
         p.gbounds[g] = D_global;
@@ -1784,6 +1917,24 @@ ShardPlan plan_shard(const uint64_t* len, uint64_t D_global, uint32_t groups, ui
     }
     p.bounds[G] = p.order.size();
     return p;
+}
+
+// Per document group, how many of its first (longest) local documents are
+// split: those of at least the group's split_len tokens (split_len_of over the
+// global group's tokens, so every rank of a sharded corpus agrees).
+void update_split(tmt_handle* h)
+{
+    if (h->group_bounds.empty()) return;
+    const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
+    h->group_nlong.assign(G, 0);
+    if (h->weighted) return;
+    for (uint32_t g = 0; g < G; ++g) {
+        const uint64_t sl = split_len_of(h->group_tokens[g], h->cfg.K, h->split_min);
+        if (!sl) continue;
+        uint32_t n = 0;
+        for (uint64_t q = h->group_bounds[g]; q < h->group_bounds[g + 1] && h->order_len[q] >= sl; ++q) ++n;
+        h->group_nlong[g] = n;
+    }
 }
 
 void validate_config(const tmt_config& c)
@@ -1887,7 +2038,11 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         h->tok_offset = plan.tok_offset;
         h->group_bounds = plan.bounds;
         h->gbounds = plan.gbounds;
+        h->group_tokens = plan.gtokens;
         const std::vector<uint32_t>& order = plan.order;
+        h->order_len.resize(D);
+        for (uint64_t q = 0; q < D; ++q) h->order_len[q] = doc_off[order[q] + 1] - doc_off[order[q]];
+        update_split(h);
 
         h->d_doc_off = h->dalloc<uint64_t>(D + 1);
         h->d_words = h->dalloc<uint32_t>(n_all);
@@ -1966,7 +2121,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
         }
         h->d_doc_len = h->dalloc<int32_t>(D);
         h->d_doc_order = h->dalloc<uint32_t>(D);
-        h->d_counter = h->dalloc<uint32_t>(1);
+        h->d_counter = h->dalloc<uint32_t>(2);      // phase 2's (warp) and phase 1's (block) document counters
         h->d_alpha = h->dalloc<float>(K);
         h->d_asum = h->dalloc<float>(1);
         h->d_lg_alpha = h->dalloc<double>(K);
@@ -2447,6 +2602,27 @@ tmt_status tmt_get_sweep_variants(const tmt_handle* h, int32_t* out, uint32_t ca
     *n = (uint32_t)h->group_variant.size();
     if (out)
         for (uint32_t g = 0; g < *n && g < cap; ++g) out[g] = h->tuned < 0 ? -1 : h->group_variant[g];
+    return TMT_OK;
+}
+
+tmt_status tmt_set_doc_split(tmt_handle* h, uint64_t min_tokens, uint32_t step)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (step > 65536) throw ArgError("split step above 65536 positions");
+        h->split_min = min_tokens;
+        h->split_step = step ? step : kSplitStep;
+        h->drop_graphs();          // the split is an argument of the captured launches
+        update_split(h);
+    });
+}
+
+tmt_status tmt_get_doc_split(const tmt_handle* h, uint32_t* n_long, uint32_t cap, uint32_t* n)
+{
+    if (!h || !n) return TMT_ERR_INVALID_ARGUMENT;
+    *n = (uint32_t)h->group_nlong.size();
+    if (n_long)
+        for (uint32_t g = 0; g < *n && g < cap; ++g) n_long[g] = h->group_nlong[g];
     return TMT_OK;
 }
 

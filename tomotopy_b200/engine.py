@@ -108,6 +108,20 @@ class Engine:
         check(lib.tmt_get_sweep_variants(self.h, _p(out), n.value, C.byref(n)), self.h)
         return out[:n.value].tolist()
 
+    def set_doc_split(self, min_tokens=0, step=0):
+        """tmt_set_doc_split: documents of at least min_tokens tokens are
+        sampled as 8 slices merging every `step` positions (0: the engine's
+        rule / step; 2**32 - 1: never split)."""
+        check(lib.tmt_set_doc_split(self.h, int(min_tokens), int(step)), self.h)
+
+    def doc_split(self):
+        """Per document group, how many documents are split."""
+        n = C.c_uint32()
+        check(lib.tmt_get_doc_split(self.h, None, 0, C.byref(n)), self.h)
+        out = np.zeros(max(n.value, 1), dtype=np.uint32)
+        check(lib.tmt_get_doc_split(self.h, _p(out), n.value, C.byref(n)), self.h)
+        return out[:n.value].tolist()
+
     def set_graphs(self, enable):
         """Sweeps as CUDA graph launches after the autotuner's first sweeps
         (default) or as separate kernel launches; results are identical."""
