@@ -430,12 +430,16 @@ struct SweepArgs {
 //       Utils.hpp:132-155) and the count deltas are integers in units of 2^-24.
 //   SPLIT: the launch's first n_long documents are split (phase 1); the
 //       kernels without it carry no phase-1 code.
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
+//   COL: the current word's table column stays in registers across tokens of
+//       the same word; without it (CH >= 4 only) pass 1 reads the column from
+//       L1 / L2 every token, which frees ~4*CH registers for occupancy.
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool COL = true>
 __global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
     using CT = typename std::conditional<WT, float, int>::type;
-    constexpr int CHR = CH > 0 ? CH : 1;
+    static_assert(COL || (CH >= 4 && !PF), "the column-free kernel is built for 4+ blocks per lane");
+    constexpr int CHR = CH > 0 ? (COL ? CH : 1) : 1;
     extern __shared__ __align__(16) int smem[];
     const int K = (int)a.K;
     const int KP = (int)round4(a.K);
@@ -469,7 +473,7 @@ k_sweep_doc(SweepArgs a)
     // registers (the table is the group's snapshot, so it cannot change).
     auto load_col = [&](uint32_t v, float4 (&pv)[CHR]) {
         const float* ph = a.phi + (uint64_t)v * KP;
-        if (CH > 0) {
+        if (CH > 0 && COL) {
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
@@ -583,7 +587,19 @@ k_sweep_doc(SweepArgs a)
                         __syncwarp();
                         // pass 1: fma chain over this lane's topics
                         float s = 0.f;
-                        if (CH > 0) {
+                        if (CH > 0 && !COL) {
+    #pragma unroll
+                            for (int jj = 0; jj < CH; ++jj) {
+                                if (jj < nch) {
+                                    const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
+                                    const float4 P4 = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
+                                    s = __fmaf_rn(A4.x, P4.x, s);
+                                    s = __fmaf_rn(A4.y, P4.y, s);
+                                    s = __fmaf_rn(A4.z, P4.z, s);
+                                    s = __fmaf_rn(A4.w, P4.w, s);
+                                }
+                            }
+                        } else if (CH > 0) {
     #pragma unroll
                             for (int jj = 0; jj < CHR; ++jj) {
                                 if (jj < nch) {
@@ -1462,10 +1478,10 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     return s;
 }
 
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool COL = true>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT>;
+    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT, COL>;
     // attribute and occupancy once per kernel and shared-memory size (the
     // shapes depend on K and on whether the launch splits documents), so a
     // captured sweep makes no such call; the attribute allows the largest shape
@@ -1492,7 +1508,17 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
 // topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
-// document row in global memory, 4 blocks/SM.
+// document row in global memory, 4 blocks/SM; 3 (4 to 16 blocks of four per
+// lane) = variant 2 without the register column, kColMinB blocks/SM.
+constexpr int kColMinB = 6;
+
+int sweep_variants_for(uint32_t K)
+{
+    const uint32_t ch = (round4(K) + 127) / 128;
+    if (ch > 32) return 1;
+    return ch >= 4 && ch <= 16 ? 4 : 3;
+}
+
 template <int CH, bool WT>
 void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, int variant)
 {
@@ -1500,12 +1526,18 @@ void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, in
     // split documents: integer counts, up to 4 blocks of four topics per lane
     constexpr bool kSplit = !WT && CH >= 1 && CH <= 4;
     if (kSplit && a.n_long > 0) {
-        if (variant == 2) launch_sweep_t<CH, 4, false, WT, kSplit>(h, a, sh);
+        if (variant >= 2) launch_sweep_t<CH, 4, false, WT, kSplit>(h, a, sh);
         else if (variant == 1) launch_sweep_t<CH, 3, false, WT, kSplit>(h, a, sh);
         else launch_sweep_t<CH, 2, kPrefetch, WT, kSplit>(h, a, sh);
         return;
     }
-    if (variant == 2) launch_sweep_t<CH, 4, false, WT>(h, a, sh);
+    if constexpr (CH >= 4 && CH <= 16) {
+        if (variant == 3) {
+            launch_sweep_t<CH, kColMinB, false, WT, false, false>(h, a, sh);
+            return;
+        }
+    }
+    if (variant >= 2) launch_sweep_t<CH, 4, false, WT>(h, a, sh);
     else if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
     else launch_sweep_t<CH, 2, kPrefetch, WT>(h, a, sh);
 }
@@ -1527,7 +1559,7 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const uint32_t KP = round4(a.K);
     const uint32_t ch = (KP + 127) / 128;
     const bool wt = a.wt != nullptr;
-    const SweepShape sh = sweep_shape(a.K, wt, variant == 2, !wt && a.n_long > 0);
+    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, !wt && a.n_long > 0);
     if (!wt && a.n_long > 0 && sh.warps != (uint32_t)kSweepWarps)
         throw CudaError("split documents need a block of " + std::to_string(kSweepWarps) + " warps");
     SweepArgs b = a;
@@ -2106,7 +2138,7 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             // the first n_variants sweeps run eagerly, one variant each, and
             // every group keeps its fastest
             const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
-            h->n_variants = round4(K) <= 4096 ? 3 : 1;
+            h->n_variants = sweep_variants_for(K);
             h->variant = 0;
             h->tune_step = 0;
             h->tuned = -1;
