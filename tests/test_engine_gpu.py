@@ -172,14 +172,16 @@ def test_pageable_uploads_through_staging():
 @pytest.mark.parametrize("K,groups", [(1, 1), (5, 1), (20, 1), (33, 3), (100, 1), (100, 4), (250, 1), (1000, 1),
                                       (1000, 2), (1100, 1), (3000, 1)])
 def test_sweeps_bitexact(K, groups):
-    """Every sweep's z and counts equal the oracle's doc-major sweep exactly."""
+    """Every sweep's z and counts equal the oracle's doc-major sweep exactly:
+    the autotuner's sweeps (every kernel variant, in the order 0, 1, .., n-1,
+    n-1, .., 0) and the graph sweeps after them."""
     off, w, V = corpus(V=600, D=90, mean=50, seed=K, min_cf=2, rm_top=3)
     alpha = np.float32(0.1) if K != 20 else (0.05 * (np.arange(K) + 1)).astype(np.float32)
     eng = T.Engine(K, V, alpha=alpha, eta=0.01, seed=7, optim_interval=0, sweep_groups=groups)
     eng.upload(off, w)
     st = oracle_state(off, w, V, K, alpha, 0.01, 7)
     step = 0
-    for n in (1, 2):
+    for n in (1, 2, 2, 5):
         eng.train(n)
         st.doc_live_sweeps(n, start_step=step, groups=groups)
         step += n
