@@ -201,6 +201,23 @@ tmt_status tmt_set_doc_topic_mask(tmt_handle* h, const uint32_t* mask_bits);
  * alpha optimiser is skipped (DMR fits its own lambda).  After the upload;
  * alpha_rows == NULL clears.  Single GPU. */
 tmt_status tmt_set_doc_alpha(tmt_handle* h, uint32_t M, const float* alpha_rows, const uint32_t* doc_row);
+/* Shared document rows: PTModel's pseudo-documents (PTModel.hpp:13-24, 72-114).
+ * Document d's tokens count in row row_of_doc[d] of an R x K n_dk (the
+ * pseudo-document's numByTopicPDoc column) instead of its own row: the
+ * conditional's document factor is (n_row,k + alpha_k), a sweep samples each
+ * row's documents one after another (ascending document index) with the row
+ * live -- as PT's PARTITION keeps a pseudo-document's documents on one worker
+ * (PTModel.hpp:206-235) -- and the rows are scheduled like documents (longest
+ * first, equal-token groups).  The rows are recounted from z on every call,
+ * so a caller that re-assigns pseudo-documents (PTModel::samplePseudoDoc,
+ * every pseudoDocSamplingInterval sweeps; it stays on the host) calls this
+ * again.  tmt_ll's ll_docs and the alpha optimiser then run over the R rows
+ * (PTModel::getLLRest's pseudo-document terms, without the lambda term over
+ * numDocsByPDoc, which the caller adds; PTModel::optimizeParameters);
+ * tmt_download_doc_topic returns the R rows.  Documents are not split.
+ * After the upload; integer counts, one GPU, no per-document masks or alphas;
+ * row_of_doc == NULL returns to one row per document (recounted from z). */
+tmt_status tmt_set_doc_rows(tmt_handle* h, uint64_t R, const uint32_t* row_of_doc);
 /* Word priors: LDAModel::setWordPrior (LDAModel.hpp:1031-1045) as applied by
  * prepareWordPriors (:724-737).  Word word_ids[p] (< V, each once) gets the
  * K-vector priors[p*K .. p*K+K-1] (finite, >= 0) as its eta column; every

@@ -39,7 +39,8 @@ class SweepSpec(C.Structure):
                 ("doc_off", C.c_void_p), ("words", C.c_void_p),
                 ("ndk", C.c_void_p), ("nkw", C.c_void_p), ("nk", C.c_void_p),
                 ("nkw_next", C.c_void_p), ("nk_next", C.c_void_p), ("z", C.c_void_p),
-                ("split_len", C.c_uint64), ("slices", C.c_uint32), ("step", C.c_uint32)]
+                ("split_len", C.c_uint64), ("slices", C.c_uint32), ("step", C.c_uint32),
+                ("unit_off", C.c_void_p), ("unit_docs", C.c_void_p)]
 
 
 # The long-document split of the device sweep (engine.cu, split_len_of): a
@@ -616,6 +617,75 @@ class StateM(State):
             c = self.c
             a = lib.orc_ll_docs_m_f64(c.D, self.K, _ptr(self.ndk), _ptr(c.doc_len), _ptr(self.alpha_rows),
                                       _ptr(self.doc_row))
+        return a, b
+
+
+class StateR(State):
+    """Shared document rows (PT's pseudo-documents, PTModel.hpp:13-24): document
+    d counts in row row_of[d] of R rows of n_dk; a sweep samples each row's
+    documents one after another (ascending index) with the row live, the rows
+    ordered and grouped as documents are (by their total length).  ll_docs and
+    the alpha optimiser run over the rows."""
+
+    def __init__(self, corpus, K, alpha, eta, seed, row_of, R, z0=None):
+        self.row_of = np.ascontiguousarray(row_of, dtype=np.uint32)
+        self.R = int(R)
+        super().__init__(corpus, K, alpha, eta, seed, z0=z0)
+
+    def set_rows(self, row_of, R):
+        self.row_of = np.ascontiguousarray(row_of, dtype=np.uint32)
+        self.R = int(R)
+        self.recount()
+
+    def recount(self):
+        super().recount()              # n_kw, n_k (and per-document rows, replaced below)
+        c = self.c
+        self.ndk = np.zeros((self.R, self.K), dtype=np.int32)
+        ok = c.words < c.V
+        doc = np.repeat(np.arange(c.D), np.diff(c.doc_off.astype(np.int64)))
+        np.add.at(self.ndk, (self.row_of[doc[ok]].astype(np.int64), self.z[ok].astype(np.int64)), 1)
+        self.row_len = np.zeros(self.R, dtype=np.int32)
+        np.add.at(self.row_len, self.row_of.astype(np.int64), c.doc_len)
+        lens = np.diff(c.doc_off.astype(np.int64))
+        self.unit_len = np.zeros(self.R, dtype=np.int64)
+        np.add.at(self.unit_len, self.row_of.astype(np.int64), lens)
+        self.unit_docs = np.argsort(self.row_of, kind="stable").astype(np.uint32)
+        self.unit_off = np.concatenate([[0], np.cumsum(np.bincount(self.row_of, minlength=self.R))]).astype(np.uint64)
+
+    def group_bounds(self, groups):
+        order = np.argsort(-self.unit_len, kind="stable").astype(np.uint64)
+        total = int(self.unit_len.sum())
+        prefix = np.concatenate([[0], np.cumsum(self.unit_len[order.astype(np.int64)])[:-1]]) if self.R else \
+            np.zeros(0)
+        bounds = [0] + [int(np.sum(prefix * groups < g * total)) for g in range(1, groups)] + [self.R]
+        return order, bounds
+
+    def doc_live_sweeps(self, iters, start_step=0, groups=1):
+        c = self.c
+        order, b = self.group_bounds(groups)
+        parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
+        for it in range(iters):
+            for part in parts:
+                if len(part) == 0:
+                    continue
+                nkw2 = self.nkw.copy()
+                nk2 = self.nk.copy()
+                sp = SweepSpec(K=self.K, V=c.V, alpha=self.alpha.ctypes.data, eta=self.eta, seed=self.seed,
+                               iter=start_step + it, doc_off=c.doc_off.ctypes.data, words=c.words.ctypes.data,
+                               ndk=self.ndk.ctypes.data, nkw=self.nkw.ctypes.data, nk=self.nk.ctypes.data,
+                               nkw_next=nkw2.ctypes.data, nk_next=nk2.ctypes.data, z=self.z.ctypes.data,
+                               split_len=0, slices=SPLIT_SLICES, step=SPLIT_STEP,
+                               unit_off=self.unit_off.ctypes.data, unit_docs=self.unit_docs.ctypes.data)
+                lib.orc_sweep_docs(C.byref(sp), _ptr(part), len(part))
+                self.nkw = nkw2
+                self.nk = nk2
+
+    def optimize_alpha(self):
+        lib.orc_optimize_alpha(self.R, self.K, _ptr(self.ndk), _ptr(self.row_len), _ptr(self.alpha))
+
+    def ll_f64(self):
+        a = lib.orc_ll_docs_f64(self.R, self.K, _ptr(self.ndk), _ptr(self.row_len), _ptr(self.alpha))
+        b = lib.orc_ll_rest_f64(self.K, self.c.V, _ptr(self.nkw), _ptr(self.nk), self.eta)
         return a, b
 
 

@@ -1249,6 +1249,14 @@ void orc_sweep_docs(const orc_sweep_spec* sp, const uint64_t* docs, uint64_t n_d
         c.d = d;
         c.al = sp->arow ? sp->alpha_rows + (size_t)sp->arow[d] * K : sp->alpha;
         int32_t* row = sp->ndk + d * K;
+        if (sp->unit_off) {              /* a shared row: its documents in order, the row live */
+            for (uint32_t k = 0; k < K; ++k) A[k] = sweep_afold(&c, row[k], k);
+            for (uint64_t u = sp->unit_off[d]; u < sp->unit_off[d + 1]; ++u) {
+                const uint64_t dd = sp->unit_docs[u];
+                sweep_tokens(&c, sp->doc_off[dd], sp->doc_off[dd + 1], row, A, NULL);
+            }
+            continue;
+        }
         const uint64_t b = sp->doc_off[d], e = sp->doc_off[d + 1], L = e - b;
         if (!sp->split_len || L < sp->split_len || sp->slices < 2) {
             for (uint32_t k = 0; k < K; ++k) A[k] = sweep_afold(&c, row[k], k);

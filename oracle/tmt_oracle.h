@@ -248,6 +248,10 @@ typedef struct {
     int32_t* ndk; const int32_t* nkw; const int32_t* nk;
     int32_t* nkw_next; int32_t* nk_next; uint16_t* z;
     uint64_t split_len; uint32_t slices, step;   /* split_len 0: no document is split */
+    /* shared rows (PT's pseudo-documents): docs[] then lists rows; row r's
+     * documents are unit_docs[unit_off[r] .. unit_off[r+1]), sampled one after
+     * another with the row live; NULL: every document is its own row */
+    const uint64_t* unit_off; const uint32_t* unit_docs;
 } orc_sweep_spec;
 /* the documents docs[0 .. n_docs) of one group (see tmt_oracle.c) */
 void orc_sweep_docs(const orc_sweep_spec* sp, const uint64_t* docs, uint64_t n_docs);

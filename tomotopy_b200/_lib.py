@@ -99,6 +99,7 @@ SIGNATURES = {
     "tmt_set_global_step": (C.c_int, [_H, C.c_uint64]),
     "tmt_set_seed": (C.c_int, [_H, C.c_uint64]),
     "tmt_set_graphs": (C.c_int, [_H, C.c_int32]),
+    "tmt_set_doc_rows": (C.c_int, [_H, C.c_uint64, _P]),
     "tmt_set_doc_split": (C.c_int, [_H, C.c_uint64, C.c_uint32]),
     "tmt_get_doc_split": (C.c_int, [_H, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tmt_get_sweep_variants": (C.c_int, [_H, _P, C.c_uint32, C.POINTER(C.c_uint32)]),

@@ -161,6 +161,31 @@ __global__ void k_counts(const uint64_t* __restrict__ doc_off, const uint32_t* _
     }
 }
 
+// n_dk and the valid-token counts per row from z: document d's tokens go to
+// row row_of[d] (PT's pseudo-documents), or to row d when row_of is NULL.
+// ndk and len must be zero on entry.
+__global__ void k_counts_rows(const uint64_t* __restrict__ doc_off, const uint32_t* __restrict__ words,
+                              const uint16_t* __restrict__ z, uint64_t D, uint32_t K, uint32_t V,
+                              const uint32_t* __restrict__ row_of, int32_t* __restrict__ ndk,
+                              int32_t* __restrict__ len)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t d = warp; d < D; d += nwarps) {
+        const uint64_t r = row_of ? row_of[d] : d;
+        int cnt = 0;
+        for (uint64_t i = doc_off[d] + lane; i < doc_off[d + 1]; i += 32) {
+            if (words[i] >= V) continue;
+            atomicAdd(&ndk[r * K + z[i]], 1);
+            ++cnt;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
+        if (lane == 0 && cnt) atomicAdd(&len[r], cnt);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // the training sweep
 // ---------------------------------------------------------------------------
@@ -409,6 +434,12 @@ struct SweepArgs {
     uint32_t n_long;
     uint32_t split_step;     // positions per slice between merges
     uint32_t* long_counter;  // phase 1's document counter
+    // shared rows (PT's pseudo-documents, tmt_set_doc_rows): doc_order holds
+    // rows; row r's documents are unit_docs[unit_off[r] .. unit_off[r+1]),
+    // sampled one after another with the row live.  NULL: every document is
+    // its own row.
+    const uint64_t* unit_off;
+    const uint32_t* unit_docs;
 };
 
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
@@ -794,7 +825,8 @@ k_sweep_doc(SweepArgs a)
         }
     }
 
-    // Phase 2: the other documents, one per warp, in order with the row live.
+    // Phase 2: the other documents (or shared rows), one per warp, in order
+    // with the row live.
     for (;;) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(a.doc_counter, 1u);
@@ -815,7 +847,14 @@ k_sweep_doc(SweepArgs a)
             rowf[k] = f;
         }
         __syncwarp();
-        run_tokens(a.doc_off[d], a.doc_off[d + 1], rowi, rowf, nullptr);
+        if (a.unit_off) {
+            for (uint64_t u = a.unit_off[d]; u < a.unit_off[d + 1]; ++u) {
+                const uint64_t dd = a.unit_docs[u];
+                run_tokens(a.doc_off[dd], a.doc_off[dd + 1], rowi, rowf, nullptr);
+            }
+        } else {
+            run_tokens(a.doc_off[d], a.doc_off[d + 1], rowi, rowf, nullptr);
+        }
         __syncwarp();
         if (a.rowi_smem)
             for (int k = lane; k < K; k += 32) grow[k] = rowi[k];
@@ -1138,6 +1177,14 @@ struct tmt_handle {
     std::vector<uint64_t> order_len;
     uint64_t split_min = 0;          // 0: the rule (split_len_of); >= 2^32 - 1: never
     uint32_t split_step = kSplitStep;
+    // shared rows (tmt_set_doc_rows: PT's pseudo-documents): n_rows rows of
+    // n_dk replace the per-document rows; 0: one row per document
+    uint64_t n_rows = 0;
+    uint64_t row_cap = 0;            // rows the n_dk, length and order buffers hold
+    uint64_t unit_cap = 0;           // rows d_unit_off holds
+    uint64_t* d_unit_off = nullptr;  // n_rows + 1
+    uint32_t* d_unit_docs = nullptr; // D
+    uint32_t* d_row_of = nullptr;    // D
     // a corpus sharded across GPUs (tmt_upload_shard); world == 1: this GPU holds all of it
     uint32_t rank = 0, world = 1;
     uint64_t D_global = 0, tok_offset = 0;
@@ -1630,7 +1677,9 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.arow = h->d_arow;
     a.mask = h->d_mask;
     a.mw = (h->cfg.K + 31) / 32;
-    a.n_long = h->weighted ? 0 : h->group_nlong[g];
+    a.n_long = (h->weighted || h->n_rows) ? 0 : h->group_nlong[g];
+    a.unit_off = h->n_rows ? h->d_unit_off : nullptr;
+    a.unit_docs = h->n_rows ? h->d_unit_docs : nullptr;
     a.split_step = h->split_step;
     a.long_counter = h->d_counter + 1;
     return a;
@@ -1837,8 +1886,8 @@ void do_optimize(tmt_handle* h)
                                                       (const float*)h->d_doc_wlen, h->d_asum, h->d_part_nom,
                                                       h->d_part_den);
         else
-            k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_alpha, h->d_doc_len, h->d_asum,
-                                                      h->d_part_nom, h->d_part_den);
+            k_alpha_sums<<<grid, 256, 0, h->stream>>>(h->d_ndk, h->n_rows ? h->n_rows : h->D, K, h->d_alpha,
+                                                      h->d_doc_len, h->d_asum, h->d_part_nom, h->d_part_den);
         launch_check(h);
         uint32_t nparts = h->n_apart;
         const double* nom = h->d_part_nom;
@@ -1853,8 +1902,8 @@ void do_optimize(tmt_handle* h)
             nom = h->d_alpha_fold;
             den = h->d_alpha_fold + K;
         }
-        k_alpha_update<<<1, 1024, 0, h->stream>>>(nom, den, nparts, K, h->D_global, h->d_alpha, h->d_asum,
-                                                  h->d_dg_points);
+        k_alpha_update<<<1, 1024, 0, h->stream>>>(nom, den, nparts, K, h->n_rows ? h->n_rows : h->D_global,
+                                                  h->d_alpha, h->d_asum, h->d_dg_points);
         launch_check(h);
     }
 }
@@ -1877,7 +1926,8 @@ void do_ll(tmt_handle* h, double* d_out)
         k_ll_final<<<1, 256, 0, h->stream>>>(h->d_partials, h->n_partials, reinterpret_cast<const float*>(h->d_nk[0]),
                                              K, veta, d_out, h->d_esum);
     } else {
-        k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->D, K, h->d_lg_alpha, h->d_alpha,
+        k_ll_partials<<<h->n_partials, 256, 0, h->stream>>>(h->d_ndk, h->n_rows ? h->n_rows : h->D, K,
+                                                            h->d_lg_alpha, h->d_alpha,
                                                             h->d_doc_len, h->d_asum_ll,
                                                             h->d_nkw[h->cur], h->cfg.V, eta, std::lgamma(eta),
                                                             h->d_partials, h->prior_args(), h->d_alpha_rows,
@@ -1959,7 +2009,7 @@ void update_split(tmt_handle* h)
     if (h->group_bounds.empty()) return;
     const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
     h->group_nlong.assign(G, 0);
-    if (h->weighted) return;
+    if (h->weighted || h->n_rows) return;
     for (uint32_t g = 0; g < G; ++g) {
         const uint64_t sl = split_len_of(h->group_tokens[g], h->cfg.K, h->split_min);
         if (!sl) continue;
@@ -2067,6 +2117,12 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             h->ar_user = nullptr;
         }
         h->weighted = weights != nullptr;
+        h->n_rows = 0;
+        h->row_cap = D;
+        h->unit_cap = 0;
+        h->d_unit_off = nullptr;
+        h->d_unit_docs = nullptr;
+        h->d_row_of = nullptr;
         h->tok_offset = plan.tok_offset;
         h->group_bounds = plan.bounds;
         h->gbounds = plan.gbounds;
@@ -2497,7 +2553,7 @@ tmt_status tmt_download_doc_topic(tmt_handle* h, int32_t* n_dk)
         if (!h->uploaded) throw StateError("no corpus uploaded");
         if (!n_dk) throw ArgError("n_dk is NULL");
         if (h->weighted) throw StateError("the counts are weighted (float): read them with tmt_download_counts_f32");
-        d2h(h, n_dk, h->d_ndk, h->D * (uint64_t)h->cfg.K * sizeof(int32_t));
+        d2h(h, n_dk, h->d_ndk, (h->n_rows ? h->n_rows : h->D) * (uint64_t)h->cfg.K * sizeof(int32_t));
     });
 }
 
@@ -2521,6 +2577,7 @@ tmt_status tmt_set_doc_topic_mask(tmt_handle* h, const uint32_t* mask_bits)
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("set_doc_topic_mask before the corpus was uploaded");
         if (h->world > 1) throw ArgError("per-document masks on a corpus sharded across GPUs are not supported");
+        if (h->n_rows && mask_bits) throw StateError("per-document masks and shared rows do not combine");
         h->drop_graphs();
         if (!mask_bits) { h->d_mask = nullptr; return; }
         const uint64_t mw = (h->cfg.K + 31) / 32;
@@ -2536,6 +2593,7 @@ tmt_status tmt_set_doc_alpha(tmt_handle* h, uint32_t M, const float* alpha_rows,
     return guarded(h, [&] {
         if (!h->uploaded) throw StateError("set_doc_alpha before the corpus was uploaded");
         if (h->world > 1) throw ArgError("per-document alphas on a corpus sharded across GPUs are not supported");
+        if (h->n_rows && alpha_rows) throw StateError("per-document alphas and shared rows do not combine");
         h->drop_graphs();
         if (!alpha_rows) { h->d_arow = nullptr; h->d_alpha_rows = nullptr; h->d_row_asum = nullptr; return; }
         const uint32_t K = h->cfg.K;
@@ -2646,6 +2704,90 @@ tmt_status tmt_set_doc_split(tmt_handle* h, uint64_t min_tokens, uint32_t step)
         h->split_step = step ? step : kSplitStep;
         h->drop_graphs();          // the split is an argument of the captured launches
         update_split(h);
+    });
+}
+
+tmt_status tmt_set_doc_rows(tmt_handle* h, uint64_t R, const uint32_t* row_of_doc)
+{
+    if (!h) return TMT_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->uploaded) throw StateError("set_doc_rows before the corpus was uploaded");
+        if (h->world > 1) throw ArgError("shared rows on a corpus sharded across GPUs are not supported");
+        if (h->weighted) throw StateError("shared rows take integer counts; this corpus has weighted counts");
+        if (row_of_doc && (h->d_mask || h->d_arow))
+            throw StateError("shared rows do not combine with per-document masks or alphas");
+        const uint64_t D = h->D;
+        const uint32_t K = h->cfg.K, V = h->cfg.V;
+        if (row_of_doc) {
+            if (R == 0 || R >= 0xFFFFFFFFull) throw ArgError("R must be in 1 .. 2^32 - 2");
+            for (uint64_t d = 0; d < D; ++d)
+                if (row_of_doc[d] >= R) throw ArgError("row_of_doc[" + std::to_string(d) + "] >= R");
+        }
+        h->drop_graphs();                 // the rows are arguments of the captured launches
+        std::vector<uint64_t> off(D + 1);
+        CK(cudaMemcpyAsync(off.data(), h->d_doc_off, (D + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const uint64_t rows = row_of_doc ? R : D;
+        if (rows > h->row_cap) {
+            h->d_ndk = h->dalloc<int32_t>(rows * K);
+            h->d_doc_len = h->dalloc<int32_t>(rows);
+            h->d_doc_order = h->dalloc<uint32_t>(rows);
+            h->row_cap = rows;
+        }
+        ShardPlan plan;
+        std::vector<uint64_t> lens;
+        if (row_of_doc) {
+            // row r's documents in ascending order (a counting sort on the row)
+            std::vector<uint64_t> unit_off(R + 1, 0);
+            lens.assign(R, 0);
+            for (uint64_t d = 0; d < D; ++d) {
+                ++unit_off[row_of_doc[d] + 1];
+                lens[row_of_doc[d]] += off[d + 1] - off[d];
+            }
+            for (uint64_t r = 0; r < R; ++r) unit_off[r + 1] += unit_off[r];
+            std::vector<uint32_t> docs(std::max<uint64_t>(D, 1));
+            std::vector<uint64_t> fill(unit_off.begin(), unit_off.end() - 1);
+            for (uint64_t d = 0; d < D; ++d) docs[fill[row_of_doc[d]]++] = (uint32_t)d;
+            if (!h->d_unit_docs) {
+                h->d_unit_docs = h->dalloc<uint32_t>(std::max<uint64_t>(D, 1));
+                h->d_row_of = h->dalloc<uint32_t>(std::max<uint64_t>(D, 1));
+            }
+            if (R > h->unit_cap) {
+                h->d_unit_off = h->dalloc<uint64_t>(R + 1);
+                h->unit_cap = R;
+            }
+            CK(cudaMemcpyAsync(h->d_unit_off, unit_off.data(), (R + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                               h->stream));
+            if (D) {
+                CK(cudaMemcpyAsync(h->d_unit_docs, docs.data(), D * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                   h->stream));
+                CK(cudaMemcpyAsync(h->d_row_of, row_of_doc, D * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+            }
+        } else {
+            lens.resize(D);
+            for (uint64_t d = 0; d < D; ++d) lens[d] = off[d + 1] - off[d];
+        }
+        plan = plan_shard(lens.data(), rows, h->groups, 0, rows);
+        h->order_len.resize(rows);
+        for (uint64_t q = 0; q < rows; ++q) h->order_len[q] = lens[plan.order[q]];
+        h->n_rows = row_of_doc ? R : 0;
+        h->group_bounds = plan.bounds;
+        h->gbounds = plan.gbounds;
+        h->group_tokens = plan.gtokens;
+        update_split(h);
+        if (rows)
+            CK(cudaMemcpyAsync(h->d_doc_order, plan.order.data(), rows * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               h->stream));
+        // the rows' counts and lengths, recounted from z
+        CK(cudaMemsetAsync(h->d_ndk, 0, rows * (uint64_t)K * sizeof(int32_t), h->stream));
+        CK(cudaMemsetAsync(h->d_doc_len, 0, rows * sizeof(int32_t), h->stream));
+        if (D) {
+            const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)h->num_sms * 16, (D * 32 + 255) / 256);
+            k_counts_rows<<<grid, 256, 0, h->stream>>>(h->d_doc_off, h->d_words, h->d_z, D, K, V,
+                                                       row_of_doc ? h->d_row_of : nullptr, h->d_ndk, h->d_doc_len);
+            launch_check(h);
+        }
+        CK(cudaStreamSynchronize(h->stream));
     });
 }
 

@@ -51,6 +51,7 @@ class Engine:
         weights (TermWeight IDF / PMI) are given."""
         self._doc_off = np.ascontiguousarray(doc_off, dtype=np.uint64)
         self._words = np.ascontiguousarray(words, dtype=np.uint32)
+        self._n_rows = None
         zz = np.ascontiguousarray(z0, dtype=np.uint16) if z0 is not None else None
         self.D = len(self._doc_off) - 1
         self.n_all = int(self._doc_off[-1]) if self.D >= 0 else 0
@@ -107,6 +108,20 @@ class Engine:
         out = np.zeros(max(n.value, 1), dtype=np.int32)
         check(lib.tmt_get_sweep_variants(self.h, _p(out), n.value, C.byref(n)), self.h)
         return out[:n.value].tolist()
+
+    def set_doc_rows(self, row_of_doc, R=None):
+        """tmt_set_doc_rows: document d counts in row row_of_doc[d] of R shared
+        rows (PT's pseudo-documents); None returns to one row per document."""
+        if row_of_doc is None:
+            check(lib.tmt_set_doc_rows(self.h, 0, None), self.h)
+            self._n_rows = None
+            return
+        rows = np.ascontiguousarray(row_of_doc, dtype=np.uint32)
+        if len(rows) != self.D:
+            raise ValueError("row_of_doc needs one entry per document")
+        R = int(rows.max()) + 1 if R is None else int(R)
+        check(lib.tmt_set_doc_rows(self.h, R, _p(rows)), self.h)
+        self._n_rows = R
 
     def set_doc_split(self, min_tokens=0, step=0):
         """tmt_set_doc_split: documents of at least min_tokens tokens are
@@ -175,14 +190,15 @@ class Engine:
         return z[:self.n_all], nkw, nk, alpha
 
     def doc_topic(self):
-        """n_dk [D x K]; float when weighted."""
+        """n_dk [D x K] (the R shared rows after set_doc_rows); float when weighted."""
         if getattr(self, "weighted", False):
             ndk = np.zeros((max(self.D, 1), self.K), dtype=np.float32)
             check(lib.tmt_download_counts_f32(self.h, _p(ndk), None, None, None), self.h)
-        else:
-            ndk = np.zeros((max(self.D, 1), self.K), dtype=np.int32)
-            check(lib.tmt_download_doc_topic(self.h, _p(ndk)), self.h)
-        return ndk[:self.D]
+            return ndk[:self.D]
+        n = getattr(self, "_n_rows", None) or self.D
+        ndk = np.zeros((max(n, 1), self.K), dtype=np.int32)
+        check(lib.tmt_download_doc_topic(self.h, _p(ndk)), self.h)
+        return ndk[:n]
 
     def doc_weight_sums(self):
         """Per-document weight sums of a weighted corpus."""
