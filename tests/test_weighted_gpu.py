@@ -55,8 +55,12 @@ def test_weighted_sweeps_bitexact(kind, K, groups):
 
 
 def test_unit_weights_equal_integer_counts():
+    """With every weight 1 the weighted sweep is the integer sweep -- the
+    integer sweep with long documents sampled in order, as weighted counts
+    always are (splitting applies to integer counts only)."""
     c = corpus(seed=4)
     a = T.Engine(40, c.V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
+    a.set_doc_split(2 ** 32 - 1)
     a.upload(c.doc_off, c.words)
     b = T.Engine(40, c.V, alpha=0.1, eta=0.01, seed=3, optim_interval=0)
     b.upload(c.doc_off, c.words, weights=np.ones(len(c.words), np.float32))
