@@ -657,10 +657,11 @@ k_sweep_doc(SweepArgs a)
                         // scan of scan_steps = ceil(log2(that)) steps gives the other lanes
                         // the values of the full scan, and the total sits in lane
                         // 2^scan_steps - 1
-                        const float x = hs_scan_n(s, lane, a.scan_steps);
+                        // (above 128 topics every lane holds topics: the five steps, unrolled)
+                        const float x = CH >= 2 ? hs_scan32(s, lane) : hs_scan_n(s, lane, a.scan_steps);
                         float E = __shfl_up_sync(FULL, x, 1);
                         if (lane == 0) E = 0.f;
-                        const float total = __shfl_sync(FULL, x, (1 << a.scan_steps) - 1);
+                        const float total = __shfl_sync(FULL, x, CH >= 2 ? 31 : (1 << a.scan_steps) - 1);
                         const float r = __fmul_rn(u, total);
                         const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
                         int znew = K - 1;
