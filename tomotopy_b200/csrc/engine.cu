@@ -47,6 +47,15 @@ namespace {
 using namespace tmtk;
 constexpr int kSweepWarps = 8;           // warps per sweep block
 
+// One Hillis-Steele step with the lane test folded into an fma: m is 1 for
+// lanes at or above `off`, else 0, and for the finite sums here fma(y, 1, x)
+// rounds exactly as x + y and fma(y, 0, x) is x -- the values of the usual
+// predicated add, in fewer instructions.
+__device__ __forceinline__ float hs_step(float x, int off, float m)
+{
+    return __fmaf_rn(__shfl_up_sync(FULL, x, off), m, x);
+}
+
 // Long documents: a document of at least split_len tokens (all ids counted)
 // is sampled by a whole block as kSweepWarps slices side by side, merging
 // their n_dk changes every split_step positions (k_sweep_doc, phase 1).  The
@@ -494,6 +503,20 @@ k_sweep_doc(SweepArgs a)
     }
     // blocks of four owned by this lane
     const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
+    float lm[5];                         // hs_step's lane masks
+#pragma unroll
+    for (int i = 0; i < 5; ++i) lm[i] = lane >= (1 << i) ? 1.f : 0.f;
+    auto scan32 = [&](float x) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) x = hs_step(x, 1 << i, lm[i]);
+        return x;
+    };
+    auto scan_n = [&](float x, int steps) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+            if (i < steps) x = hs_step(x, 1 << i, lm[i]);
+        return x;
+    };
     const float eta = a.eta, veta = a.veta;
     const uint32_t iter = a.iter_ptr ? *a.iter_ptr : a.iter;
 
@@ -600,21 +623,20 @@ k_sweep_doc(SweepArgs a)
                         // until the draw is made, so pass 1's chain leaves the own topic
                         // out exactly and its owner adds Ao * phi_own last: no
                         // subtract-and-add that could cancel when the own topic dominates its lane
-                        float Ao = 0.f;
+                        // (every lane forms the new count and Ao; lane 0 stores them)
+                        CT n_rm;
+                        if constexpr (WT) {
+                            n_rm = __fsub_rn(rowi[zo], wt);
+                            n_rm = n_rm > 0.f ? n_rm : 0.f;
+                        } else {
+                            n_rm = rowi[zo] - 1;
+                        }
+                        const float Ao = afold((float)n_rm, zo);
+                        __syncwarp();
                         if (lane == 0) {
-                            if constexpr (WT) {
-                                float n = __fsub_rn(rowi[zo], wt);
-                                n = n > 0.f ? n : 0.f;
-                                rowi[zo] = n;
-                                Ao = afold(n, zo);
-                            } else {
-                                const int n = rowi[zo] - 1;
-                                rowi[zo] = n;
-                                Ao = afold((float)n, zo);
-                            }
+                            rowi[zo] = n_rm;
                             rowf[zo] = 0.f;
                         }
-                        Ao = __shfl_sync(FULL, Ao, 0);
                         __syncwarp();
                         // pass 1: fma chain over this lane's topics
                         float s = 0.f;
@@ -658,9 +680,8 @@ k_sweep_doc(SweepArgs a)
                         // the values of the full scan, and the total sits in lane
                         // 2^scan_steps - 1
                         // (above 128 topics every lane holds topics: the five steps, unrolled)
-                        const float x = CH >= 2 ? hs_scan32(s, lane) : hs_scan_n(s, lane, a.scan_steps);
-                        float E = __shfl_up_sync(FULL, x, 1);
-                        if (lane == 0) E = 0.f;
+                        const float x = CH >= 2 ? scan32(s) : scan_n(s, a.scan_steps);
+                        const float E = __fmul_rn(__shfl_up_sync(FULL, x, 1), lm[0]);   // 0 in lane 0
                         const float total = __shfl_sync(FULL, x, CH >= 2 ? 31 : (1 << a.scan_steps) - 1);
                         const float r = __fmul_rn(u, total);
                         const unsigned m = __ballot_sync(FULL, nch > 0 && r < __fadd_rn(E, s));
@@ -714,8 +735,11 @@ k_sweep_doc(SweepArgs a)
                                     const int t = mm + lane;
                                     const int k = 128 * (t >> 2) + 4 * h + (t & 3);
                                     float x2 = 0.f;
-                                    if (t < nh) x2 = k == zo ? __fmul_rn(Ao, phi_own) : __fmul_rn(rowf[k], __ldg(ph + k));
-                                    x2 = hs_scan_n(x2, lane, kSteps2);
+                                    // rowf[zo] reads 0 until the draw: fma(sel, phi_own, 0 * phi) is
+                                    // Ao * phi_own at zo and fma(0, phi_own, p) == p elsewhere
+                                    if (t < nh)
+                                        x2 = __fmaf_rn(k == zo ? Ao : 0.f, phi_own, __fmul_rn(rowf[k], __ldg(ph + k)));
+                                    x2 = scan_n(x2, kSteps2);
                                     const unsigned mb =
                                         __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
                                     if (mb) { found = mm + __ffs(mb) - 1; break; }
@@ -724,12 +748,17 @@ k_sweep_doc(SweepArgs a)
                             }
                             znew = 128 * (found >> 2) + 4 * h + (found & 3);
                         }
+                        // the new topic's count: every lane forms it, lane 0 stores
+                        CT n_add;
+                        if constexpr (WT) n_add = __fadd_rn(rowi[znew], wt);
+                        else n_add = rowi[znew] + 1;
+                        const float A_add = afold((float)n_add, znew);
+                        __syncwarp();
                         if (lane == 0) {
                             rowf[zo] = Ao;            // the own topic's slot back (znew's update follows)
+                            rowi[znew] = n_add;
+                            rowf[znew] = A_add;
                             if constexpr (WT) {
-                                const float n = __fadd_rn(rowi[znew], wt);
-                                rowi[znew] = n;
-                                rowf[znew] = afold(n, znew);
                                 if (znew != zo) {
                                     const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(wt, 16777216.f));
                                     unsigned long long* dw = reinterpret_cast<unsigned long long*>(a.dkw) + (uint64_t)v * K;
@@ -738,9 +767,6 @@ k_sweep_doc(SweepArgs a)
                                     // n_k's deltas are the column sums of these (k_dk_sum)
                                 }
                             } else {
-                                const int n = rowi[znew] + 1;
-                                rowi[znew] = n;
-                                rowf[znew] = afold((float)n, znew);
                                 if (znew != zo) {
                                     atomicSub(&a.nkw_next[(uint64_t)v * K + zo], 1);
                                     atomicAdd(&a.nkw_next[(uint64_t)v * K + znew], 1);
