@@ -470,19 +470,12 @@ struct SweepArgs {
 //       Utils.hpp:132-155) and the count deltas are integers in units of 2^-24.
 //   SPLIT: the launch's first n_long documents are split (phase 1); the
 //       kernels without it carry no phase-1 code.
-//   COL: where the current word's table column lives across tokens of the
-//       same word: 1 = in registers (4*CH per lane); 2 = in a per-warp
-//       shared-memory buffer, refilled when the word changes (CH >= 4: frees
-//       the registers, whose upkeep through the token loop costs ~90
-//       instructions per token at CH = 8, while every read still hits);
-//       0 = none, pass 1 reads the column from L1 / L2 every token (CH >= 4).
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, int COL = 1>
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
 __global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
     using CT = typename std::conditional<WT, float, int>::type;
-    static_assert(COL == 1 || (CH >= 4 && !PF && !SPLIT), "the column outside registers is built for 4+ blocks per lane");
-    constexpr int CHR = CH > 0 ? (COL == 1 ? CH : 1) : 1;
+    constexpr int CHR = CH > 0 ? CH : 1;
     extern __shared__ __align__(16) int smem[];
     const int K = (int)a.K;
     const int KP = (int)round4(a.K);
@@ -499,8 +492,6 @@ k_sweep_doc(SweepArgs a)
     constexpr bool split = SPLIT && !WT;
     int* s_C = s_rowi + ((a.rowi_smem || split) ? nwarps * KP : 0);
     int* s_dlt = s_C + KP;
-    // COL == 2: this warp's copy of the current word's table column
-    float* mycol = reinterpret_cast<float*>(s_C + (split ? 2 * KP : 0)) + warp * KP;
     __shared__ uint32_t s_q;
     if (dnk_smem) {
         for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
@@ -532,18 +523,10 @@ k_sweep_doc(SweepArgs a)
     // registers (the table is the group's snapshot, so it cannot change).
     auto load_col = [&](uint32_t v, float4 (&pv)[CHR]) {
         const float* ph = a.phi + (uint64_t)v * KP;
-        if constexpr (CH > 0 && COL == 1) {
+        if constexpr (CH > 0) {
 #pragma unroll
             for (int jj = 0; jj < CHR; ++jj)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
-        } else if constexpr (CH > 0 && COL == 2) {
-            // each lane copies its own blocks (pass 1 reads only those); pass 2
-            // reads other lanes' entries after the removal's warp barriers
-#pragma unroll
-            for (int jj = 0; jj < CH; ++jj)
-                if (jj < nch)
-                    *reinterpret_cast<float4*>(mycol + 128 * jj + 4 * lane) =
-                        __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
     };
     auto load_word = [&](uint32_t v, int zo, float w, float& phio) {
@@ -653,21 +636,7 @@ k_sweep_doc(SweepArgs a)
                         __syncwarp();
                         // pass 1: fma chain over this lane's topics
                         float s = 0.f;
-                        if (CH > 0 && COL != 1) {
-    #pragma unroll
-                            for (int jj = 0; jj < CH; ++jj) {
-                                if (jj < nch) {
-                                    const float4 A4 = *reinterpret_cast<const float4*>(rowf + 128 * jj + 4 * lane);
-                                    const float4 P4 = COL == 2
-                                        ? *reinterpret_cast<const float4*>(mycol + 128 * jj + 4 * lane)
-                                        : __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
-                                    s = __fmaf_rn(A4.x, P4.x, s);
-                                    s = __fmaf_rn(A4.y, P4.y, s);
-                                    s = __fmaf_rn(A4.z, P4.z, s);
-                                    s = __fmaf_rn(A4.w, P4.w, s);
-                                }
-                            }
-                        } else if (CH > 0) {
+                        if (CH > 0) {
     #pragma unroll
                             for (int jj = 0; jj < CHR; ++jj) {
                                 if (jj < nch) {
@@ -753,8 +722,7 @@ k_sweep_doc(SweepArgs a)
                                     // rowf[zo] reads 0 until the draw: fma(sel, phi_own, 0 * phi) is
                                     // Ao * phi_own at zo and fma(0, phi_own, p) == p elsewhere
                                     if (t < nh)
-                                        x2 = __fmaf_rn(k == zo ? Ao : 0.f, phi_own,
-                                                       __fmul_rn(rowf[k], COL == 2 ? mycol[k] : __ldg(ph + k)));
+                                        x2 = __fmaf_rn(k == zo ? Ao : 0.f, phi_own, __fmul_rn(rowf[k], __ldg(ph + k)));
                                     x2 = scan_n(x2, kSteps2);
                                     const unsigned mb =
                                         __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
@@ -1551,9 +1519,7 @@ struct SweepShape {
 // private row in shared memory whatever the variant, and the block the
 // document's row and the step's merged changes (K <= kSplitMaxK keeps the
 // block at kSweepWarps warps)
-// smem_col: a per-warp copy of the current word's table column (variant 3)
-SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool split = false,
-                       bool smem_col = false)
+SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool split = false)
 {
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
@@ -1562,7 +1528,7 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     // (k_dk_sum): 64-bit shared-memory atomics per token cost ~17 ms a sweep
     s.dnk_smem = !weighted && K <= 16384u;
     s.rowi_smem = K <= 8192 && !rowi_global;
-    const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0) + (smem_col ? 4 * KP : 0);
+    const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0);
     const uint32_t fixed = (s.dnk_smem ? 4 * KP : 0) + (split ? 8 * KP : 0);
     uint32_t w = (budget - fixed) / per_warp;
     s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
@@ -1570,10 +1536,10 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     return s;
 }
 
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, int COL = 1>
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT, COL>;
+    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT>;
     // attribute and occupancy once per kernel and shared-memory size (the
     // shapes depend on K and on whether the launch splits documents), so a
     // captured sweep makes no such call; the attribute allows the largest shape
@@ -1600,16 +1566,12 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
 // topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
-// document row in global memory, 4 blocks/SM; 3 (4 to 16 blocks of four per
-// lane) = variant 2 with the word's column in shared memory instead of
-// registers, kSmemColMinB blocks/SM.
-constexpr int kSmemColMinB = 3;
-
+// document row in global memory, 4 blocks/SM.  (Measured and dropped at
+// K = 1000: the word's column read from L1 every token, 6 blocks/SM, and a
+// per-warp shared-memory copy of it -- fewer instructions, slower sweeps.)
 int sweep_variants_for(uint32_t K)
 {
-    const uint32_t ch = (round4(K) + 127) / 128;
-    if (ch > 32) return 1;
-    return ch >= 4 && ch <= 16 ? 4 : 3;
+    return (round4(K) + 127) / 128 > 32 ? 1 : 3;
 }
 
 template <int CH, bool WT>
@@ -1623,12 +1585,6 @@ void launch_sweep_ch(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, in
         else if (variant == 1) launch_sweep_t<CH, 3, false, WT, kSplit>(h, a, sh);
         else launch_sweep_t<CH, 2, kPrefetch, WT, kSplit>(h, a, sh);
         return;
-    }
-    if constexpr (CH >= 4 && CH <= 16) {
-        if (variant == 3) {
-            launch_sweep_t<CH, kSmemColMinB, false, WT, false, 2>(h, a, sh);
-            return;
-        }
     }
     if (variant >= 2) launch_sweep_t<CH, 4, false, WT>(h, a, sh);
     else if (variant == 1) launch_sweep_t<CH, 3, false, WT>(h, a, sh);
@@ -1653,7 +1609,7 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const uint32_t ch = (KP + 127) / 128;
     const bool wt = a.wt != nullptr;
     const bool split = !wt && a.n_long > 0;
-    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, split, variant == 3 && !split && ch >= 4 && ch <= 16);
+    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, split);
     if (!wt && a.n_long > 0 && sh.warps != (uint32_t)kSweepWarps)
         throw CudaError("split documents need a block of " + std::to_string(kSweepWarps) + " warps");
     SweepArgs b = a;
