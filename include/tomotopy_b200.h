@@ -249,8 +249,9 @@ tmt_status tmt_set_optim(tmt_handle* h, uint32_t optim_interval, uint32_t burn_i
  * by vocabulary range; its sorted tokens make each slice a vocabulary range).
  * Without it one warp samples a document in order and the document's length
  * bounds its group's time.  Default (min_tokens = 0): per document group,
- * split_len = max(256, ceil(2 * group tokens / 4096)), for integer counts
- * with K <= 2048; min_tokens >= 2^32 - 1: never; step 0: 16.  The split
+ * split_len = max(8 * 7 * step, ceil(group tokens / 4096)) -- a split
+ * document is at least 8 times the 7 * step tokens a draw may see stale --
+ * for integer counts with K <= 512; min_tokens >= 2^32 - 1: never; step 0: 16.  The split
  * depends only on the corpus and these settings (never on timing or the
  * device), so results stay bit-reproducible. */
 tmt_status tmt_set_doc_split(tmt_handle* h, uint64_t min_tokens, uint32_t step);

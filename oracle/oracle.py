@@ -45,20 +45,20 @@ class SweepSpec(C.Structure):
 
 # The long-document split of the device sweep (engine.cu, split_len_of): a
 # document of at least split_len tokens is sampled as SPLIT_SLICES slices side
-# by side, merging their n_dk changes every SPLIT_STEP positions.  split_len
-# per document group: max(SPLIT_MIN, ceil(2 * group tokens / 4096)), for
-# integer counts with K <= SPLIT_MAX_K.
-SPLIT_SLICES, SPLIT_STEP, SPLIT_MIN, SPLIT_MAX_K = 8, 16, 256, 512
+# by side, merging their n_dk changes every `step` positions.  split_len per
+# document group: max(8 * (SPLIT_SLICES - 1) * step, ceil(group tokens / 4096)),
+# for integer counts with K <= SPLIT_MAX_K.
+SPLIT_SLICES, SPLIT_STEP, SPLIT_MAX_K = 8, 16, 512
 
 
-def split_len_of(group_tokens, K, min_len=0):
+def split_len_of(group_tokens, K, min_len=0, step=SPLIT_STEP):
     """The split threshold of a document group (0: no document is split).
     min_len: the engine's override (0: the rule; >= 2^32 - 1: never)."""
     if K > SPLIT_MAX_K or min_len >= 0xFFFFFFFF:
         return 0
     if min_len:
         return int(min_len)
-    return max(SPLIT_MIN, (2 * int(group_tokens) + 4095) // 4096)
+    return max(8 * (SPLIT_SLICES - 1) * int(step), (int(group_tokens) + 4095) // 4096)
 
 
 class SynthSpec(C.Structure):
@@ -374,7 +374,7 @@ class State:
         order, b = self.group_bounds(groups)
         lens = np.diff(c.doc_off.astype(np.int64))
         parts = [np.ascontiguousarray(order[b[g]:b[g + 1]]) for g in range(groups)]
-        splits = [split_len_of(lens[p.astype(np.int64)].sum(), self.K, split_min) for p in parts]
+        splits = [split_len_of(lens[p.astype(np.int64)].sum(), self.K, split_min, split_step) for p in parts]
         extra = self._spec_extra()
         for it in range(iters):
             for part, sl in zip(parts, splits):

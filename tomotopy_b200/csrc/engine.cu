@@ -58,21 +58,25 @@ __device__ __forceinline__ float hs_step(float x, int off, float m)
 
 // Long documents: a document of at least split_len tokens (all ids counted)
 // is sampled by a whole block as kSweepWarps slices side by side, merging
-// their n_dk changes every split_step positions (k_sweep_doc, phase 1).  The
-// threshold of a document group is max(kSplitMin, ceil(2 * tokens / 4096)) --
-// documents longer than twice the group's work per warp of a 4096-warp
-// machine -- so it depends on the corpus only, never on the device or on
-// timing; integer counts with K <= kSplitMaxK (the kernels with phase 1 are
-// built for up to 4 blocks of four topics per lane).  tmt_set_doc_split overrides the threshold and the step.
+// their n_dk changes every split_step positions (k_sweep_doc, phase 1).  A
+// token then sees up to (kSweepWarps - 1) * split_step of its document's
+// other tokens as of the step's start.  The threshold of a document group is
+// max(8 * (kSweepWarps - 1) * split_step, ceil(tokens / 4096)): documents
+// longer than the group's work per warp of a 4096-warp machine, and at least
+// 8 stale windows long (at 16 positions per step: 896 tokens; splitting from
+// 421 tokens measured 0.49% lower ll_per_word at the k=100 configuration
+// after 500 sweeps, from 842 tokens 0.03%).  It depends on the corpus only,
+// never on the device or on timing; integer counts with K <= kSplitMaxK (the
+// kernels with phase 1 are built for up to 4 blocks of four topics per lane).
+// tmt_set_doc_split overrides the threshold and the step.
 constexpr uint32_t kSplitStep = 16;
-constexpr uint64_t kSplitMin = 256;
 constexpr uint32_t kSplitMaxK = 512;
 
-uint64_t split_len_of(uint64_t group_tokens, uint32_t K, uint64_t min_len)
+uint64_t split_len_of(uint64_t group_tokens, uint32_t K, uint64_t min_len, uint32_t step)
 {
     if (K > kSplitMaxK || min_len >= 0xFFFFFFFFull) return 0;
     if (min_len) return min_len;
-    return std::max<uint64_t>(kSplitMin, (2 * group_tokens + 4095) / 4096);
+    return std::max<uint64_t>(8ull * (kSweepWarps - 1) * step, (group_tokens + 4095) / 4096);
 }
 
 
@@ -2014,7 +2018,7 @@ void update_split(tmt_handle* h)
     h->group_nlong.assign(G, 0);
     if (h->weighted || h->n_rows) return;
     for (uint32_t g = 0; g < G; ++g) {
-        const uint64_t sl = split_len_of(h->group_tokens[g], h->cfg.K, h->split_min);
+        const uint64_t sl = split_len_of(h->group_tokens[g], h->cfg.K, h->split_min, h->split_step);
         if (!sl) continue;
         uint32_t n = 0;
         for (uint64_t q = h->group_bounds[g]; q < h->group_bounds[g + 1] && h->order_len[q] >= sl; ++q) ++n;
