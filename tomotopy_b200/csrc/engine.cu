@@ -56,13 +56,6 @@ __device__ __forceinline__ float hs_step(float x, int off, float m)
     return __fmaf_rn(__shfl_up_sync(FULL, x, off), m, x);
 }
 
-// A hint that a global line is read soon: brings it into L1 (no register
-// written, no fault possible on the valid addresses it is given).
-__device__ __forceinline__ void prefetch_l1(const void* p)
-{
-    asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
-}
-
 // Long documents: a document of at least split_len tokens (all ids counted)
 // is sampled by a whole block as kSweepWarps slices side by side, merging
 // their n_dk changes every split_step positions (k_sweep_doc, phase 1).  A
@@ -630,19 +623,6 @@ k_sweep_doc(SweepArgs a)
                             new_col = vn != v;
                             if (new_col) load_col(vn, pvn);
                             load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, phion);
-                        } else if (!PF && CH >= 4 && jn >= 0) {
-                            // the next token's column and own-topic count into L1 while this
-                            // token is sampled: its loads at the end of this token then hit
-                            // (no registers held; results unchanged)
-                            const uint32_t vp = __shfl_sync(FULL, my_w, jn);
-                            const int zp = (int)__shfl_sync(FULL, my_z, jn);
-                            if (vp != v) {
-                                const float* pp = a.phi + (uint64_t)vp * KP;
-#pragma unroll
-                                for (int jj = 0; jj < CHR; ++jj)
-                                    if (jj < nch) prefetch_l1(pp + 128 * jj + 4 * lane);
-                            }
-                            if (lane == 0) prefetch_l1(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)vp * K + zp);
                         }
                         const float u = __shfl_sync(FULL, my_u, j);
                         const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
