@@ -453,6 +453,7 @@ struct SweepArgs {
     // its own row.
     const uint64_t* unit_off;
     const uint32_t* unit_docs;
+    uint64_t max_len;        // the launch's longest document (or shared row), all ids counted
 };
 
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
@@ -479,11 +480,16 @@ struct SweepArgs {
 //       shared memory present -- so the token loop carries none of those
 //       checks or pointers (~60 fewer warp instructions per token at K = 1000;
 //       the same arithmetic).
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false>
+//   ROW16: the document's count row lives in shared memory as 16-bit counts
+//       (the host guarantees every document of the launch is shorter than
+//       65,536 tokens), half the space of 32-bit rows: variant 2 keeps its 4
+//       blocks per SM without reading the row through L1.
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
 __global__ void __launch_bounds__(kSweepWarps * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
     static_assert(!(PLAIN && WT), "plain LDA has integer counts");
+    static_assert(!(ROW16 && (WT || SPLIT)), "16-bit rows: integer counts, no split documents");
     using CT = typename std::conditional<WT, float, int>::type;
     constexpr int CHR = CH > 0 ? CH : 1;
     extern __shared__ __align__(16) int smem[];
@@ -584,7 +590,7 @@ k_sweep_doc(SweepArgs a)
     // Samples the tokens [b, e) of the current document in order with the
     // document row rowi (counts) / rowf (A_k) live; with dlt != NULL every
     // change of the row is added to dlt as well.
-    auto run_tokens = [&](uint64_t b, uint64_t e, CT* rowi, float* rowf, int* dlt) {
+    auto run_tokens = [&](uint64_t b, uint64_t e, auto* rowi, float* rowf, int* dlt) {
             for (uint64_t base = b; base < e; base += 32) {
                 const uint64_t my_i = base + lane;
                 uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
@@ -633,7 +639,7 @@ k_sweep_doc(SweepArgs a)
                         // out exactly and its owner adds Ao * phi_own last: no
                         // subtract-and-add that could cancel when the own topic dominates its lane
                         // (every lane forms the new count and Ao; lane 0 stores them)
-                        CT n_rm;
+                        CT n_rm;             // (from a 16-bit row: promoted, and stored back below 65,536)
                         if constexpr (WT) {
                             n_rm = __fsub_rn(rowi[zo], wt);
                             n_rm = n_rm > 0.f ? n_rm : 0.f;
@@ -860,12 +866,14 @@ k_sweep_doc(SweepArgs a)
         const uint64_t d = a.doc_order[pos];
         set_doc(d);
         CT* grow = reinterpret_cast<CT*>(a.ndk) + d * (uint64_t)K;
-        CT* rowi = a.rowi_smem ? reinterpret_cast<CT*>(s_rowi + warp * KP) : grow;
+        using RT = typename std::conditional<ROW16, uint16_t, CT>::type;
+        const bool row_smem = ROW16 || a.rowi_smem;
+        RT* rowi = row_smem ? reinterpret_cast<RT*>(s_rowi) + warp * KP : reinterpret_cast<RT*>(grow);
         for (int k = lane; k < KP; k += 32) {
             float f = 0.f;
             if (k < K) {
                 const CT n = grow[k];
-                if (a.rowi_smem) rowi[k] = n;
+                if (row_smem) rowi[k] = (RT)n;
                 f = afold((float)n, k);
             }
             rowf[k] = f;
@@ -880,8 +888,8 @@ k_sweep_doc(SweepArgs a)
             run_tokens(a.doc_off[d], a.doc_off[d + 1], rowi, rowf, nullptr);
         }
         __syncwarp();
-        if (a.rowi_smem)
-            for (int k = lane; k < K; k += 32) grow[k] = rowi[k];
+        if (row_smem)
+            for (int k = lane; k < K; k += 32) grow[k] = (CT)rowi[k];
         __syncwarp();
     }
     if (dnk_smem) {
@@ -1524,6 +1532,7 @@ struct SweepShape {
     uint32_t warps;      // warps per block
     uint32_t smem;       // dynamic shared memory bytes
     uint32_t rowi_smem, dnk_smem;
+    uint32_t row16;      // the rows in shared memory as 16-bit counts (ROW16 kernels)
 };
 
 // rowi_global: the document's count row stays in global memory (L1-cached),
@@ -1532,7 +1541,8 @@ struct SweepShape {
 // private row in shared memory whatever the variant, and the block the
 // document's row and the step's merged changes (K <= kSplitMaxK keeps the
 // block at kSweepWarps warps)
-SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool split = false)
+// row16: with rowi_global, the rows stay in shared memory as 16-bit counts
+SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool split = false, bool row16 = false)
 {
     const uint32_t KP = round4(K);
     const uint32_t budget = 200 * 1024;
@@ -1541,7 +1551,8 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     // (k_dk_sum): 64-bit shared-memory atomics per token cost ~17 ms a sweep
     s.dnk_smem = !weighted && K <= 16384u;
     s.rowi_smem = K <= 8192 && !rowi_global;
-    const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0);
+    s.row16 = row16 && rowi_global && !weighted && !split && K <= 8192;
+    const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0) + (s.row16 ? 2 * KP : 0);
     const uint32_t fixed = (s.dnk_smem ? 4 * KP : 0) + (split ? 8 * KP : 0);
     uint32_t w = (budget - fixed) / per_warp;
     s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
@@ -1549,10 +1560,10 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     return s;
 }
 
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false>
+template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT, PLAIN>;
+    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT, PLAIN, ROW16>;
     // attribute and occupancy once per kernel and shared-memory size (the
     // shapes depend on K and on whether the launch splits documents), so a
     // captured sweep makes no such call; the attribute allows the largest shape
@@ -1599,7 +1610,12 @@ void launch_sweep_cp(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, in
         else launch_sweep_t<CH, 2, kPrefetch, WT, kSplit, PLAIN>(h, a, sh);
         return;
     }
-    if (variant >= 2) launch_sweep_t<CH, 4, false, WT, false, PLAIN>(h, a, sh);
+    if (variant >= 2) {
+        if constexpr (!WT) {
+            if (sh.row16) return launch_sweep_t<CH, 4, false, WT, false, PLAIN, true>(h, a, sh);
+        }
+        launch_sweep_t<CH, 4, false, WT, false, PLAIN>(h, a, sh);
+    }
     else if (variant == 1) launch_sweep_t<CH, 3, false, WT, false, PLAIN>(h, a, sh);
     else launch_sweep_t<CH, 2, kPrefetch, WT, false, PLAIN>(h, a, sh);
 }
@@ -1632,7 +1648,8 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const uint32_t ch = (KP + 127) / 128;
     const bool wt = a.wt != nullptr;
     const bool split = !wt && a.n_long > 0;
-    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, split);
+    // 16-bit rows when every document of the launch is shorter than 65,536 tokens
+    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, split, a.max_len < 65536);
     if (!wt && a.n_long > 0 && sh.warps != (uint32_t)kSweepWarps)
         throw CudaError("split documents need a block of " + std::to_string(kSweepWarps) + " warps");
     SweepArgs b = a;
@@ -1706,6 +1723,7 @@ SweepArgs sweep_args(tmt_handle* h, const int32_t* nkw, const int32_t* nk, int32
     a.mask = h->d_mask;
     a.mw = (h->cfg.K + 31) / 32;
     a.n_long = (h->weighted || h->n_rows) ? 0 : h->group_nlong[g];
+    a.max_len = pos_end > pos_begin ? h->order_len[pos_begin] : 0;    // longest first
     a.unit_off = h->n_rows ? h->d_unit_off : nullptr;
     a.unit_docs = h->n_rows ? h->d_unit_docs : nullptr;
     a.split_step = h->split_step;
