@@ -545,8 +545,9 @@ k_sweep_doc(SweepArgs a)
                 if (jj < nch) pv[jj] = __ldg(reinterpret_cast<const float4*>(ph + 128 * jj + 4 * lane));
         }
     };
-    auto load_word = [&](uint32_t v, int zo, float w, float& phio) {
-        const CT nkw_o = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)v * K + zo);
+    // nkw_o = n_kw[zo, v] and ri = rm1[zo] of the snapshot, loaded for a batch
+    // of 32 tokens at once (the table cannot change during the launch)
+    auto load_word = [&](uint32_t v, int zo, float w, CT nkw_o, float ri, float& phio) {
         float eo = eta;
         if (!PLAIN && a.pr.idx) {
             const float* pe = prior_col(a.pr, v, K);
@@ -562,7 +563,7 @@ k_sweep_doc(SweepArgs a)
         } else {
             float rinv;
             if (PLAIN || a.rm1) {
-                rinv = __ldg(a.rm1 + zo);
+                rinv = ri;
             } else {
                 const CT nk_o = __ldg(reinterpret_cast<const CT*>(a.nk) + zo);
                 rinv = __fdiv_rn(1.0f, __fadd_rn((float)(nk_o - 1), so()));
@@ -590,15 +591,24 @@ k_sweep_doc(SweepArgs a)
     // Samples the tokens [b, e) of the current document in order with the
     // document row rowi (counts) / rowf (A_k) live; with dlt != NULL every
     // change of the row is added to dlt as well.
+    const bool has_ri = !WT && (PLAIN || a.rm1 != nullptr);
     auto run_tokens = [&](uint64_t b, uint64_t e, auto* rowi, float* rowf, int* dlt) {
             for (uint64_t base = b; base < e; base += 32) {
                 const uint64_t my_i = base + lane;
                 uint32_t my_w = 0xFFFFFFFFu, my_z = 0xFFFF;
                 float my_u = 0.f, my_wt = 0.f;
+                // this lane's token's own-topic count and reciprocal in the snapshot:
+                // 32 independent loads per batch instead of one on every token's chain
+                CT my_nkw = CT(0);
+                float my_ri = 0.f;
                 if (my_i < e) {
                     my_w = a.words[my_i];
                     my_z = a.z[my_i];
                     if (WT) my_wt = a.wt[my_i];
+                    if (my_w < a.V) {
+                        my_nkw = __ldg(reinterpret_cast<const CT*>(a.nkw) + (uint64_t)my_w * K + my_z);
+                        if (has_ri) my_ri = __ldg(a.rm1 + my_z);
+                    }
                     const uint64_t gi = my_i + a.tok_offset;
                     my_u = tmt::u01(tmt::philox_u32((uint32_t)gi, (uint32_t)(gi >> 32), tmt::kStreamSweep,
                                                     iter, a.seed));
@@ -615,7 +625,8 @@ k_sweep_doc(SweepArgs a)
                         v_have = v;
                     }
                     float phi_own;
-                    load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phi_own);
+                    load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, __shfl_sync(FULL, my_nkw, j),
+                              has_ri ? __shfl_sync(FULL, my_ri, j) : 0.f, phi_own);
                     for (;;) {
                         const int jn = vm ? __ffs(vm) - 1 : -1;
                         uint32_t vn = 0;
@@ -628,7 +639,8 @@ k_sweep_doc(SweepArgs a)
                             zon = (int)__shfl_sync(FULL, my_z, jn);
                             new_col = vn != v;
                             if (new_col) load_col(vn, pvn);
-                            load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, phion);
+                            load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, __shfl_sync(FULL, my_nkw, jn),
+                                      has_ri ? __shfl_sync(FULL, my_ri, jn) : 0.f, phion);
                         }
                         const float u = __shfl_sync(FULL, my_u, j);
                         const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
@@ -800,7 +812,8 @@ k_sweep_doc(SweepArgs a)
                                 load_col(v, pv);
                                 v_have = v;
                             }
-                            load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, phi_own);
+                            load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, __shfl_sync(FULL, my_nkw, j),
+                                      has_ri ? __shfl_sync(FULL, my_ri, j) : 0.f, phi_own);
                         }
                     }
                 }
