@@ -785,6 +785,7 @@ def main():
     wall = time.perf_counter() - t0
     info = eng.info()
     variants = eng.sweep_variants()
+    tuning_ms = [[round(float(x), 3) for x in row] for row in eng.sweep_timings()]
     split = eng.doc_split()
     launches = info.kernel_launches - launches0
     clk = clocks.stop()
@@ -847,7 +848,7 @@ def main():
             "config": cfgd,
             "corpus": {"realV": int(V), "tokens": N_all_ranks, "tokens_all_ids": int(len(words)) * world},
             "engine": {"sweep_groups": int(info.sweep_groups), "sweep_variants": variants,
-                       "split_docs_per_group": split, "tuning_sweeps": tuning, "term_weight": args.tw,
+                       "tuning_ms": tuning_ms, "split_docs_per_group": split, "tuning_sweeps": tuning, "term_weight": args.tw,
                        "optim_interval": 0},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,

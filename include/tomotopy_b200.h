@@ -266,6 +266,11 @@ tmt_status tmt_set_graphs(tmt_handle* h, int32_t enable);
 /* The sweep-kernel variant the autotuner chose for each document group
  * (-1 while tuning); *n = the number of groups.  Diagnostics only. */
 tmt_status tmt_get_sweep_variants(const tmt_handle* h, int32_t* out, uint32_t cap, uint32_t* n);
+/* The autotuner's measurements: out[g * n_variants + v] = milliseconds of
+ * group g's launches under variant v, summed over the tuning sweeps that ran
+ * it (0 where none has); *n_groups, *n_variants.  Diagnostics only. */
+tmt_status tmt_get_sweep_timings(const tmt_handle* h, float* out, uint32_t cap, uint32_t* n_groups,
+                                 uint32_t* n_variants);
 
 /* Weighted counts (tmt_upload_corpus_weighted): n_dk (D x K row-major),
  * n_kw (V x K, column v = K floats: numByTopicWord of ModelStateLDA<float>),

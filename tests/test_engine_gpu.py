@@ -186,6 +186,12 @@ def test_sweeps_bitexact(K, groups):
         st.doc_live_sweeps(n, start_step=step, groups=groups)
         step += n
         assert_same_state(eng, st)
+    # the tuner is done: each group runs the variant it timed fastest
+    tm, var = eng.sweep_timings(), eng.sweep_variants()
+    assert tm.shape[0] == len(var) and -1 not in var
+    for g, v in enumerate(var):
+        if tm[g].sum() > 0:
+            assert v == int(np.argmin(tm[g])) and (tm[g] > 0).all()
 
 
 @pytest.mark.parametrize("K,groups", [(24, 8), (300, 3)])

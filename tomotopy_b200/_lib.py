@@ -103,6 +103,7 @@ SIGNATURES = {
     "tmt_set_doc_split": (C.c_int, [_H, C.c_uint64, C.c_uint32]),
     "tmt_get_doc_split": (C.c_int, [_H, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tmt_get_sweep_variants": (C.c_int, [_H, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "tmt_get_sweep_timings": (C.c_int, [_H, _P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "tmt_set_optim": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
     "tmt_infer_batch": (C.c_int, [_H, _P, _P, C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P]),
     "tmt_infer_batch_weighted": (C.c_int, [_H, _P, _P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P, _P, _P]),

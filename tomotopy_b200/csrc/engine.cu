@@ -46,6 +46,11 @@ namespace {
 
 using namespace tmtk;
 constexpr int kSweepWarps = 8;           // warps per sweep block
+// warps per block of the 16-bit-row kernels (4 blocks/SM): 7 leave 72
+// registers a thread where 8 leave 64 (at 64 the token loop spills, and
+// spilled registers come back from L2; measured 96.9 vs 101.1 ms per sweep
+// at k = 1000)
+constexpr int kRow16Warps = 7;
 
 // One Hillis-Steele step with the lane test folded into an fma: m is 1 for
 // lanes at or above `off`, else 0, and for the finite sums here fma(y, 1, x)
@@ -457,8 +462,9 @@ struct SweepArgs {
 };
 
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
-// aligned regions): [n_k deltas: KP ints] [per warp: (float)n_dk + alpha, KP
-// floats, zero padded] [per warp: n_dk, KP ints (floats with weighted counts)].
+// aligned regions): [alpha: KP floats] [n_k deltas: KP ints] [per warp:
+// (float)n_dk + alpha, KP floats, zero padded] [per warp: n_dk, KP ints
+// (floats with weighted counts)].  Static: the pass-2 column scratch.
 // With weighted counts the n_k deltas are KP long longs.
 
 
@@ -485,7 +491,7 @@ struct SweepArgs {
 //       65,536 tokens), half the space of 32-bit rows: variant 2 keeps its 4
 //       blocks per SM without reading the row through L1.
 template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
-__global__ void __launch_bounds__(kSweepWarps * 32, MINB)
+__global__ void __launch_bounds__((ROW16 ? kRow16Warps : kSweepWarps) * 32, MINB)
 k_sweep_doc(SweepArgs a)
 {
     static_assert(!(PLAIN && WT), "plain LDA has integer counts");
@@ -499,8 +505,16 @@ k_sweep_doc(SweepArgs a)
     // n_k deltas in shared memory: integer counts only (weighted counts take
     // theirs from the word deltas after the sweep, k_dk_sum)
     const bool dnk_smem = !WT && (PLAIN || a.dnk_smem);
-    int* s_dnk = smem;
-    float* s_rowf = reinterpret_cast<float*>(smem + (dnk_smem ? KP : 0));
+    // alpha (plain LDA reads it from here; the copy is made whatever the kernel)
+    float* s_alpha = reinterpret_cast<float*>(smem);
+    // the hit lane's blocks of four of the word's column, for pass 2 (CH > 0):
+    // a shared-memory read instead of a second trip to L2 for the column
+    // (not in the 4-blocks/SM kernels: at 64 registers the scratch's
+    // addressing spills, and spilled registers come back from L2)
+    constexpr bool kScratch = CH > 0 && MINB < 4;
+    __shared__ __align__(16) float s_xs[kScratch ? kSweepWarps * 4 * CHR : 4];
+    int* s_dnk = smem + KP;
+    float* s_rowf = reinterpret_cast<float*>(s_dnk + (dnk_smem ? KP : 0));
     float* rowf = s_rowf + warp * KP;
     int* s_rowi = reinterpret_cast<int*>(s_rowf + nwarps * KP);
     // split documents (integer counts): the document's row C and the slices'
@@ -509,10 +523,11 @@ k_sweep_doc(SweepArgs a)
     int* s_C = s_rowi + ((a.rowi_smem || split) ? nwarps * KP : 0);
     int* s_dlt = s_C + KP;
     __shared__ uint32_t s_q;
-    if (dnk_smem) {
-        for (int k = threadIdx.x; k < K; k += blockDim.x) s_dnk[k] = 0;
-        __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        s_alpha[k] = a.alpha[k];
+        if (dnk_smem) s_dnk[k] = 0;
     }
+    __syncthreads();
     // blocks of four owned by this lane
     const int nch = 4 * lane < K ? ((K - 4 * lane + 127) >> 7) : 0;
     float lm[5];                         // hs_step's lane masks
@@ -584,7 +599,7 @@ k_sweep_doc(SweepArgs a)
         }
     };
     auto afold = [&](float n, int k) -> float {
-        const float x = __fadd_rn(n, __ldg(alpha + k));
+        const float x = __fadd_rn(n, PLAIN ? s_alpha[k] : __ldg(alpha + k));
         if constexpr (PLAIN) return x;
         else return dmask ? __fmul_rn(x, (float)((__ldg(dmask + (k >> 5)) >> (k & 31)) & 1u)) : x;
     };
@@ -745,6 +760,15 @@ k_sweep_doc(SweepArgs a)
                                 // 32 at a time; up to 16 topics (CH == 4) a 4-step scan gives the
                                 // same prefix values
                                 constexpr int kSteps2 = CH == 4 ? 4 : 5;
+                                if (kScratch) {
+                                    // lane h's column blocks into the warp's scratch (t-th topic at t)
+                                    if (lane == h) {
+    #pragma unroll
+                                        for (int jj = 0; jj < CHR; ++jj)
+                                            if (jj < nch) *reinterpret_cast<float4*>(s_xs + 4 * (CHR * warp + jj)) = pv[jj];
+                                    }
+                                    __syncwarp();
+                                }
                                 float carry = 0.f;
                                 for (int mm = 0; mm < nh; mm += 32) {
                                     const int t = mm + lane;
@@ -753,7 +777,8 @@ k_sweep_doc(SweepArgs a)
                                     // rowf[zo] reads 0 until the draw: fma(sel, phi_own, 0 * phi) is
                                     // Ao * phi_own at zo and fma(0, phi_own, p) == p elsewhere
                                     if (t < nh)
-                                        x2 = __fmaf_rn(k == zo ? Ao : 0.f, phi_own, __fmul_rn(rowf[k], __ldg(ph + k)));
+                                        x2 = __fmaf_rn(k == zo ? Ao : 0.f, phi_own,
+                                                       __fmul_rn(rowf[k], kScratch ? s_xs[4 * CHR * warp + t] : __ldg(ph + k)));
                                     x2 = scan_n(x2, kSteps2);
                                     const unsigned mb =
                                         __ballot_sync(FULL, t < nh && r < __fadd_rn(Eh, __fadd_rn(carry, x2)));
@@ -1566,9 +1591,10 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     s.rowi_smem = K <= 8192 && !rowi_global;
     s.row16 = row16 && rowi_global && !weighted && !split && K <= 8192;
     const uint32_t per_warp = 4 * KP + ((s.rowi_smem || split) ? 4 * KP : 0) + (s.row16 ? 2 * KP : 0);
-    const uint32_t fixed = (s.dnk_smem ? 4 * KP : 0) + (split ? 8 * KP : 0);
+    // alpha (KP floats) ahead of the n_k deltas
+    const uint32_t fixed = 4 * KP + (s.dnk_smem ? 4 * KP : 0) + (split ? 8 * KP : 0);
     uint32_t w = (budget - fixed) / per_warp;
-    s.warps = std::max(1u, std::min((uint32_t)kSweepWarps, w));
+    s.warps = std::max(1u, std::min((uint32_t)(s.row16 ? kRow16Warps : kSweepWarps), w));
     s.smem = fixed + s.warps * per_warp;
     return s;
 }
@@ -1603,7 +1629,8 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
 // topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
-// document row in global memory, 4 blocks/SM.  (Measured and dropped at
+// document row as 16-bit counts in shared memory (7 warps a block) or, for
+// documents of 65,536+ tokens, in global memory, 4 blocks/SM.  (Measured and dropped at
 // K = 1000: the word's column read from L1 every token, 6 blocks/SM, and a
 // per-warp shared-memory copy of it -- fewer instructions, slower sweeps.)
 int sweep_variants_for(uint32_t K)
@@ -2751,6 +2778,23 @@ tmt_status tmt_get_sweep_variants(const tmt_handle* h, int32_t* out, uint32_t ca
     *n = (uint32_t)h->group_variant.size();
     if (out)
         for (uint32_t g = 0; g < *n && g < cap; ++g) out[g] = h->tuned < 0 ? -1 : h->group_variant[g];
+    return TMT_OK;
+}
+
+tmt_status tmt_get_sweep_timings(const tmt_handle* h, float* out, uint32_t cap, uint32_t* n_groups,
+                                 uint32_t* n_variants)
+{
+    if (!h || !n_groups || !n_variants) return TMT_ERR_INVALID_ARGUMENT;
+    *n_groups = (uint32_t)h->group_ms.size();
+    *n_variants = (uint32_t)h->n_variants;
+    if (out) {
+        uint32_t i = 0;
+        for (const auto& g : h->group_ms)
+            for (float ms : g) {
+                if (i < cap) out[i] = ms;
+                ++i;
+            }
+    }
     return TMT_OK;
 }
 

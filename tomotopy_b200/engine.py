@@ -109,6 +109,14 @@ class Engine:
         check(lib.tmt_get_sweep_variants(self.h, _p(out), n.value, C.byref(n)), self.h)
         return out[:n.value].tolist()
 
+    def sweep_timings(self):
+        """The autotuner's milliseconds per document group and variant (G x n_variants)."""
+        g, v = C.c_uint32(), C.c_uint32()
+        check(lib.tmt_get_sweep_timings(self.h, None, 0, C.byref(g), C.byref(v)), self.h)
+        out = np.zeros(max(g.value * v.value, 1), dtype=np.float32)
+        check(lib.tmt_get_sweep_timings(self.h, _p(out), out.size, C.byref(g), C.byref(v)), self.h)
+        return out[:g.value * v.value].reshape(g.value, v.value)
+
     def set_doc_rows(self, row_of_doc, R=None):
         """tmt_set_doc_rows: document d counts in row row_of_doc[d] of R shared
         rows (PT's pseudo-documents); None returns to one row per document."""
