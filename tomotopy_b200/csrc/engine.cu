@@ -46,11 +46,14 @@ namespace {
 
 using namespace tmtk;
 constexpr int kSweepWarps = 8;           // warps per sweep block
-// warps per block of the 16-bit-row kernels (4 blocks/SM): 7 leave 72
-// registers a thread where 8 leave 64 (at 64 the token loop spills, and
-// spilled registers come back from L2; measured 96.9 vs 101.1 ms per sweep
-// at k = 1000)
-constexpr int kRow16Warps = 7;
+// The 16-bit-row kernels (variant 2): 5 warps a block, 5 blocks/SM.  At 8
+// warps x 4 blocks the token loop gets 64 registers and spills (spilled
+// registers come back from L2: the resident warps' columns keep L1 from
+// holding them); smaller blocks also leave L1 more of the SM's 256 KB.
+// Measured at k = 1000 (ms per sweep): 8 x 4 101.1, 7 x 4 97.6, 6 x 4 92.4,
+// 5 x 4 94.7, 4 x 6 92.7, 5 x 5 91.4.
+constexpr int kRow16Warps = 5;
+constexpr int kRow16MinB = 5;
 
 // One Hillis-Steele step with the lane test folded into an fma: m is 1 for
 // lanes at or above `off`, else 0, and for the finite sums here fma(y, 1, x)
@@ -491,7 +494,7 @@ struct SweepArgs {
 //       65,536 tokens), half the space of 32-bit rows: variant 2 keeps its 4
 //       blocks per SM without reading the row through L1.
 template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
-__global__ void __launch_bounds__((ROW16 ? kRow16Warps : kSweepWarps) * 32, MINB)
+__global__ void __launch_bounds__((ROW16 ? kRow16Warps : kSweepWarps) * 32, ROW16 ? kRow16MinB : MINB)
 k_sweep_doc(SweepArgs a)
 {
     static_assert(!(PLAIN && WT), "plain LDA has integer counts");
@@ -1629,8 +1632,9 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 
 // Variants (identical results, different speed): 0 = prefetch (up to 1024
 // topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
-// document row as 16-bit counts in shared memory (7 warps a block) or, for
-// documents of 65,536+ tokens, in global memory, 4 blocks/SM.  (Measured and dropped at
+// document row as 16-bit counts in shared memory (5 warps a block, 5
+// blocks/SM) or, for documents of 65,536+ tokens, in global memory (4
+// blocks/SM).  (Measured and dropped at
 // K = 1000: the word's column read from L1 every token, 6 blocks/SM, and a
 // per-warp shared-memory copy of it -- fewer instructions, slower sweeps.)
 int sweep_variants_for(uint32_t K)
