@@ -50,7 +50,8 @@ constexpr int kSweepWarps = 8;           // warps per sweep block
 // warps x 4 blocks the token loop gets 64 registers and spills (spilled
 // registers come back from L2: the resident warps' columns keep L1 from
 // holding them); smaller blocks also leave L1 more of the SM's 256 KB.
-// Measured at k = 1000 (ms per sweep): 8 x 4 101.1, 7 x 4 97.6, 6 x 4 92.4,
+// Measured at k = 1000 (ms per sweep): 8 x 4 101.1 (before alpha moved to
+// shared memory; 101.9 after, spilling), 7 x 4 97.6, 6 x 4 92.4,
 // 5 x 4 94.7, 4 x 6 92.7, 5 x 5 91.4.
 constexpr int kRow16Warps = 5;
 constexpr int kRow16MinB = 5;
@@ -467,8 +468,8 @@ struct SweepArgs {
 // Shared-memory layout of a sweep block (offsets in 4-byte words, 16-byte
 // aligned regions): [alpha: KP floats] [n_k deltas: KP ints] [per warp:
 // (float)n_dk + alpha, KP floats, zero padded] [per warp: n_dk, KP ints
-// (floats with weighted counts)].  Static: the pass-2 column scratch.
-// With weighted counts the n_k deltas are KP long longs.
+// (floats with weighted counts)]; with weighted counts there are no n_k
+// deltas here.  Static: the pass-2 column scratch.
 
 
 
@@ -491,8 +492,8 @@ struct SweepArgs {
 //       the same arithmetic).
 //   ROW16: the document's count row lives in shared memory as 16-bit counts
 //       (the host guarantees every document of the launch is shorter than
-//       65,536 tokens), half the space of 32-bit rows: variant 2 keeps its 4
-//       blocks per SM without reading the row through L1.
+//       65,536 tokens), half the space of 32-bit rows: variant 2 runs 5
+//       blocks of 5 warps per SM without reading the row through L1.
 template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
 __global__ void __launch_bounds__((ROW16 ? kRow16Warps : kSweepWarps) * 32, ROW16 ? kRow16MinB : MINB)
 k_sweep_doc(SweepArgs a)
@@ -512,8 +513,9 @@ k_sweep_doc(SweepArgs a)
     float* s_alpha = reinterpret_cast<float*>(smem);
     // the hit lane's blocks of four of the word's column, for pass 2 (CH > 0):
     // a shared-memory read instead of a second trip to L2 for the column
-    // (not in the 4-blocks/SM kernels: at 64 registers the scratch's
-    // addressing spills, and spilled registers come back from L2)
+    // (not in the MINB-4 kernels: in the 16-bit-row kernel it measured
+    // slower, 94.9 vs 92.7 ms per sweep at k = 1000, and at 64 registers its
+    // addressing spills, spilled registers coming back from L2)
     constexpr bool kScratch = CH > 0 && MINB < 4;
     __shared__ __align__(16) float s_xs[kScratch ? kSweepWarps * 4 * CHR : 4];
     int* s_dnk = smem + KP;
