@@ -478,8 +478,6 @@ struct SweepArgs {
 // and shared-memory float4 reads are conflict-free.
 //   CH > 0: at most CH blocks per lane (KP <= 128*CH <= 4096), unrolled.
 //   CH == 0: any K, runtime loops.
-//   PF: the next token's word weights are loaded while the current token is
-//       sampled (the loads do not depend on the document row).
 //   WT: weighted counts (TermWeight IDF / PMI): n_dk, n_kw, n_k are floats,
 //       every token carries a weight w, a removal clamps at 0 (updateCnt<true>,
 //       Utils.hpp:132-155) and the count deltas are integers in units of 2^-24.
@@ -492,9 +490,9 @@ struct SweepArgs {
 //       the same arithmetic).
 //   ROW16: the document's count row lives in shared memory as 16-bit counts
 //       (the host guarantees every document of the launch is shorter than
-//       65,536 tokens), half the space of 32-bit rows: variant 2 runs 5
+//       65,536 tokens), half the space of 32-bit rows: variant 1 runs 5
 //       blocks of 5 warps per SM without reading the row through L1.
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
+template <int CH, int MINB, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
 __global__ void __launch_bounds__((ROW16 ? kRow16Warps : kSweepWarps) * 32, ROW16 ? kRow16MinB : MINB)
 k_sweep_doc(SweepArgs a)
 {
@@ -509,7 +507,7 @@ k_sweep_doc(SweepArgs a)
     // n_k deltas in shared memory: integer counts only (weighted counts take
     // theirs from the word deltas after the sweep, k_dk_sum)
     const bool dnk_smem = !WT && (PLAIN || a.dnk_smem);
-    // alpha (plain LDA reads it from here; the copy is made whatever the kernel)
+    // alpha (read from here unless per-document alpha rows are set)
     float* s_alpha = reinterpret_cast<float*>(smem);
     // the hit lane's blocks of four of the word's column, for pass 2 (CH > 0):
     // a shared-memory read instead of a second trip to L2 for the column
@@ -604,7 +602,8 @@ k_sweep_doc(SweepArgs a)
         }
     };
     auto afold = [&](float n, int k) -> float {
-        const float x = __fadd_rn(n, PLAIN ? s_alpha[k] : __ldg(alpha + k));
+        // (the shared copy unless the document has its own alpha row)
+        const float x = __fadd_rn(n, (PLAIN || !a.arow) ? s_alpha[k] : __ldg(alpha + k));
         if constexpr (PLAIN) return x;
         else return dmask ? __fmul_rn(x, (float)((__ldg(dmask + (k >> 5)) >> (k & 31)) & 1u)) : x;
     };
@@ -649,19 +648,6 @@ k_sweep_doc(SweepArgs a)
                               has_ri ? __shfl_sync(FULL, my_ri, j) : 0.f, phi_own);
                     for (;;) {
                         const int jn = vm ? __ffs(vm) - 1 : -1;
-                        uint32_t vn = 0;
-                        int zon = 0;
-                        float4 pvn[CHR];
-                        float phion = 0.f;
-                        bool new_col = false;
-                        if (PF && jn >= 0) {
-                            vn = __shfl_sync(FULL, my_w, jn);
-                            zon = (int)__shfl_sync(FULL, my_z, jn);
-                            new_col = vn != v;
-                            if (new_col) load_col(vn, pvn);
-                            load_word(vn, zon, WT ? __shfl_sync(FULL, my_wt, jn) : 1.f, __shfl_sync(FULL, my_nkw, jn),
-                                      has_ri ? __shfl_sync(FULL, my_ri, jn) : 0.f, phion);
-                        }
                         const float u = __shfl_sync(FULL, my_u, j);
                         const float wt = WT ? __shfl_sync(FULL, my_wt, j) : 1.f;
                         const float* ph = a.phi + (uint64_t)v * KP;
@@ -826,25 +812,14 @@ k_sweep_doc(SweepArgs a)
                         if (jn < 0) break;
                         j = jn;
                         vm &= vm - 1;
-                        if (PF) {
-                            if (new_col) {
-    #pragma unroll
-                                for (int jj = 0; jj < CHR; ++jj) pv[jj] = pvn[jj];
-                                v_have = vn;
-                            }
-                            v = vn;
-                            zo = zon;
-                            phi_own = phion;
-                        } else {
-                            v = __shfl_sync(FULL, my_w, j);
-                            zo = (int)__shfl_sync(FULL, my_z, j);
-                            if (v != v_have) {
-                                load_col(v, pv);
-                                v_have = v;
-                            }
-                            load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, __shfl_sync(FULL, my_nkw, j),
-                                      has_ri ? __shfl_sync(FULL, my_ri, j) : 0.f, phi_own);
+                        v = __shfl_sync(FULL, my_w, j);
+                        zo = (int)__shfl_sync(FULL, my_z, j);
+                        if (v != v_have) {
+                            load_col(v, pv);
+                            v_have = v;
                         }
+                        load_word(v, zo, WT ? __shfl_sync(FULL, my_wt, j) : 1.f, __shfl_sync(FULL, my_nkw, j),
+                                  has_ri ? __shfl_sync(FULL, my_ri, j) : 0.f, phi_own);
                     }
                 }
                 if (my_i < e && my_w < a.V) a.z[my_i] = (uint16_t)my_new;
@@ -1604,10 +1579,10 @@ SweepShape sweep_shape(uint32_t K, bool weighted, bool rowi_global = false, bool
     return s;
 }
 
-template <int CH, int MINB, bool PF, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
+template <int CH, int MINB, bool WT, bool SPLIT = false, bool PLAIN = false, bool ROW16 = false>
 void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
 {
-    auto kern = k_sweep_doc<CH, MINB, PF, WT, SPLIT, PLAIN, ROW16>;
+    auto kern = k_sweep_doc<CH, MINB, WT, SPLIT, PLAIN, ROW16>;
     // attribute and occupancy once per kernel and shared-memory size (the
     // shapes depend on K and on whether the launch splits documents), so a
     // captured sweep makes no such call; the attribute allows the largest shape
@@ -1632,38 +1607,38 @@ void launch_sweep_t(tmt_handle* h, const SweepArgs& a, const SweepShape& sh)
     launch_check(h);
 }
 
-// Variants (identical results, different speed): 0 = prefetch (up to 1024
-// topics), 2 blocks/SM; 1 = no prefetch, 3 blocks/SM; 2 = no prefetch, the
-// document row as 16-bit counts in shared memory (5 warps a block, 5
-// blocks/SM) or, for documents of 65,536+ tokens, in global memory (4
-// blocks/SM).  (Measured and dropped at
-// K = 1000: the word's column read from L1 every token, 6 blocks/SM, and a
-// per-warp shared-memory copy of it -- fewer instructions, slower sweeps.)
+// Variants (identical results, different speed): 0 = the document row in
+// shared memory as 32-bit counts, 3 blocks/SM; 1 = the row as 16-bit counts
+// in shared memory (5 warps a block, 5 blocks/SM) or, for documents of
+// 65,536+ tokens, in global memory (4 blocks/SM).  (Measured and dropped:
+// loading the next token's column into registers during the current token,
+// 2 blocks/SM -- slower at every benchmark configuration once the per-token
+// loads came off the chain, e.g. 20.5 vs 11.4 ms per group at k = 1000, and
+// two of the tuner's sweeps spent on it; at K = 1000, the word's column
+// read from L1 every token, 6 blocks/SM, and a per-warp shared-memory copy
+// of it -- fewer instructions, slower sweeps.)
 int sweep_variants_for(uint32_t K)
 {
-    return (round4(K) + 127) / 128 > 32 ? 1 : 3;
+    return (round4(K) + 127) / 128 > 32 ? 1 : 2;
 }
 
 template <int CH, bool WT, bool PLAIN>
 void launch_sweep_cp(tmt_handle* h, const SweepArgs& a, const SweepShape& sh, int variant)
 {
-    constexpr bool kPrefetch = CH <= 8;   // above, the prefetch registers spill
     // split documents: integer counts, up to 4 blocks of four topics per lane
     constexpr bool kSplit = !WT && CH >= 1 && CH <= 4;
     if (kSplit && a.n_long > 0) {
-        if (variant >= 2) launch_sweep_t<CH, 4, false, WT, kSplit, PLAIN>(h, a, sh);
-        else if (variant == 1) launch_sweep_t<CH, 3, false, WT, kSplit, PLAIN>(h, a, sh);
-        else launch_sweep_t<CH, 2, kPrefetch, WT, kSplit, PLAIN>(h, a, sh);
+        if (variant >= 1) launch_sweep_t<CH, 4, WT, kSplit, PLAIN>(h, a, sh);
+        else launch_sweep_t<CH, 3, WT, kSplit, PLAIN>(h, a, sh);
         return;
     }
-    if (variant >= 2) {
+    if (variant >= 1) {
         if constexpr (!WT) {
-            if (sh.row16) return launch_sweep_t<CH, 4, false, WT, false, PLAIN, true>(h, a, sh);
+            if (sh.row16) return launch_sweep_t<CH, 4, WT, false, PLAIN, true>(h, a, sh);
         }
-        launch_sweep_t<CH, 4, false, WT, false, PLAIN>(h, a, sh);
+        launch_sweep_t<CH, 4, WT, false, PLAIN>(h, a, sh);
     }
-    else if (variant == 1) launch_sweep_t<CH, 3, false, WT, false, PLAIN>(h, a, sh);
-    else launch_sweep_t<CH, 2, kPrefetch, WT, false, PLAIN>(h, a, sh);
+    else launch_sweep_t<CH, 3, WT, false, PLAIN>(h, a, sh);
 }
 
 // plain: the launch has none of the conditional's options (PLAIN kernels)
@@ -1685,7 +1660,7 @@ void launch_sweep_w(tmt_handle* h, const SweepArgs& b, const SweepShape& sh, uin
     else if (ch <= 8) launch_sweep_ch<8, WT>(h, b, sh, variant, plain);
     else if (ch <= 16) launch_sweep_ch<16, WT>(h, b, sh, variant, plain);
     else if (ch <= 32) launch_sweep_ch<32, WT>(h, b, sh, variant, plain);
-    else launch_sweep_t<0, 3, false, WT>(h, b, sh);
+    else launch_sweep_t<0, 3, WT>(h, b, sh);
 }
 
 void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
@@ -1695,7 +1670,7 @@ void launch_sweep(tmt_handle* h, const SweepArgs& a, int variant)
     const bool wt = a.wt != nullptr;
     const bool split = !wt && a.n_long > 0;
     // 16-bit rows when every document of the launch is shorter than 65,536 tokens
-    const SweepShape sh = sweep_shape(a.K, wt, variant >= 2, split, a.max_len < 65536);
+    const SweepShape sh = sweep_shape(a.K, wt, variant >= 1, split, a.max_len < 65536);
     if (!wt && a.n_long > 0 && sh.warps != (uint32_t)kSweepWarps)
         throw CudaError("split documents need a block of " + std::to_string(kSweepWarps) + " warps");
     SweepArgs b = a;
@@ -2283,8 +2258,8 @@ tmt_status upload_impl(tmt_handle* h, const uint32_t* wid, const uint64_t* doc_o
             CK(cudaStreamSynchronize(s0));
         }
         {
-            // the first n_variants sweeps run eagerly, one variant each, and
-            // every group keeps its fastest
+            // the first 2 n_variants sweeps run eagerly, the variants in the
+            // order 0 .. n-1, n-1 .. 0, and every group keeps its fastest
             const uint32_t G = (uint32_t)h->group_bounds.size() - 1;
             h->n_variants = sweep_variants_for(K);
             h->variant = 0;
