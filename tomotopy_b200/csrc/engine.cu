@@ -52,7 +52,7 @@ constexpr int kSweepWarps = 8;           // warps per sweep block
 // holding them); smaller blocks also leave L1 more of the SM's 256 KB.
 // Measured at k = 1000 (ms per sweep): 8 x 4 101.1 (before alpha moved to
 // shared memory; 101.9 after, spilling), 7 x 4 97.6, 6 x 4 92.4,
-// 5 x 4 94.7, 4 x 6 92.7, 5 x 5 91.4.
+// 5 x 4 94.7, 4 x 6 92.7, 4 x 7 97.1, 3 x 8 98.0, 5 x 5 91.4.
 constexpr int kRow16Warps = 5;
 constexpr int kRow16MinB = 5;
 
