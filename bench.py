@@ -53,7 +53,7 @@ def bytes_per_sweep(N, K, V):
 # dram__bytes_write.sum), keyed by config: shown beside the roofline as the
 # capture it came from; the bench itself measures no DRAM traffic, so its
 # roofline.traffic stays null.
-NCU_TRAFFIC = {"c3": {"bytes_per_sweep": 107.8e9 + 9.6e9,
+NCU_TRAFFIC = {"c3": {"bytes_per_sweep": 108.3e9 + 9.6e9,
                       "source": "profiles/k_sweep_doc_c3_traffic.md (100k-document capture scaled by tokens, "
                                 "plus k_phi_copy)"}}
 
