@@ -219,7 +219,7 @@ __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __res
                            uint32_t KP, float eta, float veta, float* __restrict__ phi, int32_t* __restrict__ nkw_next,
                            int32_t* __restrict__ nk_next, uint32_t smem_k, PriorArgs pr, float* __restrict__ rm1)
 {
-    extern __shared__ float s_R[];
+    extern __shared__ __align__(16) float s_R[];
     const bool r_smem = K <= smem_k;
     if (r_smem)
         for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
@@ -230,6 +230,24 @@ __global__ void k_phi_copy(const int32_t* __restrict__ nkw, const int32_t* __res
             rm1[k] = __fdiv_rn(1.0f, __fadd_rn((float)(nk[k] - 1), esum_of(pr, k, veta)));
         }
     __syncthreads();
+    if (r_smem && (K & 3) == 0 && !pr.idx) {
+        // K a multiple of 4 (KP == K) and no word priors: 16-byte loads and
+        // stores, the same values
+        const uint32_t K4 = K >> 2;
+        for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
+            const int4* src = reinterpret_cast<const int4*>(nkw + v * K);
+            int4* dst = reinterpret_cast<int4*>(nkw_next + v * K);
+            float4* ph = reinterpret_cast<float4*>(phi + v * KP);
+            for (uint32_t k4 = threadIdx.x; k4 < K4; k4 += blockDim.x) {
+                const int4 n = __ldg(src + k4);
+                dst[k4] = n;
+                const float4 R = reinterpret_cast<const float4*>(s_R)[k4];
+                ph[k4] = make_float4(__fmul_rn(__fadd_rn((float)n.x, eta), R.x), __fmul_rn(__fadd_rn((float)n.y, eta), R.y),
+                                     __fmul_rn(__fadd_rn((float)n.z, eta), R.z), __fmul_rn(__fadd_rn((float)n.w, eta), R.w));
+            }
+        }
+        return;
+    }
     for (uint64_t v = blockIdx.x; v < V; v += gridDim.x) {
         const int32_t* src = nkw + v * K;
         int32_t* dst = nkw_next + v * K;
